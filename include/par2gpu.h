@@ -1,0 +1,327 @@
+/*
+ * par2gpu.h -- C ABI of the B200 PAR2 create engine (libpar2gpu.so).
+ *
+ * Drop-in boundary for the create path of javi11/par2rust v0.1.0.  Each entry
+ * point below names the reference interface it replaces (file:line within the
+ * par2rust crate).  Plain pointers and sizes only; no CUDA or torch types in
+ * the signatures (streams are passed as `void *` holding a cudaStream_t).
+ *
+ * Threading: calls are synchronous and thread-safe; the library serialises
+ * work on its per-process device context.  Progress callbacks run on the
+ * calling thread.  Strings and arrays returned by the library are owned by
+ * the caller and released with the matching p2g_*_free function.
+ *
+ * Errors: every entry point returns a p2g_status.  The P2G_ERR_* values from
+ * IO to INVALID_VOLUME_SCHEME map one to one onto the reference's Par2Error
+ * variants (src/error.rs:7-41); p2g_last_error_message() gives the same text
+ * and p2g_last_error_detail() the TooManyInputBlocks fields (thread-local).
+ */
+#ifndef PAR2GPU_H
+#define PAR2GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define P2G_ABI_VERSION 1
+
+/* src/creator.rs:102-108 */
+#define P2G_MAX_FILES 32768u
+#define P2G_MAX_INPUT_BLOCKS 32768u
+#define P2G_MAX_RECOVERY_BLOCKS 65535u
+/* src/source.rs:17 */
+#define P2G_HASH16K_LEN 16384u
+
+/* Par2Error, src/error.rs:7-41, plus the device-side failures. */
+typedef enum p2g_status {
+    P2G_OK = 0,
+    P2G_ERR_IO = 1,                      /* Par2Error::Io */
+    P2G_ERR_INVALID_SLICE_SIZE = 2,      /* Par2Error::InvalidSliceSize */
+    P2G_ERR_INVALID_FILE_NAME = 3,       /* Par2Error::InvalidFileName */
+    P2G_ERR_NO_INPUT_FILES = 4,          /* Par2Error::NoInputFiles */
+    P2G_ERR_EMPTY_FILE = 5,              /* Par2Error::EmptyFile */
+    P2G_ERR_TOO_MANY_FILES = 6,          /* Par2Error::TooManyFiles */
+    P2G_ERR_TOO_MANY_RECOVERY_BLOCKS = 7,/* Par2Error::TooManyRecoveryBlocks */
+    P2G_ERR_TOO_MANY_INPUT_BLOCKS = 8,   /* Par2Error::TooManyInputBlocks */
+    P2G_ERR_INVALID_VOLUME_SCHEME = 9,   /* Par2Error::InvalidVolumeScheme */
+    P2G_ERR_INVALID_ARGUMENT = 20,       /* bad pointer / alignment / size at the ABI */
+    P2G_ERR_CUDA = 21,                   /* CUDA runtime error or no usable device */
+    P2G_ERR_OOM = 22,                    /* device or pinned-host allocation failed */
+    P2G_ERR_TIMEOUT = 23                 /* a bounded device wait gave up */
+} p2g_status;
+
+/* Par2Error::TooManyInputBlocks{count, slice_size, suggested}, src/error.rs:29-37 */
+typedef struct p2g_error_detail {
+    uint64_t count;
+    uint64_t slice_size;
+    uint64_t suggested;
+} p2g_error_detail;
+
+const char *p2g_last_error_message(void);
+void p2g_last_error_detail(p2g_error_detail *out);
+int p2g_abi_version(void);
+
+/* SliceChecksum, src/source.rs:28-31.  20 bytes, exactly one IFSC entry
+ * (md5 ‖ crc32 little-endian), src/packet/file_verify.rs:12-23. */
+typedef struct p2g_slice_checksum {
+    uint8_t md5[16];
+    uint32_t crc32;
+} p2g_slice_checksum;
+
+/* SourceFile, src/source.rs:37-47.  Filled by p2g_scan; freed with
+ * p2g_source_file_free.  Callers may also fill one themselves (as the
+ * reference's tests fabricate SourceFile values). */
+typedef struct p2g_source_file {
+    uint8_t *name;      /* display name bytes, no NUL terminator required */
+    size_t name_len;
+    char *path;         /* NUL-terminated on-disk path */
+    uint64_t length;
+    uint8_t hash_full[16];
+    uint8_t hash16k[16];
+    uint8_t file_id[16];
+    p2g_slice_checksum *slice_checksums;
+    uint64_t slice_count;
+} p2g_source_file;
+void p2g_source_file_free(p2g_source_file *sf);
+
+/* VolumeScheme, src/creator.rs:111-139. */
+typedef enum p2g_scheme_kind {
+    P2G_SCHEME_SINGLE = 0,
+    P2G_SCHEME_EXPONENTIAL = 1,
+    P2G_SCHEME_UNIFORM = 2,  /* Uniform{count} */
+    P2G_SCHEME_LIMITED = 3,  /* Limited{max_blocks_per_volume, inner} */
+    P2G_SCHEME_EXPLICIT = 4  /* Explicit(sizes) */
+} p2g_scheme_kind;
+typedef struct p2g_volume_scheme {
+    uint32_t kind;
+    uint32_t count;
+    uint32_t max_blocks_per_volume;
+    const struct p2g_volume_scheme *inner;
+    const uint32_t *explicit_sizes;
+    uint32_t explicit_count;
+} p2g_volume_scheme;
+
+/* CreateOptions, src/creator.rs:142-173 (defaults: slice 4096, R 0, Single). */
+typedef struct p2g_create_options {
+    const char *output;
+    uint64_t slice_size;
+    uint32_t recovery_block_count;
+    p2g_volume_scheme volume_scheme;
+    const char *const *comments; /* UTF-8 strings */
+    uint32_t comment_count;
+} p2g_create_options;
+
+/* ProgressEvent, src/progress.rs:26-60. */
+typedef enum p2g_event_kind {
+    P2G_EV_SCAN_STARTED = 0,
+    P2G_EV_SCAN_PROGRESS = 1,
+    P2G_EV_SCAN_COMPLETED = 2,
+    P2G_EV_ENCODE_STARTED = 3,
+    P2G_EV_ENCODE_PROGRESS = 4,
+    P2G_EV_ENCODE_COMPLETED = 5,
+    P2G_EV_INDEX_WRITTEN = 6,
+    P2G_EV_VOLUME_WRITTEN = 7
+} p2g_event_kind;
+typedef struct p2g_progress_event {
+    uint32_t kind;
+    const char *path;
+    uint64_t total_slices;
+    uint64_t slices_done;
+    uint32_t volume_index;
+    uint32_t total_volumes;
+    uint64_t input_blocks;
+    uint32_t recovery_blocks;
+    uint64_t input_block_done;
+} p2g_progress_event;
+/* ProgressReporter::on_event, src/progress.rs:18-20 */
+typedef void (*p2g_progress_fn)(const p2g_progress_event *ev, void *user);
+
+typedef struct p2g_path_list {
+    char **paths;
+    uint32_t count;
+} p2g_path_list;
+void p2g_path_list_free(p2g_path_list *pl);
+void p2g_string_free(char *s);
+
+/* ---- create pipeline ------------------------------------------------- */
+
+/* SourceFile::scan, src/source.rs:53-55 / scan_with_progress :59-136.
+ * Per-slice MD5+CRC32, hash16k and hash_full run on the device. */
+p2g_status p2g_scan(const char *path, const uint8_t *display_name, size_t name_len,
+                    uint64_t slice_size, p2g_source_file *out);
+p2g_status p2g_scan_with_progress(const char *path, const uint8_t *display_name,
+                                  size_t name_len, uint64_t slice_size, p2g_progress_fn cb,
+                                  void *user, p2g_source_file *out);
+
+/* run_create, src/creator.rs:182-184 / run_create_with_progress :188-321.
+ * Writes the index and volume files; `out` lists them, index first. */
+p2g_status p2g_run_create(const p2g_create_options *opts, const p2g_source_file *sources,
+                          uint32_t n, p2g_path_list *out);
+p2g_status p2g_run_create_with_progress(const p2g_create_options *opts,
+                                        const p2g_source_file *sources, uint32_t n,
+                                        p2g_progress_fn cb, void *user, p2g_path_list *out);
+
+/* run_create_fused, src/creator.rs:447-700: inputs are (path, display name)
+ * pairs; each file is read once and scanned and encoded from the same
+ * device-resident copy. */
+typedef struct p2g_input {
+    const char *path;
+    const uint8_t *display_name;
+    size_t name_len;
+} p2g_input;
+p2g_status p2g_run_create_fused(const p2g_create_options *opts, const p2g_input *inputs,
+                                uint32_t n, p2g_progress_fn cb, void *user, p2g_path_list *out);
+
+/* write_index_file, src/creator.rs:847-860 */
+p2g_status p2g_write_index_file(const p2g_create_options *opts, const p2g_source_file *sources,
+                                uint32_t n, char **out_path);
+
+/* In-memory form of run_create_fused (no filesystem): the same index and
+ * volume bytes, returned in caller-freed buffers.  `sources_out`, when not
+ * NULL, receives n scanned SourceFile records (free each with
+ * p2g_source_file_free).  Inputs are host pointers (pinned memory is copied
+ * without staging). */
+typedef struct p2g_buffer_input {
+    const uint8_t *data;
+    uint64_t length;
+    const uint8_t *display_name;
+    size_t name_len;
+} p2g_buffer_input;
+typedef struct p2g_output_file {
+    char *name;
+    uint8_t *data;
+    uint64_t length;
+} p2g_output_file;
+typedef struct p2g_output_set {
+    p2g_output_file *files;
+    uint32_t count;
+} p2g_output_set;
+p2g_status p2g_create_in_memory(const p2g_create_options *opts, const p2g_buffer_input *inputs,
+                                uint32_t n, p2g_source_file *sources_out, p2g_output_set *out);
+void p2g_output_set_free(p2g_output_set *os);
+
+/* ---- hot-path seams -------------------------------------------------- */
+
+/* Pointer placement for the seams below. */
+#define P2G_HOST_POINTERS 0u
+#define P2G_DEVICE_POINTERS 1u
+
+/* gf_mul_xor_dispatch, src/galois_simd.rs:640-643 (and the scalar reference
+ * gf_mul_xor_scalar, src/reedsolomon.rs:87-126): out ^= coeff * in over
+ * little-endian GF(2^16) symbols.  len must be even. */
+p2g_status p2g_gf_mul_xor(uint16_t coeff, const uint8_t *input, uint8_t *output, size_t len,
+                          uint32_t flags, void *stream);
+
+/* encode_all_recovery_blocks, src/creator.rs:883-1018 (RsEncoder
+ * src/reedsolomon.rs:39-60): recovery[r] = XOR_s c(r,s) * source[s] with
+ * c(r,s) = base_s ^ (first_exponent + r).  Source slice s is read at
+ * src + s*src_stride (zero-padded slices), recovery row r is written at
+ * recovery + r*recovery_stride.  With P2G_DEVICE_POINTERS, src_stride and
+ * recovery_stride must be multiples of 16 and both pointers 16-byte
+ * aligned, and the work is enqueued on `stream` (0 = legacy default). */
+typedef struct p2g_encode_job {
+    const uint8_t *src;
+    uint64_t src_stride;
+    uint32_t input_count;
+    uint64_t slice_size;
+    uint32_t recovery_count;
+    uint16_t first_exponent;
+    uint8_t *recovery;
+    uint64_t recovery_stride;
+    uint32_t flags;
+    void *stream;
+} p2g_encode_job;
+p2g_status p2g_encode(const p2g_encode_job *job);
+
+/* The per-slice half of scan_via_mmap, src/source.rs:165-220: MD5 and
+ * CRC32 of `count` slices (slice i at src + i*src_stride, slice_size bytes,
+ * already zero-padded). */
+p2g_status p2g_slice_checksums(const uint8_t *src, uint64_t src_stride, uint32_t count,
+                               uint64_t slice_size, p2g_slice_checksum *out, uint32_t flags,
+                               void *stream);
+
+/* The file half of scan_via_mmap, src/source.rs:222-228: hash_full (MD5 of
+ * the real bytes) and hash16k (MD5 of the first min(len,16384) bytes) of
+ * `n` files, file f at data[f] (host or device per flags). */
+p2g_status p2g_file_hashes(const uint8_t *const *data, const uint64_t *lengths, uint32_t n,
+                           uint8_t *hash_full_out, uint8_t *hash16k_out, uint32_t flags,
+                           void *stream);
+
+/* The packet MD5 of build_recovery_packet + build_packet
+ * (src/packet/recovery.rs:11-19, src/format.rs:33-54): for each row r,
+ * MD5(set_id ‖ "PAR 2.0\0RecvSlic" ‖ le32(first_exponent+r) ‖ row r). */
+p2g_status p2g_recovery_packet_md5(const uint8_t set_id[16], const uint8_t *recovery,
+                                   uint64_t recovery_stride, uint32_t count, uint64_t slice_size,
+                                   uint16_t first_exponent, uint8_t *md5_out, uint32_t flags,
+                                   void *stream);
+
+/* One whole create job with the source already in device memory: the
+ * device work of run_create_fused minus file I/O.  `src` holds the n files
+ * back to back in caller order, each starting on a slice boundary and
+ * zero-padded to a whole number of slices (slice s at src + s*slice_size).
+ * Produces, in device memory: recovery rows (recovery_stride apart), the
+ * per-slice checksums, hash16k and (unless P2G_JOB_SKIP_HASH_FULL) hash_full
+ * per file, and the recovery-packet MD5s.  The set id is derived on the host
+ * from the device hash16k values (src/source.rs:303-309,
+ * src/packet/main_packet.rs:25-42); names are the files' display names.
+ * All work is ordered on `stream`. */
+#define P2G_JOB_SKIP_HASH_FULL 2u
+typedef struct p2g_device_job {
+    const uint8_t *src;
+    uint32_t file_count;
+    const uint64_t *file_lengths;       /* host array */
+    const uint8_t *const *names;        /* host array of display names */
+    const size_t *name_lens;
+    uint64_t slice_size;
+    uint32_t recovery_count;
+    uint8_t *recovery;                  /* device */
+    uint64_t recovery_stride;
+    p2g_slice_checksum *checksums;      /* device, one per input slice */
+    uint8_t *hash_full;                 /* device, 16 per file */
+    uint8_t *hash16k;                   /* device, 16 per file */
+    uint8_t *packet_md5;                /* device, 16 per recovery row */
+    uint8_t set_id_out[16];             /* host, filled */
+    uint32_t flags;
+    void *stream;
+} p2g_device_job;
+p2g_status p2g_run_device_job(p2g_device_job *job);
+
+/* ---- host helpers of the reference's public format/packet modules ----- */
+
+/* generate_input_bases, src/reedsolomon.rs:130-149 */
+p2g_status p2g_input_bases(uint32_t count, uint16_t *out);
+/* gf_mul / gf_pow, src/galois.rs:57-87 */
+uint16_t p2g_gf_mul(uint16_t a, uint16_t b);
+uint16_t p2g_gf_pow(uint16_t base, uint32_t exp);
+/* resolve_volume_sizes, src/creator.rs:325-431: returns the volume count in
+ * *n_out (sizes written when out != NULL and cap allows). */
+p2g_status p2g_resolve_volume_sizes(const p2g_volume_scheme *scheme, uint32_t total,
+                                    uint32_t *out, uint32_t cap, uint32_t *n_out);
+/* derive_volume_filename, src/creator.rs:1046-1057 (caller frees) */
+char *p2g_volume_filename(const char *index_path, uint16_t first_exponent, uint32_t count);
+/* build_packet, src/format.rs:33-54; returns the packet length, writes when out != NULL */
+size_t p2g_build_packet(const uint8_t set_id[16], const uint8_t type_tag[16],
+                        const uint8_t *body, size_t body_len, uint8_t *out);
+/* build_main_packet, src/packet/main_packet.rs:25-42 */
+size_t p2g_build_main_packet(uint64_t slice_size, const uint8_t *file_ids, uint32_t n,
+                             uint8_t set_id_out[16], uint8_t *out);
+/* compute_file_id, src/source.rs:303-309 */
+void p2g_compute_file_id(const uint8_t hash16k[16], uint64_t length, const uint8_t *name,
+                         size_t name_len, uint8_t out[16]);
+/* host MD5 used for packet framing (md5_impl::digest, src/md5_impl.rs:24-48) */
+void p2g_md5(const uint8_t *data, size_t len, uint8_t out[16]);
+
+/* ---- device / runtime info ------------------------------------------- */
+/* Number of kernel launches this process has issued through the library
+ * (monotonic); lets callers count device work inside a timed region. */
+uint64_t p2g_kernel_launch_count(void);
+/* 0 when a device is usable; fills a short description. */
+p2g_status p2g_device_info(char *buf, size_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

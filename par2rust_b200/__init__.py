@@ -1,0 +1,650 @@
+"""par2rust_b200 -- B200 PAR2 create engine, Python mirror of the par2rust API.
+
+The names follow the reference crate's public surface (src/lib.rs:42-61):
+``run_create``, ``run_create_with_progress``, ``run_create_fused``,
+``write_index_file``, ``CreateOptions``, ``VolumeScheme``, ``SourceFile``
+(with ``scan`` / ``scan_with_progress``), ``ProgressEvent``,
+``ProgressReporter``, ``Par2Error`` and the ``MAX_*`` limits.  Every call
+goes through the C ABI of ``libpar2gpu.so`` (include/par2gpu.h); the
+Reed-Solomon accumulator and all bulk hashing run as sm_100a kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Callable, Iterable, List, Optional, Sequence, Tuple, Union
+
+from . import _ffi
+from ._ffi import lib
+
+MAX_FILES = 32_768
+MAX_INPUT_BLOCKS = 32_768
+MAX_RECOVERY_BLOCKS = 65_535
+HASH16K_LEN = 16 * 1024
+
+HOST_POINTERS = 0
+DEVICE_POINTERS = 1
+JOB_SKIP_HASH_FULL = 2
+
+
+# ---------------------------------------------------------------------------
+# Errors: Par2Error variants (src/error.rs:7-41)
+# ---------------------------------------------------------------------------
+class Par2Error(Exception):
+    status = -1
+
+
+class IoError(Par2Error):
+    status = 1
+
+
+class InvalidSliceSize(Par2Error):
+    status = 2
+
+
+class InvalidFileName(Par2Error):
+    status = 3
+
+
+class NoInputFiles(Par2Error):
+    status = 4
+
+
+class EmptyFile(Par2Error):
+    status = 5
+
+
+class TooManyFiles(Par2Error):
+    status = 6
+
+
+class TooManyRecoveryBlocks(Par2Error):
+    status = 7
+
+
+class TooManyInputBlocks(Par2Error):
+    status = 8
+
+    def __init__(self, msg, count=0, slice_size=0, suggested=0):
+        super().__init__(msg)
+        self.count, self.slice_size, self.suggested = count, slice_size, suggested
+
+
+class InvalidVolumeScheme(Par2Error):
+    status = 9
+
+
+class InvalidArgument(Par2Error):
+    status = 20
+
+
+class CudaError(Par2Error):
+    status = 21
+
+
+class OutOfMemory(Par2Error):
+    status = 22
+
+
+class DeviceTimeout(Par2Error):
+    status = 23
+
+
+_ERRORS = {c.status: c for c in (IoError, InvalidSliceSize, InvalidFileName, NoInputFiles, EmptyFile, TooManyFiles,
+                                 TooManyRecoveryBlocks, TooManyInputBlocks, InvalidVolumeScheme, InvalidArgument,
+                                 CudaError, OutOfMemory, DeviceTimeout)}
+
+
+def _check(status: int) -> None:
+    if status == 0:
+        return
+    msg = (lib().p2g_last_error_message() or b"").decode("utf-8", "replace")
+    cls = _ERRORS.get(status, Par2Error)
+    if cls is TooManyInputBlocks:
+        d = _ffi.p2g_error_detail()
+        lib().p2g_last_error_detail(C.byref(d))
+        raise TooManyInputBlocks(msg, d.count, d.slice_size, d.suggested)
+    raise cls(msg)
+
+
+# ---------------------------------------------------------------------------
+# VolumeScheme (src/creator.rs:111-139) and CreateOptions (:142-173)
+# ---------------------------------------------------------------------------
+class VolumeScheme:
+    kind = 0
+
+    @staticmethod
+    def Single() -> "VolumeScheme":
+        return _Single()
+
+    @staticmethod
+    def Exponential() -> "VolumeScheme":
+        return _Exponential()
+
+    @staticmethod
+    def Uniform(count: int) -> "VolumeScheme":
+        return _Uniform(count)
+
+    @staticmethod
+    def Limited(max_blocks_per_volume: int, inner: "VolumeScheme") -> "VolumeScheme":
+        return _Limited(max_blocks_per_volume, inner)
+
+    @staticmethod
+    def Explicit(sizes: Sequence[int]) -> "VolumeScheme":
+        return _Explicit(list(sizes))
+
+    def _to_c(self, keep: list) -> _ffi.p2g_volume_scheme:
+        s = _ffi.p2g_volume_scheme()
+        s.kind = self.kind
+        s.count = getattr(self, "count", 0)
+        s.max_blocks_per_volume = getattr(self, "max_blocks_per_volume", 0)
+        inner = getattr(self, "inner", None)
+        if inner is not None:
+            ic = inner._to_c(keep)
+            keep.append(ic)
+            s.inner = C.pointer(ic)
+        sizes = getattr(self, "sizes", None)
+        if sizes is not None:
+            arr = (C.c_uint32 * max(len(sizes), 1))(*sizes)
+            keep.append(arr)
+            s.explicit_sizes = arr
+            s.explicit_count = len(sizes)
+        return s
+
+    def __eq__(self, other):
+        return type(self) is type(other) and self.__dict__ == other.__dict__
+
+    def __repr__(self):
+        args = ", ".join(f"{k}={v!r}" for k, v in self.__dict__.items())
+        return f"VolumeScheme.{type(self).__name__.lstrip('_')}({args})"
+
+
+class _Single(VolumeScheme):
+    kind = 0
+
+
+class _Exponential(VolumeScheme):
+    kind = 1
+
+
+class _Uniform(VolumeScheme):
+    kind = 2
+
+    def __init__(self, count):
+        self.count = int(count)
+
+
+class _Limited(VolumeScheme):
+    kind = 3
+
+    def __init__(self, max_blocks_per_volume, inner):
+        self.max_blocks_per_volume = int(max_blocks_per_volume)
+        self.inner = inner
+
+
+class _Explicit(VolumeScheme):
+    kind = 4
+
+    def __init__(self, sizes):
+        self.sizes = [int(x) for x in sizes]
+
+
+@dataclass
+class CreateOptions:
+    output: Union[str, Path] = ""
+    slice_size: int = 4096
+    recovery_block_count: int = 0
+    volume_scheme: VolumeScheme = field(default_factory=VolumeScheme.Single)
+    comments: List[str] = field(default_factory=list)
+
+    def _to_c(self, keep: list) -> _ffi.p2g_create_options:
+        o = _ffi.p2g_create_options()
+        out = os.fsencode(str(self.output))
+        keep.append(out)
+        o.output = out
+        o.slice_size = int(self.slice_size)
+        o.recovery_block_count = int(self.recovery_block_count)
+        o.volume_scheme = self.volume_scheme._to_c(keep)
+        if self.comments:
+            enc = [c.encode("utf-8") for c in self.comments]
+            arr = (C.c_char_p * len(enc))(*enc)
+            keep.extend([enc, arr])
+            o.comments = arr
+            o.comment_count = len(enc)
+        return o
+
+
+# ---------------------------------------------------------------------------
+# Progress (src/progress.rs)
+# ---------------------------------------------------------------------------
+_EVENT_NAMES = ["ScanStarted", "ScanProgress", "ScanCompleted", "EncodeStarted", "EncodeProgress",
+                "EncodeCompleted", "IndexWritten", "VolumeWritten"]
+
+
+@dataclass
+class ProgressEvent:
+    kind: str
+    path: Optional[str] = None
+    total_slices: int = 0
+    slices_done: int = 0
+    volume_index: int = 0
+    total_volumes: int = 0
+    input_blocks: int = 0
+    recovery_blocks: int = 0
+    input_block_done: int = 0
+
+
+class ProgressReporter:
+    """Receiver for progress events (ProgressReporter::on_event)."""
+
+    def on_event(self, event: ProgressEvent) -> None:  # pragma: no cover - interface
+        raise NotImplementedError
+
+
+def _progress_cb(reporter):
+    if reporter is None:
+        return _ffi.PROGRESS_FN(), None
+
+    def cb(evp, _user):
+        e = evp.contents
+        reporter.on_event(ProgressEvent(
+            kind=_EVENT_NAMES[e.kind], path=e.path.decode("utf-8", "replace") if e.path else None,
+            total_slices=e.total_slices, slices_done=e.slices_done, volume_index=e.volume_index,
+            total_volumes=e.total_volumes, input_blocks=e.input_blocks, recovery_blocks=e.recovery_blocks,
+            input_block_done=e.input_block_done))
+
+    f = _ffi.PROGRESS_FN(cb)
+    return f, f
+
+
+# ---------------------------------------------------------------------------
+# SourceFile (src/source.rs:28-136)
+# ---------------------------------------------------------------------------
+@dataclass
+class SliceChecksum:
+    md5: bytes
+    crc32: int
+
+
+@dataclass
+class SourceFile:
+    name: bytes
+    path: Path
+    length: int
+    hash_full: bytes
+    hash16k: bytes
+    file_id: bytes
+    slice_checksums: List[SliceChecksum]
+
+    @staticmethod
+    def scan(path, display_name: bytes, slice_size: int) -> "SourceFile":
+        return SourceFile.scan_with_progress(path, display_name, slice_size, None)
+
+    @staticmethod
+    def scan_with_progress(path, display_name: bytes, slice_size: int,
+                           reporter: Optional[ProgressReporter]) -> "SourceFile":
+        sf = _ffi.p2g_source_file()
+        name = bytes(display_name)
+        nbuf = (C.c_uint8 * max(len(name), 1)).from_buffer_copy(name or b"\0")
+        cb, _keep = _progress_cb(reporter)
+        _check(lib().p2g_scan_with_progress(os.fsencode(str(path)), nbuf, len(name), int(slice_size), cb, None,
+                                            C.byref(sf)))
+        try:
+            return SourceFile._from_c(sf)
+        finally:
+            lib().p2g_source_file_free(C.byref(sf))
+
+    @staticmethod
+    def _from_c(sf: _ffi.p2g_source_file) -> "SourceFile":
+        n = sf.slice_count
+        cks = [SliceChecksum(bytes(sf.slice_checksums[i].md5), int(sf.slice_checksums[i].crc32)) for i in range(n)]
+        return SourceFile(name=C.string_at(sf.name, sf.name_len), path=Path(os.fsdecode(sf.path or b"")),
+                          length=sf.length, hash_full=bytes(sf.hash_full), hash16k=bytes(sf.hash16k),
+                          file_id=bytes(sf.file_id), slice_checksums=cks)
+
+    def _to_c(self, keep: list) -> _ffi.p2g_source_file:
+        sf = _ffi.p2g_source_file()
+        nb = (C.c_uint8 * max(len(self.name), 1)).from_buffer_copy(self.name or b"\0")
+        pb = os.fsencode(str(self.path))
+        arr = (_ffi.p2g_slice_checksum * max(len(self.slice_checksums), 1))()
+        for i, sc in enumerate(self.slice_checksums):
+            arr[i].md5[:] = list(sc.md5)
+            arr[i].crc32 = sc.crc32
+        keep.extend([nb, pb, arr])
+        sf.name = C.cast(nb, C.POINTER(C.c_uint8))
+        sf.name_len = len(self.name)
+        sf.path = pb
+        sf.length = self.length
+        sf.hash_full[:] = list(self.hash_full)
+        sf.hash16k[:] = list(self.hash16k)
+        sf.file_id[:] = list(self.file_id)
+        sf.slice_checksums = C.cast(arr, C.POINTER(_ffi.p2g_slice_checksum))
+        sf.slice_count = len(self.slice_checksums)
+        return sf
+
+
+def _sources_to_c(sources: Sequence[SourceFile], keep: list):
+    arr = (_ffi.p2g_source_file * max(len(sources), 1))()
+    for i, s in enumerate(sources):
+        arr[i] = s._to_c(keep)
+    return arr
+
+
+def _path_list(pl: _ffi.p2g_path_list) -> List[Path]:
+    out = [Path(os.fsdecode(pl.paths[i])) for i in range(pl.count)]
+    lib().p2g_path_list_free(C.byref(pl))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Create entry points (src/creator.rs:182-860)
+# ---------------------------------------------------------------------------
+def run_create(opts: CreateOptions, sources: Sequence[SourceFile]) -> List[Path]:
+    return run_create_with_progress(opts, sources, None)
+
+
+def run_create_with_progress(opts: CreateOptions, sources: Sequence[SourceFile],
+                             reporter: Optional[ProgressReporter]) -> List[Path]:
+    keep: list = []
+    o = opts._to_c(keep)
+    arr = _sources_to_c(sources, keep)
+    pl = _ffi.p2g_path_list()
+    cb, _k = _progress_cb(reporter)
+    _check(lib().p2g_run_create_with_progress(C.byref(o), arr, len(sources), cb, None, C.byref(pl)))
+    return _path_list(pl)
+
+
+def run_create_fused(opts: CreateOptions, inputs: Sequence[Tuple[Union[str, Path], bytes]],
+                     reporter: Optional[ProgressReporter] = None) -> List[Path]:
+    keep: list = []
+    o = opts._to_c(keep)
+    arr = (_ffi.p2g_input * max(len(inputs), 1))()
+    for i, (p, name) in enumerate(inputs):
+        pb = os.fsencode(str(p))
+        nb = (C.c_uint8 * max(len(name), 1)).from_buffer_copy(bytes(name) or b"\0")
+        keep.extend([pb, nb])
+        arr[i].path = pb
+        arr[i].display_name = C.cast(nb, C.POINTER(C.c_uint8))
+        arr[i].name_len = len(name)
+    pl = _ffi.p2g_path_list()
+    cb, _k = _progress_cb(reporter)
+    _check(lib().p2g_run_create_fused(C.byref(o), arr, len(inputs), cb, None, C.byref(pl)))
+    return _path_list(pl)
+
+
+def write_index_file(opts: CreateOptions, sources: Sequence[SourceFile]) -> Path:
+    keep: list = []
+    o = opts._to_c(keep)
+    arr = _sources_to_c(sources, keep)
+    out = C.c_void_p()
+    _check(lib().p2g_write_index_file(C.byref(o), arr, len(sources), C.byref(out)))
+    p = C.string_at(out.value)
+    lib().p2g_string_free(out)
+    return Path(os.fsdecode(p))
+
+
+def create_in_memory(opts: CreateOptions, inputs: Sequence[Tuple[bytes, object]],
+                     return_sources: bool = False):
+    """run_create_fused without a filesystem.
+
+    ``inputs`` are (display_name, data) pairs; data is any buffer (bytes,
+    numpy array, pinned torch tensor, ...).  Returns a list of
+    (file_name, bytes) for the index and each volume, plus the scanned
+    SourceFile records when ``return_sources``.
+    """
+    keep: list = []
+    o = opts._to_c(keep)
+    arr = (_ffi.p2g_buffer_input * max(len(inputs), 1))()
+    for i, (name, data) in enumerate(inputs):
+        ptr, length = _host_buffer(data, keep)
+        nb = (C.c_uint8 * max(len(name), 1)).from_buffer_copy(bytes(name) or b"\0")
+        keep.append(nb)
+        arr[i].data = ptr
+        arr[i].length = length
+        arr[i].display_name = C.cast(nb, C.POINTER(C.c_uint8))
+        arr[i].name_len = len(name)
+    srcs = (_ffi.p2g_source_file * max(len(inputs), 1))() if return_sources else None
+    os_ = _ffi.p2g_output_set()
+    _check(lib().p2g_create_in_memory(C.byref(o), arr, len(inputs), srcs, C.byref(os_)))
+    files = []
+    for i in range(os_.count):
+        f = os_.files[i]
+        files.append((os.fsdecode(f.name), C.string_at(f.data, f.length)))
+    lib().p2g_output_set_free(C.byref(os_))
+    if not return_sources:
+        return files
+    out_src = []
+    for i in range(len(inputs)):
+        out_src.append(SourceFile._from_c(srcs[i]))
+        lib().p2g_source_file_free(C.byref(srcs[i]))
+    return files, out_src
+
+
+def _host_buffer(data, keep: list) -> Tuple[int, int]:
+    """(address, length) of a host buffer without copying when possible."""
+    if hasattr(data, "data_ptr") and hasattr(data, "is_cuda"):  # torch tensor (CPU)
+        if data.is_cuda:
+            raise InvalidArgument("expected a host tensor")
+        t = data.contiguous()
+        keep.append(t)
+        return t.data_ptr(), t.numel() * t.element_size()
+    import numpy as np
+
+    a = np.frombuffer(data, dtype=np.uint8) if not isinstance(data, np.ndarray) else data
+    a = np.ascontiguousarray(a).view(np.uint8).reshape(-1)
+    keep.append(a)
+    return a.ctypes.data, a.nbytes
+
+
+# ---------------------------------------------------------------------------
+# Kernel-level seams
+# ---------------------------------------------------------------------------
+def gf_mul_xor(coeff: int, input: bytes, output: bytearray) -> None:
+    """output ^= coeff * input over LE GF(2^16) symbols (gf_mul_xor_dispatch)."""
+    import numpy as np
+
+    inp = np.frombuffer(bytes(input), dtype=np.uint8)
+    out = np.frombuffer(output, dtype=np.uint8)
+    _check(lib().p2g_gf_mul_xor(int(coeff), inp.ctypes.data, out.ctypes.data, len(inp), HOST_POINTERS, None))
+
+
+def encode(src, slice_size: int, recovery_count: int, first_exponent: int = 0, input_count: Optional[int] = None):
+    """encode_all_recovery_blocks over host memory: src holds input_count
+    zero-padded slices back to back; returns recovery bytes (R*slice)."""
+    import numpy as np
+
+    a = np.ascontiguousarray(np.frombuffer(src, dtype=np.uint8) if not isinstance(src, np.ndarray) else src)
+    a = a.view(np.uint8).reshape(-1)
+    S = input_count if input_count is not None else a.nbytes // slice_size
+    out = np.zeros(recovery_count * slice_size, dtype=np.uint8)
+    job = _ffi.p2g_encode_job(src=a.ctypes.data, src_stride=slice_size, input_count=S, slice_size=slice_size,
+                              recovery_count=recovery_count, first_exponent=first_exponent,
+                              recovery=out.ctypes.data, recovery_stride=slice_size, flags=HOST_POINTERS, stream=None)
+    _check(lib().p2g_encode(C.byref(job)))
+    return out
+
+
+def encode_device(src_ptr: int, src_stride: int, input_count: int, slice_size: int, recovery_count: int,
+                  rec_ptr: int, rec_stride: int, stream: int = 0, first_exponent: int = 0) -> None:
+    job = _ffi.p2g_encode_job(src=src_ptr, src_stride=src_stride, input_count=input_count, slice_size=slice_size,
+                              recovery_count=recovery_count, first_exponent=first_exponent, recovery=rec_ptr,
+                              recovery_stride=rec_stride, flags=DEVICE_POINTERS, stream=stream or None)
+    _check(lib().p2g_encode(C.byref(job)))
+
+
+def slice_checksums(src, slice_size: int, count: Optional[int] = None) -> List[SliceChecksum]:
+    import numpy as np
+
+    a = np.ascontiguousarray(np.frombuffer(src, dtype=np.uint8) if not isinstance(src, np.ndarray) else src)
+    n = count if count is not None else a.nbytes // slice_size
+    out = (_ffi.p2g_slice_checksum * max(n, 1))()
+    _check(lib().p2g_slice_checksums(a.ctypes.data, slice_size, n, slice_size, C.addressof(out), HOST_POINTERS, None))
+    return [SliceChecksum(bytes(out[i].md5), int(out[i].crc32)) for i in range(n)]
+
+
+def file_hashes(buffers: Sequence[bytes]) -> List[Tuple[bytes, bytes]]:
+    """(hash_full, hash16k) per buffer, computed on the device."""
+    import numpy as np
+
+    arrs = [np.frombuffer(bytes(b) + b"\0" * 4, dtype=np.uint8) for b in buffers]
+    n = len(arrs)
+    ptrs = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in arrs])
+    lens = (C.c_uint64 * max(n, 1))(*[len(b) for b in buffers])
+    hf = (C.c_uint8 * (16 * max(n, 1)))()
+    h16 = (C.c_uint8 * (16 * max(n, 1)))()
+    _check(lib().p2g_file_hashes(ptrs, lens, n, C.addressof(hf), C.addressof(h16), HOST_POINTERS, None))
+    return [(bytes(hf[16 * i:16 * i + 16]), bytes(h16[16 * i:16 * i + 16])) for i in range(n)]
+
+
+def recovery_packet_md5(set_id: bytes, recovery, slice_size: int, count: int, first_exponent: int = 0) -> List[bytes]:
+    import numpy as np
+
+    a = np.ascontiguousarray(np.frombuffer(recovery, dtype=np.uint8) if not isinstance(recovery, np.ndarray) else recovery)
+    out = (C.c_uint8 * (16 * max(count, 1)))()
+    _check(lib().p2g_recovery_packet_md5(bytes(set_id), a.ctypes.data, slice_size, count, slice_size, first_exponent,
+                                         C.addressof(out), HOST_POINTERS, None))
+    return [bytes(out[16 * i:16 * i + 16]) for i in range(count)]
+
+
+class DeviceJobBuffers:
+    """Device outputs of one create job (torch uint8 CUDA tensors)."""
+
+    def __init__(self, S: int, n_files: int, slice_size: int, recovery_count: int, device):
+        import torch
+
+        self.rec_stride = (slice_size + 15) // 16 * 16
+        self.recovery = torch.empty(max(recovery_count, 1) * self.rec_stride, dtype=torch.uint8, device=device)
+        self.checksums = torch.empty(max(S, 1) * 20, dtype=torch.uint8, device=device)
+        self.hash_full = torch.empty(max(n_files, 1) * 16, dtype=torch.uint8, device=device)
+        self.hash16k = torch.empty(max(n_files, 1) * 16, dtype=torch.uint8, device=device)
+        self.packet_md5 = torch.empty(max(recovery_count, 1) * 16, dtype=torch.uint8, device=device)
+        self.set_id = b""
+
+
+def run_device_job(src, file_lengths: Sequence[int], names: Sequence[bytes], slice_size: int, recovery_count: int,
+                   bufs: Optional[DeviceJobBuffers] = None, stream: Optional[int] = None,
+                   skip_hash_full: bool = False) -> DeviceJobBuffers:
+    """The device work of one create job over a device-resident source.
+
+    ``src`` is a CUDA uint8 tensor holding the files back to back, each
+    starting on a slice boundary and zero-padded to whole slices.  Work is
+    ordered on ``stream`` (default: torch's current stream).
+    """
+    import torch
+
+    S = sum((n + slice_size - 1) // slice_size for n in file_lengths)
+    if bufs is None:
+        bufs = DeviceJobBuffers(S, len(file_lengths), slice_size, recovery_count, src.device)
+    if stream is None:
+        stream = torch.cuda.current_stream(src.device).cuda_stream
+    n = len(file_lengths)
+    lens = (C.c_uint64 * max(n, 1))(*file_lengths)
+    nbufs = [C.create_string_buffer(bytes(x), len(x)) for x in names]
+    nptrs = (C.c_void_p * max(n, 1))(*[C.addressof(b) for b in nbufs])
+    nlens = (C.c_size_t * max(n, 1))(*[len(x) for x in names])
+    job = _ffi.p2g_device_job()
+    job.src = src.data_ptr()
+    job.file_count = n
+    job.file_lengths = lens
+    job.names = nptrs
+    job.name_lens = nlens
+    job.slice_size = slice_size
+    job.recovery_count = recovery_count
+    job.recovery = bufs.recovery.data_ptr()
+    job.recovery_stride = bufs.rec_stride
+    job.checksums = bufs.checksums.data_ptr()
+    job.hash_full = bufs.hash_full.data_ptr()
+    job.hash16k = bufs.hash16k.data_ptr()
+    job.packet_md5 = bufs.packet_md5.data_ptr()
+    job.flags = JOB_SKIP_HASH_FULL if skip_hash_full else 0
+    job.stream = stream
+    _check(lib().p2g_run_device_job(C.byref(job)))
+    bufs.set_id = bytes(job.set_id_out)
+    return bufs
+
+
+# ---------------------------------------------------------------------------
+# Host helpers of the reference's public modules
+# ---------------------------------------------------------------------------
+def input_bases(count: int) -> List[int]:
+    arr = (C.c_uint16 * max(count, 1))()
+    _check(lib().p2g_input_bases(count, arr))
+    return list(arr[:count])
+
+
+def gf_mul(a: int, b: int) -> int:
+    return lib().p2g_gf_mul(a, b)
+
+
+def gf_pow(base: int, exp: int) -> int:
+    return lib().p2g_gf_pow(base, exp)
+
+
+def resolve_volume_sizes(scheme: VolumeScheme, total: int) -> List[int]:
+    keep: list = []
+    sc = scheme._to_c(keep)
+    n = C.c_uint32()
+    _check(lib().p2g_resolve_volume_sizes(C.byref(sc), total, None, 0, C.byref(n)))
+    out = (C.c_uint32 * max(n.value, 1))()
+    _check(lib().p2g_resolve_volume_sizes(C.byref(sc), total, out, n.value, C.byref(n)))
+    return list(out[:n.value])
+
+
+def volume_filename(index_path, first_exponent: int, count: int) -> str:
+    p = lib().p2g_volume_filename(os.fsencode(str(index_path)), first_exponent, count)
+    s = C.string_at(p)
+    lib().p2g_string_free(p)
+    return os.fsdecode(s)
+
+
+def build_packet(set_id: bytes, type_tag: bytes, body: bytes) -> bytes:
+    n = lib().p2g_build_packet(set_id, type_tag, body, len(body), None)
+    out = (C.c_uint8 * n)()
+    lib().p2g_build_packet(set_id, type_tag, body, len(body), C.addressof(out))
+    return bytes(out)
+
+
+def build_main_packet(slice_size: int, file_ids: Sequence[bytes]) -> Tuple[bytes, bytes]:
+    """(packet bytes, set_id)"""
+    ids = b"".join(file_ids)
+    sid = (C.c_uint8 * 16)()
+    n = lib().p2g_build_main_packet(slice_size, ids, len(file_ids), None, None)
+    out = (C.c_uint8 * n)()
+    lib().p2g_build_main_packet(slice_size, ids, len(file_ids), C.addressof(sid), C.addressof(out))
+    return bytes(out), bytes(sid)
+
+
+def compute_file_id(hash16k: bytes, length: int, name: bytes) -> bytes:
+    out = (C.c_uint8 * 16)()
+    lib().p2g_compute_file_id(hash16k, length, name, len(name), C.addressof(out))
+    return bytes(out)
+
+
+def md5(data: bytes) -> bytes:
+    out = (C.c_uint8 * 16)()
+    lib().p2g_md5(data, len(data), C.addressof(out))
+    return bytes(out)
+
+
+def kernel_launch_count() -> int:
+    return int(lib().p2g_kernel_launch_count())
+
+
+def device_info() -> str:
+    buf = C.create_string_buffer(256)
+    _check(lib().p2g_device_info(buf, 256))
+    return buf.value.decode()
+
+
+__all__ = [
+    "MAX_FILES", "MAX_INPUT_BLOCKS", "MAX_RECOVERY_BLOCKS", "HASH16K_LEN", "Par2Error", "IoError", "InvalidSliceSize",
+    "InvalidFileName", "NoInputFiles", "EmptyFile", "TooManyFiles", "TooManyRecoveryBlocks", "TooManyInputBlocks",
+    "InvalidVolumeScheme", "InvalidArgument", "CudaError", "OutOfMemory", "DeviceTimeout", "VolumeScheme",
+    "CreateOptions", "ProgressEvent", "ProgressReporter", "SliceChecksum", "SourceFile", "run_create",
+    "run_create_with_progress", "run_create_fused", "write_index_file", "create_in_memory", "gf_mul_xor", "encode",
+    "encode_device", "slice_checksums", "file_hashes", "recovery_packet_md5", "input_bases", "gf_mul", "gf_pow",
+    "resolve_volume_sizes", "volume_filename", "build_packet", "build_main_packet", "compute_file_id", "md5",
+    "kernel_launch_count", "device_info", "DeviceJobBuffers", "run_device_job",
+]

@@ -1,0 +1,1196 @@
+// p2g_engine.cpp -- device context, hot-path seams and the create pipeline
+// of libpar2gpu.so (the C ABI declared in include/par2gpu.h).
+//
+// Device data layout for one create job:
+//   src      the input files back to back in caller order, each starting on a
+//            slice boundary and zero-padded to whole slices: input slice s is
+//            src + s*slice_size (the global input index of
+//            src/creator.rs:895-900 / :757-775).
+//   rec      recovery row r (exponent first_exp + r) at rec + r*rec_stride,
+//            rec_stride = slice_size rounded up to 16 bytes.
+//   basis    [s][row group][16][32] u16 coefficient-basis scratch.
+//   checks   one 20-byte IFSC record (md5 ‖ crc32) per input slice.
+#include <cuda_runtime.h>
+#include <errno.h>
+#include <fcntl.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <atomic>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "p2g_host_util.h"
+#include "p2g_internal.h"
+
+namespace p2g {
+
+static p2g_status cuda_fail(cudaError_t e, const char* what) {
+    cudaGetLastError();  // clear a sticky-free error so later calls can proceed
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(P2G_ERR_OOM, "device allocation failed: %s (%s)", cudaGetErrorString(e), what);
+    return set_error(P2G_ERR_CUDA, "CUDA error: %s (%s)", cudaGetErrorString(e), what);
+}
+#define P2G_CU(call)                                            \
+    do {                                                        \
+        cudaError_t _e = (call);                                \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call);     \
+    } while (0)
+#define P2G_TRY(expr)                       \
+    do {                                    \
+        p2g_status _s = (expr);             \
+        if (_s != P2G_OK) return _s;        \
+    } while (0)
+
+static inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = std::max<size_t>(round_up(n, 1 << 20), 1 << 20);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+// Grow-only pinned host buffer.
+struct PinBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = std::max<size_t>(round_up(n, 1 << 16), 1 << 16);
+        cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// One per process.  Calls are serialised on `mu`; the device is the one
+// current on the first calling thread (or P2G_DEVICE).
+struct Context {
+    std::recursive_mutex mu;
+    int device = -1;
+    bool ready = false;
+    cudaStream_t st[5] = {};
+    cudaEvent_t ev_fork = nullptr, ev_h16k = nullptr, ev_join[5] = {};
+    DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out;
+    PinBuf h_spans, h_h16k, h_err, h_stage;
+};
+static Context& ctx() {
+    static Context* c = new Context();  // never destroyed: the CUDA runtime may be gone at exit
+    return *c;
+}
+
+static p2g_status ensure_ready(Context& c) {
+    if (!c.ready) {
+        int dev = 0;
+        if (const char* e = getenv("P2G_DEVICE")) dev = atoi(e);
+        else if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n == 0)
+            return set_error(P2G_ERR_CUDA, "no CUDA device available (%s)",
+                             e != cudaSuccess ? cudaGetErrorString(e) : "device count 0");
+        if (dev >= n) dev = 0;
+        P2G_CU(cudaSetDevice(dev));
+        cudaDeviceProp prop;
+        P2G_CU(cudaGetDeviceProperties(&prop, dev));
+        if (prop.major < 10)
+            return set_error(P2G_ERR_CUDA, "device %d (%s, sm_%d%d) is not sm_100: this build targets B200 only", dev,
+                             prop.name, prop.major, prop.minor);
+        for (auto& s : c.st) P2G_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        P2G_CU(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
+        P2G_CU(cudaEventCreateWithFlags(&c.ev_h16k, cudaEventDisableTiming));
+        for (auto& ev : c.ev_join) P2G_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        P2G_CU(upload_tables());
+        P2G_CU(c.err.ensure(64));
+        P2G_CU(c.h_err.ensure(64));
+        c.device = dev;
+        c.ready = true;
+    }
+    P2G_CU(cudaSetDevice(c.device));
+    return P2G_OK;
+}
+
+// Fork the side streams off `caller`, join them back.
+static p2g_status fork_from(Context& c, cudaStream_t caller) {
+    P2G_CU(cudaEventRecord(c.ev_fork, caller));
+    for (auto& s : c.st) P2G_CU(cudaStreamWaitEvent(s, c.ev_fork, 0));
+    return P2G_OK;
+}
+static p2g_status join_into(Context& c, cudaStream_t caller) {
+    for (int i = 0; i < 5; ++i) {
+        P2G_CU(cudaEventRecord(c.ev_join[i], c.st[i]));
+        P2G_CU(cudaStreamWaitEvent(caller, c.ev_join[i], 0));
+    }
+    return P2G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Whole-file MD5 placement.  A file hash is one serial MD5 chain: on the
+// device each chain runs on one thread; on the host on one core.  AUTO picks
+// the side with the smaller estimated finish time from measured chain rates
+// (overridable with P2G_FILE_HASH=device|host).
+// ---------------------------------------------------------------------------
+enum class FileHashMode { Device, Host };
+static double env_double(const char* name, double dflt) {
+    const char* e = getenv(name);
+    return e ? atof(e) : dflt;
+}
+static FileHashMode choose_file_hash_mode(const std::vector<uint64_t>& lens) {
+    if (const char* e = getenv("P2G_FILE_HASH")) {
+        if (!strcmp(e, "device")) return FileHashMode::Device;
+        if (!strcmp(e, "host")) return FileHashMode::Host;
+    }
+    // chain rates in bytes/s: one device thread, one host core
+    const double dev_rate = env_double("P2G_DEVICE_MD5_RATE", 1.2e8);
+    const double host_rate = env_double("P2G_HOST_MD5_RATE", 6.0e8);
+    uint64_t mx = 0, total = 0;
+    for (uint64_t l : lens) {
+        mx = std::max(mx, l);
+        total += l;
+    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const double t_dev = (double)mx / dev_rate;
+    const double t_host = std::max((double)mx / host_rate, (double)total / (host_rate * hw));
+    return t_host < t_dev ? FileHashMode::Host : FileHashMode::Device;
+}
+
+// Host-side whole-file MD5 of several buffers on a small thread pool.
+struct HostHasher {
+    std::vector<std::thread> th;
+    void start(const std::vector<const uint8_t*>& data, const std::vector<uint64_t>& lens, std::vector<Md5>& out) {
+        out.resize(data.size());
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const unsigned nt = (unsigned)std::min<size_t>(hw, data.size());
+        auto next = std::make_shared<std::atomic<size_t>>(0);
+        for (unsigned t = 0; t < nt; ++t)
+            th.emplace_back([&data, &lens, &out, next]() {
+                for (size_t i = (*next)++; i < data.size(); i = (*next)++) out[i] = md5_of(data[i], lens[i]);
+            });
+    }
+    void join() {
+        for (auto& t : th) t.join();
+        th.clear();
+    }
+    ~HostHasher() { join(); }
+};
+
+// ---------------------------------------------------------------------------
+// Device job: everything between "source resident in HBM" and "recovery rows,
+// checksums, file hashes and packet MD5s in HBM".
+// ---------------------------------------------------------------------------
+struct JobFile {
+    uint64_t length;
+    uint64_t first_slice;
+    uint64_t slices;
+    const uint8_t* name;
+    size_t name_len;
+};
+struct DeviceJob {
+    const uint8_t* d_src = nullptr;
+    uint32_t S = 0;
+    uint64_t slice = 0;
+    uint32_t R = 0;
+    uint32_t first_exp = 0;
+    std::vector<JobFile> files;
+    uint8_t* d_rec = nullptr;
+    uint64_t rec_stride = 0;
+    p2g_slice_checksum* d_checks = nullptr;  // null: skip slice checksums
+    uint8_t* d_h16k = nullptr;
+    uint8_t* d_hfull = nullptr;  // null: hash_full not on the device
+    uint8_t* d_pkt = nullptr;    // null: skip packet MD5
+    // filled
+    std::vector<Md5> h16k, file_ids;
+    Md5 set_id{};
+    // set instead of computing from hash16k (run_create with scanned sources)
+    bool have_set_id = false;
+};
+
+static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) {
+    const uint32_t n = (uint32_t)j.files.size();
+    const uint32_t RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
+    P2G_TRY(fork_from(c, caller));
+    cudaStream_t s_enc = c.st[0], s_files = c.st[1], s_md5 = c.st[2], s_crc = c.st[3], s_full = c.st[4];
+    P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s_enc));
+
+    // per-file spans: [0, n) hash16k spans, [n, 2n) hash_full spans
+    const bool need_files = j.d_h16k && n > 0;
+    if (need_files) {
+        P2G_CU(c.h_spans.ensure(sizeof(FileSpan) * 2 * n));
+        P2G_CU(c.spans.ensure(sizeof(FileSpan) * 2 * n));
+        FileSpan* hs = c.h_spans.as<FileSpan>();
+        for (uint32_t f = 0; f < n; ++f) {
+            hs[f] = {j.files[f].first_slice * j.slice, std::min<uint64_t>(j.files[f].length, P2G_HASH16K_LEN)};
+            hs[n + f] = {j.files[f].first_slice * j.slice, j.files[f].length};
+        }
+        P2G_CU(cudaMemcpyAsync(c.spans.p, hs, sizeof(FileSpan) * 2 * n, cudaMemcpyHostToDevice, s_files));
+        P2G_CU(launch_md5_files(j.d_src, c.spans.as<FileSpan>(), n, j.d_h16k, s_files));
+        if (!j.have_set_id) {
+            P2G_CU(c.h_h16k.ensure(16 * n));
+            P2G_CU(cudaMemcpyAsync(c.h_h16k.p, j.d_h16k, 16 * n, cudaMemcpyDeviceToHost, s_files));
+        }
+        P2G_CU(cudaEventRecord(c.ev_h16k, s_files));
+        if (j.d_hfull) {
+            P2G_CU(cudaStreamWaitEvent(s_full, c.ev_h16k, 0));  // spans uploaded
+            P2G_CU(launch_md5_files(j.d_src, c.spans.as<FileSpan>() + n, n, j.d_hfull, s_full));
+        }
+    }
+    if (j.d_checks && j.S) {
+        P2G_CU(launch_md5_slices(j.d_src, j.slice, j.S, j.slice, j.d_checks, s_md5));
+        P2G_CU(launch_crc_slices(j.d_src, j.slice, j.S, j.slice, j.d_checks, s_crc));
+    }
+    if (j.R && j.S) {
+        P2G_CU(c.basis.ensure(basis_bytes(j.S, RG)));
+        P2G_CU(launch_basis(c.basis.as<uint16_t>(), j.S, RG, j.R, j.first_exp, s_enc));
+        const uint8_t* esrc = j.d_src;
+        uint64_t estride = j.slice;
+        if (j.slice % 16) {  // the TMA tile loads need 16-byte aligned slice starts
+            estride = round_up(j.slice, 16);
+            P2G_CU(c.src_al.ensure((size_t)estride * j.S));
+            P2G_CU(launch_realign(j.d_src, j.slice, c.src_al.as<uint8_t>(), estride, j.S, j.slice, s_enc));
+            esrc = c.src_al.as<uint8_t>();
+        }
+        P2G_CU(launch_encode(esrc, estride, j.S, c.basis.as<uint16_t>(), RG, j.R, j.slice, j.d_rec, j.rec_stride,
+                             c.err.as<int>(), s_enc));
+    }
+    if (!j.have_set_id) {
+        // set id = MD5(main packet body) over the sorted file ids
+        // (src/source.rs:303-309, src/packet/main_packet.rs:25-42)
+        P2G_CU(cudaEventSynchronize(c.ev_h16k));
+        j.h16k.resize(n);
+        j.file_ids.resize(n);
+        for (uint32_t f = 0; f < n; ++f) {
+            memcpy(j.h16k[f].data(), c.h_h16k.as<uint8_t>() + 16 * f, 16);
+            j.file_ids[f] = file_id_of(j.h16k[f].data(), j.files[f].length, j.files[f].name, j.files[f].name_len);
+        }
+        std::vector<uint8_t> mp;
+        j.set_id = build_main_packet(j.slice, j.file_ids, mp);
+    }
+    if (j.R && j.d_pkt)
+        P2G_CU(launch_md5_recovery(j.d_rec, j.rec_stride, j.R, j.slice, j.set_id.data(), j.first_exp, j.d_pkt, s_enc));
+    P2G_CU(cudaMemcpyAsync(c.h_err.p, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, s_enc));
+    P2G_TRY(join_into(c, caller));
+    return P2G_OK;
+}
+
+static p2g_status check_device_error(Context& c) {
+    if (*c.h_err.as<int>() != 0)
+        return set_error(P2G_ERR_TIMEOUT, "a bounded device wait gave up (TMA stage never completed)");
+    return P2G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Validation shared by the create entry points (src/creator.rs:193-218,
+// :461-508, src/source.rs:65-75).
+// ---------------------------------------------------------------------------
+static p2g_status check_common(uint32_t n, uint32_t R, uint64_t slice) {
+    if (n == 0) return set_error(P2G_ERR_NO_INPUT_FILES, "no input files supplied");
+    if (n > P2G_MAX_FILES)
+        return set_error(P2G_ERR_TOO_MANY_FILES, "too many input files (%u); PAR2 limit is 32768", n);
+    if (R > P2G_MAX_RECOVERY_BLOCKS)
+        return set_error(P2G_ERR_TOO_MANY_RECOVERY_BLOCKS, "recovery block count %u exceeds PAR2 limit of 65535", R);
+    if (slice == 0 || slice % 4)
+        return set_error(P2G_ERR_INVALID_SLICE_SIZE, "invalid slice size %llu: must be > 0 and a multiple of 4",
+                         (unsigned long long)slice);
+    return P2G_OK;
+}
+static p2g_status check_name(const uint8_t* name, size_t len, const char* path) {
+    if (len == 0 || !name || memchr(name, 0, len))
+        return set_error(P2G_ERR_INVALID_FILE_NAME,
+                         "filename \"%s\" is empty or contains a NUL byte; PAR2 does not permit either",
+                         path ? path : "");
+    return P2G_OK;
+}
+static p2g_status check_total_blocks(uint64_t total_blocks, uint64_t total_bytes, uint64_t slice) {
+    if (total_blocks > P2G_MAX_INPUT_BLOCKS) {
+        const uint64_t raw = (total_bytes + P2G_MAX_INPUT_BLOCKS - 1) / P2G_MAX_INPUT_BLOCKS;
+        const uint64_t suggested = (raw + 3) / 4 * 4;
+        set_error_detail(total_blocks, slice, suggested);
+        return set_error(P2G_ERR_TOO_MANY_INPUT_BLOCKS,
+                         "too many input blocks (%llu) at slice_size %llu; PAR2 caps total slices at 32768 — retry "
+                         "with slice_size >= %llu",
+                         (unsigned long long)total_blocks, (unsigned long long)slice, (unsigned long long)suggested);
+    }
+    return P2G_OK;
+}
+
+static void emit(p2g_progress_fn cb, void* user, p2g_progress_event ev) {
+    if (cb) cb(&ev, user);
+}
+static p2g_progress_event mk(uint32_t kind) {
+    p2g_progress_event e;
+    memset(&e, 0, sizeof e);
+    e.kind = kind;
+    return e;
+}
+
+// ---------------------------------------------------------------------------
+// File reading into pinned host memory
+// ---------------------------------------------------------------------------
+struct HostFile {
+    std::string path;
+    uint64_t length = 0;
+    uint8_t* data = nullptr;  // pinned
+    ~HostFile() {
+        if (data) cudaFreeHost(data);
+    }
+};
+static p2g_status stat_len(const char* path, uint64_t* len) {
+    struct stat sb;
+    if (stat(path, &sb) != 0) return set_error(P2G_ERR_IO, "I/O error: %s: %s", path, strerror(errno));
+    *len = (uint64_t)sb.st_size;
+    return P2G_OK;
+}
+static p2g_status read_file(HostFile& hf, uint64_t max_bytes) {
+    const int fd = open(hf.path.c_str(), O_RDONLY | O_CLOEXEC);
+    if (fd < 0) return set_error(P2G_ERR_IO, "I/O error: %s: %s", hf.path.c_str(), strerror(errno));
+    struct stat sb;
+    fstat(fd, &sb);
+    hf.length = std::min<uint64_t>((uint64_t)sb.st_size, max_bytes);
+    if (cudaHostAlloc((void**)&hf.data, std::max<uint64_t>(hf.length, 1), cudaHostAllocDefault) != cudaSuccess) {
+        close(fd);
+        cudaGetLastError();
+        return set_error(P2G_ERR_OOM, "pinned host allocation of %llu bytes failed", (unsigned long long)hf.length);
+    }
+    uint64_t got = 0;
+    while (got < hf.length) {
+        const ssize_t r = read(fd, hf.data + got, std::min<uint64_t>(hf.length - got, 1u << 30));
+        if (r < 0) {
+            if (errno == EINTR) continue;
+            const int e = errno;
+            close(fd);
+            return set_error(P2G_ERR_IO, "I/O error: %s: %s", hf.path.c_str(), strerror(e));
+        }
+        if (r == 0) break;
+        got += (uint64_t)r;
+    }
+    hf.length = got;
+    close(fd);
+    return P2G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Core in-memory create: upload, device job, download, packet assembly.
+// ---------------------------------------------------------------------------
+struct CreateInput {
+    const uint8_t* data;  // host
+    uint64_t length;
+    const uint8_t* name;
+    size_t name_len;
+    const char* path;  // for messages / events
+};
+struct CreateOutput {
+    std::vector<uint8_t> critical;
+    Md5 set_id;
+    std::vector<uint32_t> vol_sizes;
+    uint8_t* rec_host = nullptr;  // pinned, R*slice
+    std::vector<uint8_t> pkt_md5;  // 16*R
+    std::vector<p2g_source_file> sources;  // scanned records (owned here until handed out)
+};
+
+static void free_source(p2g_source_file& sf) {
+    free(sf.name);
+    free(sf.path);
+    free(sf.slice_checksums);
+    memset(&sf, 0, sizeof sf);
+}
+
+// Builds the critical packet block of run_create_with_progress
+// (src/creator.rs:219-235).
+static Md5 critical_packets(uint64_t slice, const p2g_source_file* src, uint32_t n, const char* const* comments,
+                            uint32_t n_comments, std::vector<uint8_t>& out) {
+    std::vector<Md5> ids(n);
+    for (uint32_t f = 0; f < n; ++f) memcpy(ids[f].data(), src[f].file_id, 16);
+    out.clear();
+    const Md5 set_id = build_main_packet(slice, ids, out);
+    for (uint32_t f = 0; f < n; ++f) {
+        append_file_desc(out, set_id, ids[f], src[f].hash_full, src[f].hash16k, src[f].length, src[f].name,
+                         src[f].name_len);
+        append_file_verify(out, set_id, ids[f], src[f].slice_checksums, src[f].slice_count);
+    }
+    append_creator(out, set_id);
+    for (uint32_t i = 0; i < n_comments; ++i) append_comments(out, set_id, comments[i]);
+    return set_id;
+}
+
+struct PinnedRec {
+    uint8_t* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaHostAlloc((void**)&p, std::max<size_t>(n, 1), cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = n;
+        return e;
+    }
+    ~PinnedRec() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+// Scan (+ encode when R > 0) n in-memory inputs on the device.
+// `src_known` (optional): already-scanned SourceFile records; then only the
+// encode and the packet MD5s run and the critical packets use them.
+static p2g_status device_create(Context& c, const CreateInput* in, uint32_t n, uint64_t slice, uint32_t R,
+                                const p2g_source_file* src_known, const char* const* comments, uint32_t n_comments,
+                                CreateOutput& out, PinnedRec& rec_host) {
+    std::vector<JobFile> files(n);
+    uint64_t S = 0;
+    for (uint32_t f = 0; f < n; ++f) {
+        const uint64_t slices = src_known ? src_known[f].slice_count : (in[f].length + slice - 1) / slice;
+        files[f] = {in[f].length, S, slices, in[f].name, in[f].name_len};
+        S += slices;
+    }
+    const uint64_t rec_stride = round_up(slice, 16);
+    const size_t src_bytes = (size_t)S * slice;
+    P2G_CU(c.src.ensure(src_bytes));
+    if (R) {
+        P2G_CU(c.rec.ensure((size_t)R * rec_stride));
+        P2G_CU(c.pkt.ensure(16 * (size_t)R));
+    }
+    if (!src_known) {
+        P2G_CU(c.checks.ensure(sizeof(p2g_slice_checksum) * std::max<uint64_t>(S, 1)));
+        P2G_CU(c.hfull.ensure(16 * (size_t)n));
+    }
+    P2G_CU(c.h16k.ensure(16 * (size_t)n));
+
+    // Whole-file MD5 placement and host-side hashing in the background.
+    std::vector<uint64_t> lens(n);
+    std::vector<const uint8_t*> ptrs(n);
+    for (uint32_t f = 0; f < n; ++f) {
+        lens[f] = in[f].length;
+        ptrs[f] = in[f].data;
+    }
+    const FileHashMode fmode = src_known ? FileHashMode::Host : choose_file_hash_mode(lens);
+    std::vector<Md5> host_full;  // declared before the hasher: its threads write here until joined
+    HostHasher hh;
+    if (!src_known && fmode == FileHashMode::Host) hh.start(ptrs, lens, host_full);
+
+    // Upload: each file to its first slice, zero the tail of its last slice.
+    cudaStream_t up = c.st[0];
+    for (uint32_t f = 0; f < n; ++f) {
+        uint8_t* dst = c.src.as<uint8_t>() + files[f].first_slice * slice;
+        const uint64_t cap = files[f].slices * slice;
+        const uint64_t cp = std::min(in[f].length, cap);
+        if (cp) P2G_CU(cudaMemcpyAsync(dst, in[f].data, cp, cudaMemcpyHostToDevice, up));
+        if (cap > cp) P2G_CU(cudaMemsetAsync(dst + cp, 0, cap - cp, up));
+    }
+    P2G_CU(cudaStreamSynchronize(up));
+
+    DeviceJob j;
+    j.d_src = c.src.as<uint8_t>();
+    j.S = (uint32_t)S;
+    j.slice = slice;
+    j.R = R;
+    j.first_exp = 0;
+    j.files = files;
+    j.d_rec = c.rec.as<uint8_t>();
+    j.rec_stride = rec_stride;
+    j.d_checks = src_known ? nullptr : c.checks.as<p2g_slice_checksum>();
+    j.d_h16k = src_known ? nullptr : c.h16k.as<uint8_t>();
+    j.d_hfull = (!src_known && fmode == FileHashMode::Device) ? c.hfull.as<uint8_t>() : nullptr;
+    j.d_pkt = R ? c.pkt.as<uint8_t>() : nullptr;
+    std::vector<uint8_t> crit;
+    std::vector<p2g_source_file> scanned;
+    if (src_known) {
+        j.set_id = critical_packets(slice, src_known, n, comments, n_comments, crit);
+        j.have_set_id = true;
+    }
+    cudaStream_t main = c.st[0];
+    P2G_TRY(run_device_job(c, j, main));
+
+    // Downloads
+    if (R) {
+        P2G_CU(rec_host.ensure((size_t)R * slice));
+        P2G_CU(cudaMemcpy2DAsync(rec_host.p, slice, c.rec.p, rec_stride, slice, R, cudaMemcpyDeviceToHost, main));
+        out.pkt_md5.resize(16 * (size_t)R);
+        P2G_CU(c.h_stage.ensure(16 * (size_t)R));
+        P2G_CU(cudaMemcpyAsync(c.h_stage.p, c.pkt.p, 16 * (size_t)R, cudaMemcpyDeviceToHost, main));
+    }
+    std::vector<p2g_slice_checksum> checks;
+    std::vector<uint8_t> hfull_dev;
+    if (!src_known) {
+        checks.resize(S);
+        if (S) P2G_CU(cudaMemcpyAsync(checks.data(), c.checks.p, sizeof(p2g_slice_checksum) * S,
+                                      cudaMemcpyDeviceToHost, main));
+        if (fmode == FileHashMode::Device) {
+            hfull_dev.resize(16 * (size_t)n);
+            P2G_CU(cudaMemcpyAsync(hfull_dev.data(), c.hfull.p, 16 * (size_t)n, cudaMemcpyDeviceToHost, main));
+        }
+    }
+    P2G_CU(cudaStreamSynchronize(main));
+    P2G_TRY(check_device_error(c));
+    if (R) memcpy(out.pkt_md5.data(), c.h_stage.p, 16 * (size_t)R);
+    hh.join();
+
+    if (!src_known) {
+        scanned.resize(n);
+        for (uint32_t f = 0; f < n; ++f) {
+            p2g_source_file& sf = scanned[f];
+            memset(&sf, 0, sizeof sf);
+            sf.name = (uint8_t*)malloc(std::max<size_t>(in[f].name_len, 1));
+            memcpy(sf.name, in[f].name, in[f].name_len);
+            sf.name_len = in[f].name_len;
+            const char* pth = in[f].path ? in[f].path : "";
+            sf.path = strdup(pth);
+            sf.length = in[f].length;
+            memcpy(sf.hash16k, j.h16k[f].data(), 16);
+            memcpy(sf.file_id, j.file_ids[f].data(), 16);
+            if (fmode == FileHashMode::Device)
+                memcpy(sf.hash_full, hfull_dev.data() + 16 * f, 16);
+            else
+                memcpy(sf.hash_full, host_full[f].data(), 16);
+            sf.slice_count = files[f].slices;
+            sf.slice_checksums = (p2g_slice_checksum*)malloc(sizeof(p2g_slice_checksum) * std::max<uint64_t>(1, sf.slice_count));
+            memcpy(sf.slice_checksums, checks.data() + files[f].first_slice, sizeof(p2g_slice_checksum) * sf.slice_count);
+        }
+        const Md5 sid = critical_packets(slice, scanned.data(), n, comments, n_comments, crit);
+        if (sid != j.set_id) {
+            for (auto& sf : scanned) free_source(sf);
+            return set_error(P2G_ERR_CUDA, "internal: set id mismatch between device job and packet assembly");
+        }
+    }
+    out.critical = std::move(crit);
+    out.set_id = j.set_id;
+    out.rec_host = rec_host.p;
+    out.sources = std::move(scanned);
+    return P2G_OK;
+}
+
+// Byte pieces of one volume file: critical ‖ recovery packets ‖ critical
+// (build_volume_packet, src/creator.rs:1025-1042).
+static void volume_pieces(const CreateOutput& o, uint64_t slice, uint32_t first, uint32_t count,
+                          std::vector<uint8_t>& headers, std::vector<std::pair<const uint8_t*, size_t>>& pieces) {
+    headers.assign(68 * (size_t)count, 0);
+    pieces.clear();
+    pieces.push_back({o.critical.data(), o.critical.size()});
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t e = first + k;
+        recovery_packet_header(headers.data() + 68 * (size_t)k, o.set_id, o.pkt_md5.data() + 16 * (size_t)e, slice, e);
+        pieces.push_back({headers.data() + 68 * (size_t)k, 68});
+        pieces.push_back({o.rec_host + (size_t)e * slice, (size_t)slice});
+    }
+    pieces.push_back({o.critical.data(), o.critical.size()});
+}
+
+static char* dupstr(const std::string& s) {
+    char* r = (char*)malloc(s.size() + 1);
+    memcpy(r, s.c_str(), s.size() + 1);
+    return r;
+}
+
+static void fill_path_list(p2g_path_list* out, const std::vector<std::string>& v) {
+    if (!out) return;
+    out->count = (uint32_t)v.size();
+    out->paths = (char**)calloc(std::max<size_t>(v.size(), 1), sizeof(char*));
+    for (size_t i = 0; i < v.size(); ++i) out->paths[i] = dupstr(v[i]);
+}
+
+}  // namespace p2g
+
+using namespace p2g;
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" uint64_t p2g_kernel_launch_count(void) { return launch_count(); }
+
+extern "C" p2g_status p2g_device_info(char* buf, size_t cap) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    P2G_TRY(ensure_ready(c));
+    cudaDeviceProp prop;
+    P2G_CU(cudaGetDeviceProperties(&prop, c.device));
+    if (buf && cap) snprintf(buf, cap, "%s sm_%d%d SMs=%d mem=%zuMiB", prop.name, prop.major, prop.minor,
+                             prop.multiProcessorCount, prop.totalGlobalMem >> 20);
+    return P2G_OK;
+}
+
+extern "C" void p2g_source_file_free(p2g_source_file* sf) {
+    if (sf) free_source(*sf);
+}
+extern "C" void p2g_path_list_free(p2g_path_list* pl) {
+    if (!pl) return;
+    for (uint32_t i = 0; i < pl->count; ++i) free(pl->paths[i]);
+    free(pl->paths);
+    pl->paths = nullptr;
+    pl->count = 0;
+}
+extern "C" void p2g_string_free(char* s) { free(s); }
+extern "C" void p2g_output_set_free(p2g_output_set* os) {
+    if (!os) return;
+    for (uint32_t i = 0; i < os->count; ++i) {
+        free(os->files[i].name);
+        free(os->files[i].data);
+    }
+    free(os->files);
+    os->files = nullptr;
+    os->count = 0;
+}
+
+// ---- seams ----------------------------------------------------------------
+extern "C" p2g_status p2g_gf_mul_xor(uint16_t coeff, const uint8_t* input, uint8_t* output, size_t len,
+                                     uint32_t flags, void* stream) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (len % 2) return set_error(P2G_ERR_INVALID_ARGUMENT, "buffer length must be even (16-bit symbols)");
+    if (len && (!input || !output)) return set_error(P2G_ERR_INVALID_ARGUMENT, "NULL buffer");
+    P2G_TRY(ensure_ready(c));
+    if (!len) return P2G_OK;
+    if (flags & P2G_DEVICE_POINTERS) {
+        P2G_CU(launch_gf_mul_xor(coeff, input, output, len, (cudaStream_t)stream));
+        return P2G_OK;
+    }
+    P2G_CU(c.tmp_in.ensure(len));
+    P2G_CU(c.tmp_out.ensure(len));
+    cudaStream_t s = c.st[0];
+    P2G_CU(cudaMemcpyAsync(c.tmp_in.p, input, len, cudaMemcpyHostToDevice, s));
+    P2G_CU(cudaMemcpyAsync(c.tmp_out.p, output, len, cudaMemcpyHostToDevice, s));
+    P2G_CU(launch_gf_mul_xor(coeff, c.tmp_in.as<uint8_t>(), c.tmp_out.as<uint8_t>(), len, s));
+    P2G_CU(cudaMemcpyAsync(output, c.tmp_out.p, len, cudaMemcpyDeviceToHost, s));
+    P2G_CU(cudaStreamSynchronize(s));
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (!job) return set_error(P2G_ERR_INVALID_ARGUMENT, "job is NULL");
+    const p2g_encode_job& jb = *job;
+    if (jb.slice_size == 0 || jb.slice_size % 4)
+        return set_error(P2G_ERR_INVALID_SLICE_SIZE, "invalid slice size %llu: must be > 0 and a multiple of 4",
+                         (unsigned long long)jb.slice_size);
+    if (jb.input_count > P2G_MAX_INPUT_BLOCKS)
+        return set_error(P2G_ERR_INVALID_ARGUMENT, "input_count %u exceeds 32768", jb.input_count);
+    if ((uint64_t)jb.first_exponent + jb.recovery_count > 65536ull)
+        return set_error(P2G_ERR_TOO_MANY_RECOVERY_BLOCKS, "recovery exponents exceed 65535");
+    if (jb.src_stride < jb.slice_size || jb.recovery_stride < jb.slice_size)
+        return set_error(P2G_ERR_INVALID_ARGUMENT, "stride smaller than slice_size");
+    P2G_TRY(ensure_ready(c));
+    const uint32_t S = jb.input_count, R = jb.recovery_count;
+    if (!R) return P2G_OK;
+    const uint32_t RG = (R + kRowsPerGroup - 1) / kRowsPerGroup;
+    if (jb.flags & P2G_DEVICE_POINTERS) {
+        if (((uintptr_t)jb.src | (uintptr_t)jb.recovery) % 16 || jb.src_stride % 16 || jb.recovery_stride % 16)
+            return set_error(P2G_ERR_INVALID_ARGUMENT,
+                             "device encode needs 16-byte aligned pointers and strides that are multiples of 16");
+        if (jb.recovery_stride < round_up(jb.slice_size, 16))
+            return set_error(P2G_ERR_INVALID_ARGUMENT, "recovery_stride must be >= slice_size rounded up to 16");
+        cudaStream_t s = (cudaStream_t)jb.stream;
+        if (!S) {
+            P2G_CU(cudaMemset2DAsync(jb.recovery, jb.recovery_stride, 0, jb.slice_size, R, s));
+            return P2G_OK;
+        }
+        P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
+        P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
+        P2G_CU(launch_encode(jb.src, jb.src_stride, S, c.basis.as<uint16_t>(), RG, R, jb.slice_size, jb.recovery,
+                             jb.recovery_stride, c.err.as<int>(), s));
+        return P2G_OK;
+    }
+    // host pointers: stage through device buffers
+    const uint64_t stride = round_up(jb.slice_size, 16);
+    cudaStream_t s = c.st[0];
+    P2G_CU(c.src.ensure((size_t)stride * std::max<uint32_t>(S, 1)));
+    P2G_CU(c.rec.ensure((size_t)stride * R));
+    P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s));
+    if (S) {
+        P2G_CU(cudaMemcpy2DAsync(c.src.p, stride, jb.src, jb.src_stride, jb.slice_size, S, cudaMemcpyHostToDevice, s));
+        P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
+        P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
+        P2G_CU(launch_encode(c.src.as<uint8_t>(), stride, S, c.basis.as<uint16_t>(), RG, R, jb.slice_size,
+                             c.rec.as<uint8_t>(), stride, c.err.as<int>(), s));
+    } else {
+        P2G_CU(cudaMemsetAsync(c.rec.p, 0, (size_t)stride * R, s));
+    }
+    P2G_CU(cudaMemcpy2DAsync(jb.recovery, jb.recovery_stride, c.rec.p, stride, jb.slice_size, R,
+                             cudaMemcpyDeviceToHost, s));
+    P2G_CU(cudaMemcpyAsync(c.h_err.p, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    P2G_CU(cudaStreamSynchronize(s));
+    return check_device_error(c);
+}
+
+extern "C" p2g_status p2g_slice_checksums(const uint8_t* src, uint64_t src_stride, uint32_t count,
+                                          uint64_t slice_size, p2g_slice_checksum* out, uint32_t flags,
+                                          void* stream) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (slice_size == 0 || slice_size % 4)
+        return set_error(P2G_ERR_INVALID_SLICE_SIZE, "invalid slice size %llu: must be > 0 and a multiple of 4",
+                         (unsigned long long)slice_size);
+    if (src_stride < slice_size || src_stride % 4 || (uintptr_t)src % 4)
+        return set_error(P2G_ERR_INVALID_ARGUMENT, "src must be 4-byte aligned with stride >= slice_size, multiple of 4");
+    P2G_TRY(ensure_ready(c));
+    if (!count) return P2G_OK;
+    if (flags & P2G_DEVICE_POINTERS) {
+        cudaStream_t s = (cudaStream_t)stream;
+        P2G_CU(launch_md5_slices(src, src_stride, count, slice_size, out, s));
+        P2G_CU(launch_crc_slices(src, src_stride, count, slice_size, out, s));
+        return P2G_OK;
+    }
+    cudaStream_t s = c.st[0];
+    P2G_CU(c.src.ensure((size_t)slice_size * count));
+    P2G_CU(c.checks.ensure(sizeof(p2g_slice_checksum) * count));
+    P2G_CU(cudaMemcpy2DAsync(c.src.p, slice_size, src, src_stride, slice_size, count, cudaMemcpyHostToDevice, s));
+    P2G_CU(launch_md5_slices(c.src.as<uint8_t>(), slice_size, count, slice_size, c.checks.as<p2g_slice_checksum>(), s));
+    P2G_CU(launch_crc_slices(c.src.as<uint8_t>(), slice_size, count, slice_size, c.checks.as<p2g_slice_checksum>(), s));
+    P2G_CU(cudaMemcpyAsync(out, c.checks.p, sizeof(p2g_slice_checksum) * count, cudaMemcpyDeviceToHost, s));
+    P2G_CU(cudaStreamSynchronize(s));
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_file_hashes(const uint8_t* const* data, const uint64_t* lengths, uint32_t n,
+                                      uint8_t* hash_full_out, uint8_t* hash16k_out, uint32_t flags, void* stream) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (n && (!data || !lengths)) return set_error(P2G_ERR_INVALID_ARGUMENT, "NULL arrays");
+    P2G_TRY(ensure_ready(c));
+    if (!n) return P2G_OK;
+    for (uint32_t f = 0; f < n; ++f)
+        if ((uintptr_t)data[f] % 4) return set_error(P2G_ERR_INVALID_ARGUMENT, "file %u data not 4-byte aligned", f);
+    // Spans are offsets from a common base: the lowest pointer.
+    const uint8_t* base = data[0];
+    for (uint32_t f = 1; f < n; ++f) base = std::min(base, data[f]);
+    P2G_CU(c.h_spans.ensure(sizeof(FileSpan) * 2 * n));
+    P2G_CU(c.spans.ensure(sizeof(FileSpan) * 2 * n));
+    FileSpan* hs = c.h_spans.as<FileSpan>();
+    uint64_t total = 0;
+    for (uint32_t f = 0; f < n; ++f) total += lengths[f];
+    if (flags & P2G_DEVICE_POINTERS) {
+        cudaStream_t s = (cudaStream_t)stream;
+        for (uint32_t f = 0; f < n; ++f) {
+            hs[f] = {(uint64_t)(data[f] - base), std::min<uint64_t>(lengths[f], P2G_HASH16K_LEN)};
+            hs[n + f] = {(uint64_t)(data[f] - base), lengths[f]};
+        }
+        P2G_CU(cudaMemcpyAsync(c.spans.p, hs, sizeof(FileSpan) * 2 * n, cudaMemcpyHostToDevice, s));
+        if (hash16k_out) P2G_CU(launch_md5_files(base, c.spans.as<FileSpan>(), n, hash16k_out, s));
+        if (hash_full_out) P2G_CU(launch_md5_files(base, c.spans.as<FileSpan>() + n, n, hash_full_out, s));
+        P2G_CU(cudaStreamSynchronize(s));  // h_spans is reused by the next call
+        return P2G_OK;
+    }
+    cudaStream_t s = c.st[0];
+    P2G_CU(c.src.ensure(std::max<uint64_t>(total + 16 * n, 16)));
+    uint64_t off = 0;
+    for (uint32_t f = 0; f < n; ++f) {
+        hs[f] = {off, std::min<uint64_t>(lengths[f], P2G_HASH16K_LEN)};
+        hs[n + f] = {off, lengths[f]};
+        if (lengths[f]) P2G_CU(cudaMemcpyAsync(c.src.as<uint8_t>() + off, data[f], lengths[f], cudaMemcpyHostToDevice, s));
+        off = round_up(off + lengths[f], 16);
+    }
+    P2G_CU(c.hfull.ensure(32 * (size_t)n));
+    uint8_t* d16 = c.hfull.as<uint8_t>();
+    uint8_t* dfull = d16 + 16 * (size_t)n;
+    P2G_CU(cudaMemcpyAsync(c.spans.p, hs, sizeof(FileSpan) * 2 * n, cudaMemcpyHostToDevice, s));
+    P2G_CU(launch_md5_files(c.src.as<uint8_t>(), c.spans.as<FileSpan>(), n, d16, s));
+    P2G_CU(launch_md5_files(c.src.as<uint8_t>(), c.spans.as<FileSpan>() + n, n, dfull, s));
+    if (hash16k_out) P2G_CU(cudaMemcpyAsync(hash16k_out, d16, 16 * (size_t)n, cudaMemcpyDeviceToHost, s));
+    if (hash_full_out) P2G_CU(cudaMemcpyAsync(hash_full_out, dfull, 16 * (size_t)n, cudaMemcpyDeviceToHost, s));
+    P2G_CU(cudaStreamSynchronize(s));
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_recovery_packet_md5(const uint8_t set_id[16], const uint8_t* recovery,
+                                              uint64_t recovery_stride, uint32_t count, uint64_t slice_size,
+                                              uint16_t first_exponent, uint8_t* md5_out, uint32_t flags,
+                                              void* stream) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (slice_size == 0 || slice_size % 4)
+        return set_error(P2G_ERR_INVALID_SLICE_SIZE, "invalid slice size %llu", (unsigned long long)slice_size);
+    if (recovery_stride < slice_size || recovery_stride % 4 || (uintptr_t)recovery % 4)
+        return set_error(P2G_ERR_INVALID_ARGUMENT, "recovery must be 4-byte aligned, stride >= slice_size");
+    P2G_TRY(ensure_ready(c));
+    if (!count) return P2G_OK;
+    if (flags & P2G_DEVICE_POINTERS) {
+        P2G_CU(launch_md5_recovery(recovery, recovery_stride, count, slice_size, set_id, first_exponent, md5_out,
+                                   (cudaStream_t)stream));
+        return P2G_OK;
+    }
+    cudaStream_t s = c.st[0];
+    P2G_CU(c.rec.ensure((size_t)slice_size * count));
+    P2G_CU(c.pkt.ensure(16 * (size_t)count));
+    P2G_CU(cudaMemcpy2DAsync(c.rec.p, slice_size, recovery, recovery_stride, slice_size, count, cudaMemcpyHostToDevice, s));
+    P2G_CU(launch_md5_recovery(c.rec.as<uint8_t>(), slice_size, count, slice_size, set_id, first_exponent,
+                               c.pkt.as<uint8_t>(), s));
+    P2G_CU(cudaMemcpyAsync(md5_out, c.pkt.p, 16 * (size_t)count, cudaMemcpyDeviceToHost, s));
+    P2G_CU(cudaStreamSynchronize(s));
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_run_device_job(p2g_device_job* job) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (!job) return set_error(P2G_ERR_INVALID_ARGUMENT, "job is NULL");
+    p2g_device_job& jb = *job;
+    P2G_TRY(check_common(jb.file_count, jb.recovery_count, jb.slice_size));
+    if (!jb.src || (uintptr_t)jb.src % 16 || (jb.recovery_count && ((uintptr_t)jb.recovery % 16 || jb.recovery_stride % 16 ||
+                                                                    jb.recovery_stride < round_up(jb.slice_size, 16))))
+        return set_error(P2G_ERR_INVALID_ARGUMENT,
+                         "device job needs 16-byte aligned src/recovery and recovery_stride >= round_up(slice,16)");
+    P2G_TRY(ensure_ready(c));
+    DeviceJob j;
+    uint64_t S = 0, total = 0;
+    for (uint32_t f = 0; f < jb.file_count; ++f) {
+        P2G_TRY(check_name(jb.names[f], jb.name_lens[f], ""));
+        if (jb.file_lengths[f] == 0) return set_error(P2G_ERR_EMPTY_FILE, "input file %u is empty", f);
+        const uint64_t sl = (jb.file_lengths[f] + jb.slice_size - 1) / jb.slice_size;
+        j.files.push_back({jb.file_lengths[f], S, sl, jb.names[f], jb.name_lens[f]});
+        S += sl;
+        total += jb.file_lengths[f];
+    }
+    P2G_TRY(check_total_blocks(S, total, jb.slice_size));
+    j.d_src = jb.src;
+    j.S = (uint32_t)S;
+    j.slice = jb.slice_size;
+    j.R = jb.recovery_count;
+    j.d_rec = jb.recovery;
+    j.rec_stride = jb.recovery_stride;
+    j.d_checks = jb.checksums;
+    j.d_h16k = jb.hash16k;
+    j.d_hfull = (jb.flags & P2G_JOB_SKIP_HASH_FULL) ? nullptr : jb.hash_full;
+    j.d_pkt = jb.packet_md5;
+    if (!j.d_h16k) return set_error(P2G_ERR_INVALID_ARGUMENT, "hash16k output is required (it derives the set id)");
+    P2G_TRY(run_device_job(c, j, (cudaStream_t)jb.stream));
+    memcpy(jb.set_id_out, j.set_id.data(), 16);
+    return P2G_OK;
+}
+
+// ---- create pipeline ----------------------------------------------------
+static p2g_status scan_impl(const char* path, const uint8_t* name, size_t name_len, uint64_t slice,
+                            p2g_progress_fn cb, void* user, p2g_source_file* out) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (!path || !out) return set_error(P2G_ERR_INVALID_ARGUMENT, "NULL argument");
+    P2G_TRY(check_name(name, name_len, path));
+    if (slice == 0 || slice % 4)
+        return set_error(P2G_ERR_INVALID_SLICE_SIZE, "invalid slice size %llu: must be > 0 and a multiple of 4",
+                         (unsigned long long)slice);
+    uint64_t len = 0;
+    P2G_TRY(stat_len(path, &len));
+    if (len == 0) return set_error(P2G_ERR_EMPTY_FILE, "input file \"%s\" is empty; PAR2 requires non-empty files", path);
+    const uint64_t total_slices = (len + slice - 1) / slice;
+    p2g_progress_event ev = mk(P2G_EV_SCAN_STARTED);
+    ev.path = path;
+    ev.total_slices = total_slices;
+    emit(cb, user, ev);
+    P2G_TRY(ensure_ready(c));
+    HostFile hf;
+    hf.path = path;
+    P2G_TRY(read_file(hf, len));
+    if (hf.length == 0) return set_error(P2G_ERR_EMPTY_FILE, "input file \"%s\" is empty; PAR2 requires non-empty files", path);
+    CreateInput in = {hf.data, hf.length, name, name_len, path};
+    CreateOutput o;
+    PinnedRec rec;
+    P2G_TRY(device_create(c, &in, 1, slice, 0, nullptr, nullptr, 0, o, rec));
+    const uint64_t done = o.sources[0].slice_count;
+    ev = mk(P2G_EV_SCAN_PROGRESS);
+    ev.path = path;
+    ev.slices_done = done;
+    ev.total_slices = done;
+    emit(cb, user, ev);
+    ev = mk(P2G_EV_SCAN_COMPLETED);
+    ev.path = path;
+    emit(cb, user, ev);
+    *out = o.sources[0];
+    o.sources.clear();
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_scan(const char* path, const uint8_t* display_name, size_t name_len, uint64_t slice_size,
+                               p2g_source_file* out) {
+    return scan_impl(path, display_name, name_len, slice_size, nullptr, nullptr, out);
+}
+extern "C" p2g_status p2g_scan_with_progress(const char* path, const uint8_t* display_name, size_t name_len,
+                                             uint64_t slice_size, p2g_progress_fn cb, void* user,
+                                             p2g_source_file* out) {
+    return scan_impl(path, display_name, name_len, slice_size, cb, user, out);
+}
+
+// Writes the index and (if R > 0) volume files of an already computed set.
+static p2g_status write_outputs(const p2g_create_options& o, const CreateOutput& co, uint32_t R, uint64_t slice,
+                                p2g_progress_fn cb, void* user, std::vector<std::string>& written) {
+    std::vector<std::pair<const uint8_t*, size_t>> pieces = {{co.critical.data(), co.critical.size()}};
+    P2G_TRY(write_atomic(o.output, pieces));
+    p2g_progress_event ev = mk(P2G_EV_INDEX_WRITTEN);
+    ev.path = o.output;
+    emit(cb, user, ev);
+    written.push_back(o.output);
+    if (!R) return P2G_OK;
+    uint32_t first = 0;
+    std::vector<uint8_t> headers;
+    for (uint32_t cnt : co.vol_sizes) {
+        const std::string vp = volume_filename(o.output, (uint16_t)first, cnt);
+        volume_pieces(co, slice, first, cnt, headers, pieces);
+        P2G_TRY(write_atomic(vp, pieces));
+        ev = mk(P2G_EV_VOLUME_WRITTEN);
+        ev.path = vp.c_str();
+        emit(cb, user, ev);
+        written.push_back(vp);
+        first += cnt;
+    }
+    return P2G_OK;
+}
+
+static void emit_encode_events(p2g_progress_fn cb, void* user, uint64_t S, uint32_t R, bool completed) {
+    if (!completed) {
+        p2g_progress_event ev = mk(P2G_EV_ENCODE_STARTED);
+        ev.volume_index = 0;
+        ev.total_volumes = 1;
+        ev.input_blocks = S;
+        ev.recovery_blocks = R;
+        emit(cb, user, ev);
+        return;
+    }
+    p2g_progress_event ev = mk(P2G_EV_ENCODE_PROGRESS);
+    ev.input_block_done = S;
+    ev.input_blocks = S;
+    emit(cb, user, ev);
+    ev = mk(P2G_EV_ENCODE_COMPLETED);
+    emit(cb, user, ev);
+}
+
+static p2g_status run_create_impl(const p2g_create_options* opts, const p2g_source_file* sources, uint32_t n,
+                                  p2g_progress_fn cb, void* user, p2g_path_list* out) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (!opts || !opts->output) return set_error(P2G_ERR_INVALID_ARGUMENT, "options/output is NULL");
+    const uint32_t R = opts->recovery_block_count;
+    const uint64_t slice = opts->slice_size;
+    P2G_TRY(check_common(n, R, slice));
+    uint64_t S = 0, total_bytes = 0;
+    for (uint32_t f = 0; f < n; ++f) {
+        S += sources[f].slice_count;
+        total_bytes += sources[f].length;
+    }
+    P2G_TRY(check_total_blocks(S, total_bytes, slice));
+
+    CreateOutput co;
+    co.set_id = critical_packets(slice, sources, n, opts->comments, opts->comment_count, co.critical);
+    std::vector<std::string> written;
+    {  // index first (src/creator.rs:237-241)
+        std::vector<std::pair<const uint8_t*, size_t>> pieces = {{co.critical.data(), co.critical.size()}};
+        P2G_TRY(write_atomic(opts->output, pieces));
+        p2g_progress_event ev = mk(P2G_EV_INDEX_WRITTEN);
+        ev.path = opts->output;
+        emit(cb, user, ev);
+        written.push_back(opts->output);
+    }
+    if (R > 0) {
+        P2G_TRY(resolve_volume_sizes(opts->volume_scheme, R, co.vol_sizes));
+        P2G_TRY(ensure_ready(c));
+        emit_encode_events(cb, user, S, R, false);
+        // Re-read the sources (SourceReader, src/creator.rs:63-86): exactly the
+        // slices listed in each SourceFile, zero-padded.
+        std::vector<std::unique_ptr<HostFile>> hfs(n);
+        std::vector<CreateInput> ins(n);
+        for (uint32_t f = 0; f < n; ++f) {
+            hfs[f].reset(new HostFile());
+            hfs[f]->path = sources[f].path ? sources[f].path : "";
+            P2G_TRY(read_file(*hfs[f], sources[f].slice_count * slice));
+            ins[f] = {hfs[f]->data, hfs[f]->length, sources[f].name, sources[f].name_len, sources[f].path};
+        }
+        CreateOutput enc;
+        PinnedRec rec;
+        P2G_TRY(device_create(c, ins.data(), n, slice, R, sources, opts->comments, opts->comment_count, enc, rec));
+        emit_encode_events(cb, user, S, R, true);
+        co.rec_host = enc.rec_host;
+        co.pkt_md5 = std::move(enc.pkt_md5);
+        uint32_t first = 0;
+        std::vector<uint8_t> headers;
+        std::vector<std::pair<const uint8_t*, size_t>> pieces;
+        for (uint32_t cnt : co.vol_sizes) {
+            const std::string vp = volume_filename(opts->output, (uint16_t)first, cnt);
+            volume_pieces(co, slice, first, cnt, headers, pieces);
+            P2G_TRY(write_atomic(vp, pieces));
+            p2g_progress_event ev = mk(P2G_EV_VOLUME_WRITTEN);
+            ev.path = vp.c_str();
+            emit(cb, user, ev);
+            written.push_back(vp);
+            first += cnt;
+        }
+    }
+    fill_path_list(out, written);
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_run_create(const p2g_create_options* opts, const p2g_source_file* sources, uint32_t n,
+                                     p2g_path_list* out) {
+    return run_create_impl(opts, sources, n, nullptr, nullptr, out);
+}
+extern "C" p2g_status p2g_run_create_with_progress(const p2g_create_options* opts, const p2g_source_file* sources,
+                                                   uint32_t n, p2g_progress_fn cb, void* user, p2g_path_list* out) {
+    return run_create_impl(opts, sources, n, cb, user, out);
+}
+
+extern "C" p2g_status p2g_write_index_file(const p2g_create_options* opts, const p2g_source_file* sources, uint32_t n,
+                                           char** out_path) {
+    if (!opts) return set_error(P2G_ERR_INVALID_ARGUMENT, "options is NULL");
+    p2g_create_options o = *opts;
+    o.recovery_block_count = 0;
+    o.volume_scheme = p2g_volume_scheme{P2G_SCHEME_SINGLE, 0, 0, nullptr, nullptr, 0};
+    p2g_path_list pl = {nullptr, 0};
+    p2g_status st = run_create_impl(&o, sources, n, nullptr, nullptr, &pl);
+    if (st != P2G_OK) return st;
+    if (out_path) *out_path = dupstr(pl.paths[0]);
+    p2g_path_list_free(&pl);
+    return P2G_OK;
+}
+
+// Fused validation order, src/creator.rs:461-508.
+static p2g_status fused_validate(uint32_t n, uint32_t R, uint64_t slice) { return check_common(n, R, slice); }
+
+extern "C" p2g_status p2g_run_create_fused(const p2g_create_options* opts, const p2g_input* inputs, uint32_t n,
+                                           p2g_progress_fn cb, void* user, p2g_path_list* out) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (!opts || !opts->output) return set_error(P2G_ERR_INVALID_ARGUMENT, "options/output is NULL");
+    const uint32_t R = opts->recovery_block_count;
+    const uint64_t slice = opts->slice_size;
+    P2G_TRY(fused_validate(n, R, slice));
+    std::vector<uint64_t> lens(n);
+    uint64_t S = 0, total = 0;
+    for (uint32_t f = 0; f < n; ++f) {
+        P2G_TRY(check_name(inputs[f].display_name, inputs[f].name_len, inputs[f].path));
+        P2G_TRY(stat_len(inputs[f].path, &lens[f]));
+        if (lens[f] == 0)
+            return set_error(P2G_ERR_EMPTY_FILE, "input file \"%s\" is empty; PAR2 requires non-empty files",
+                             inputs[f].path);
+        S += (lens[f] + slice - 1) / slice;
+        total += lens[f];
+    }
+    P2G_TRY(check_total_blocks(S, total, slice));
+    P2G_TRY(ensure_ready(c));
+    if (R) emit_encode_events(cb, user, S, R, false);
+    std::vector<std::unique_ptr<HostFile>> hfs(n);
+    std::vector<CreateInput> ins(n);
+    for (uint32_t f = 0; f < n; ++f) {
+        p2g_progress_event ev = mk(P2G_EV_SCAN_STARTED);
+        ev.path = inputs[f].path;
+        ev.total_slices = (lens[f] + slice - 1) / slice;
+        emit(cb, user, ev);
+        hfs[f].reset(new HostFile());
+        hfs[f]->path = inputs[f].path;
+        P2G_TRY(read_file(*hfs[f], lens[f]));
+        ins[f] = {hfs[f]->data, hfs[f]->length, inputs[f].display_name, inputs[f].name_len, inputs[f].path};
+    }
+    CreateOutput co;
+    PinnedRec rec;
+    P2G_TRY(device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co, rec));
+    for (uint32_t f = 0; f < n; ++f) {
+        p2g_progress_event ev = mk(P2G_EV_SCAN_PROGRESS);
+        ev.path = inputs[f].path;
+        ev.slices_done = ev.total_slices = co.sources[f].slice_count;
+        emit(cb, user, ev);
+        ev = mk(P2G_EV_SCAN_COMPLETED);
+        ev.path = inputs[f].path;
+        emit(cb, user, ev);
+    }
+    for (auto& sf : co.sources) free_source(sf);
+    if (R) emit_encode_events(cb, user, S, R, true);
+    if (R) {
+        // the index is written before the scheme is resolved (src/creator.rs:237-244)
+        std::vector<std::pair<const uint8_t*, size_t>> pieces = {{co.critical.data(), co.critical.size()}};
+        std::vector<uint32_t> vs;
+        p2g_status st = resolve_volume_sizes(opts->volume_scheme, R, vs);
+        if (st != P2G_OK) {
+            const std::string msg = p2g_last_error_message();
+            P2G_TRY(write_atomic(opts->output, pieces));
+            return set_error(st, "%s", msg.c_str());
+        }
+        co.vol_sizes = vs;
+    }
+    std::vector<std::string> written;
+    P2G_TRY(write_outputs(*opts, co, R, slice, cb, user, written));
+    fill_path_list(out, written);
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_create_in_memory(const p2g_create_options* opts, const p2g_buffer_input* inputs, uint32_t n,
+                                           p2g_source_file* sources_out, p2g_output_set* out) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (!opts || !out) return set_error(P2G_ERR_INVALID_ARGUMENT, "NULL argument");
+    const uint32_t R = opts->recovery_block_count;
+    const uint64_t slice = opts->slice_size;
+    P2G_TRY(fused_validate(n, R, slice));
+    uint64_t S = 0, total = 0;
+    std::vector<CreateInput> ins(n);
+    for (uint32_t f = 0; f < n; ++f) {
+        P2G_TRY(check_name(inputs[f].display_name, inputs[f].name_len, ""));
+        if (inputs[f].length == 0) return set_error(P2G_ERR_EMPTY_FILE, "input file %u is empty; PAR2 requires non-empty files", f);
+        S += (inputs[f].length + slice - 1) / slice;
+        total += inputs[f].length;
+        ins[f] = {inputs[f].data, inputs[f].length, inputs[f].display_name, inputs[f].name_len, nullptr};
+    }
+    P2G_TRY(check_total_blocks(S, total, slice));
+    std::vector<uint32_t> vs;
+    if (R) P2G_TRY(resolve_volume_sizes(opts->volume_scheme, R, vs));
+    P2G_TRY(ensure_ready(c));
+    CreateOutput co;
+    PinnedRec rec;
+    P2G_TRY(device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co, rec));
+    co.vol_sizes = vs;
+    const std::string index = opts->output ? opts->output : "recovery.par2";
+    out->count = 1 + (uint32_t)co.vol_sizes.size();
+    out->files = (p2g_output_file*)calloc(out->count, sizeof(p2g_output_file));
+    out->files[0].name = dupstr(index);
+    out->files[0].length = co.critical.size();
+    out->files[0].data = (uint8_t*)malloc(std::max<size_t>(co.critical.size(), 1));
+    memcpy(out->files[0].data, co.critical.data(), co.critical.size());
+    uint32_t first = 0;
+    std::vector<uint8_t> headers;
+    std::vector<std::pair<const uint8_t*, size_t>> pieces;
+    for (size_t v = 0; v < co.vol_sizes.size(); ++v) {
+        volume_pieces(co, slice, first, co.vol_sizes[v], headers, pieces);
+        size_t tot = 0;
+        for (auto& p : pieces) tot += p.second;
+        p2g_output_file& of = out->files[1 + v];
+        of.name = dupstr(volume_filename(index, (uint16_t)first, co.vol_sizes[v]));
+        of.length = tot;
+        of.data = (uint8_t*)malloc(std::max<size_t>(tot, 1));
+        size_t at = 0;
+        for (auto& p : pieces) {
+            memcpy(of.data + at, p.first, p.second);
+            at += p.second;
+        }
+        first += co.vol_sizes[v];
+    }
+    if (sources_out)
+        for (uint32_t f = 0; f < n; ++f) sources_out[f] = co.sources[f];
+    else
+        for (auto& sf : co.sources) free_source(sf);
+    return P2G_OK;
+}
