@@ -43,6 +43,8 @@ PUBLISHED_E2E_GBS = 0.0975  # par2rust create, same shape, Apple M4 10 threads (
 WORKLOADS = {
     "single_538m": dict(length=538_218_411, slice=524_288, R=200, scheme="exponential", seed=2),
     "single_16m": dict(length=16_777_216, slice=65_536, R=32, scheme="single", seed=1),
+    # profiling case: same slice size and recovery count, 256 slices (134 MB > L2)
+    "prof_256x512k": dict(length=256 * 524_288, slice=524_288, R=200, scheme="exponential", seed=2),
 }
 
 
@@ -56,6 +58,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the device MD5-chain rate probe")
     return ap.parse_args()
 
 
@@ -160,7 +163,9 @@ def run_reference(args, wl):
     from par2rust_b200 import workloads as W
 
     data = W.file_bytes(W.file_seed(wl["seed"], 0, 0), wl["length"])
-    cb, tt = cpu_baseline(data, wl, target_s=min(args.cpu_seconds, 20.0), steps=args.steps, warmup=args.warmup)
+    # each step is a bounded sample sized so warmup+steps take about two minutes in total
+    per_step = max(1.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
+    cb, tt = cpu_baseline(data, wl, target_s=per_step, steps=args.steps, warmup=args.warmup)
     line = {
         "metric": "encode source GB/s", "value": cb["value"], "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tt * 1e3, "higher_is_better": True,
@@ -273,26 +278,31 @@ def main():
     opts = p2g.CreateOptions(output="recovery.par2", slice_size=slice_, recovery_block_count=R,
                              volume_scheme=p2g.VolumeScheme.Exponential() if wl["scheme"] == "exponential"
                              else p2g.VolumeScheme.Single())
-    p2g.create_in_memory(opts, [(name, host_src)])  # warm
-    barrier()
-    e2e_t = []
-    for _ in range(args.e2e_steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        files = p2g.create_in_memory(opts, [(name, host_src)])
-        torch.cuda.synchronize()
-        e2e_t.append(time.perf_counter() - t0)
-    et = torch.tensor([sum(e2e_t) / len(e2e_t)], device=dev)
-    if world > 1:
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-    e2e_val = world * L / float(et.item()) / 1e9
+    e2e_val, e2e_s, files = None, None, []
+    if args.e2e_steps > 0:
+        p2g.create_in_memory(opts, [(name, host_src)])  # warm
+        barrier()
+        e2e_t = []
+        for _ in range(args.e2e_steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            files = p2g.create_in_memory(opts, [(name, host_src)])
+            torch.cuda.synchronize()
+            e2e_t.append(time.perf_counter() - t0)
+        et = torch.tensor([sum(e2e_t) / len(e2e_t)], device=dev)
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e_s = float(et.item())
+        e2e_val = world * L / e2e_s / 1e9
     d2h = R * slice_ + S * 20 + 16 * R + 32
 
     # device single-chain MD5 rate (the whole-file hash on the device)
-    t0 = time.perf_counter()
-    p2g.run_device_job(src[:64 * 1024 * 1024], [64 * 1024 * 1024], [name], slice_, 0, None)
-    torch.cuda.synchronize()
-    t_full = time.perf_counter() - t0
+    chain_gbs = None
+    if not args.no_extras:
+        t0 = time.perf_counter()
+        p2g.run_device_job(src[:64 * 1024 * 1024], [64 * 1024 * 1024], [name], slice_, 0, None)
+        torch.cuda.synchronize()
+        chain_gbs = 64 * 1024 * 1024 / (time.perf_counter() - t0) / 1e9
 
     # ---- CPU baseline (rank 0, N=1) ----
     cb = None
@@ -310,7 +320,7 @@ def main():
         "vs_baseline": value / PUBLISHED_E2E_GBS, "dtype": "u16", "data": "synthetic",
         "config": config_dict(args, wl),
         "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": L, "d2h_bytes_per_step": d2h,
-                "seconds_per_step": float(et.item()), "api": "p2g_create_in_memory (pinned host source)",
+                "seconds_per_step": e2e_s, "api": "p2g_create_in_memory (pinned host source)",
                 "output_files": len(files)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
@@ -322,7 +332,7 @@ def main():
         "cpu_baseline": cb,
         "clocks": clk,
         "gpu_launches": launches,
-        "file_md5_device_chain_gbs": 64 * 1024 * 1024 / t_full / 1e9,
+        "file_md5_device_chain_gbs": chain_gbs,
         "device": info,
         "baseline_note": "vs_baseline divides by the reference's published end-to-end create rate for this "
                          "shape (0.0975 GB/s, Apple M4, 10 threads)",

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <errno.h>
 #include <fcntl.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <sys/stat.h>
@@ -91,9 +92,11 @@ struct Context {
     std::recursive_mutex mu;
     int device = -1;
     bool ready = false;
-    cudaStream_t st[5] = {};
-    cudaEvent_t ev_fork = nullptr, ev_h16k = nullptr, ev_join[5] = {};
-    DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out;
+    static constexpr int kStreams = 7;  // encode, files, slice md5, crc, hash_full, encode (odd bands), packet md5
+    static constexpr int kBandEvents = 64;
+    cudaStream_t st[kStreams] = {};
+    cudaEvent_t ev_fork = nullptr, ev_h16k = nullptr, ev_join[kStreams] = {}, ev_band[kBandEvents] = {};
+    DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out, md5_state;
     PinBuf h_spans, h_h16k, h_err, h_stage;
 };
 static Context& ctx() {
@@ -118,10 +121,17 @@ static p2g_status ensure_ready(Context& c) {
         if (prop.major < 10)
             return set_error(P2G_ERR_CUDA, "device %d (%s, sm_%d%d) is not sm_100: this build targets B200 only", dev,
                              prop.name, prop.major, prop.minor);
-        for (auto& s : c.st) P2G_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        // st[0] carries the encode; the MD5/CRC streams get the higher
+        // priority so their small, long-running blocks are dispatched ahead of
+        // encode CTAs and share the SMs with them.
+        int lo_pri = 0, hi_pri = 0;
+        P2G_CU(cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
+        for (int i = 0; i < Context::kStreams; ++i)
+            P2G_CU(cudaStreamCreateWithPriority(&c.st[i], cudaStreamNonBlocking, (i == 0 || i == 5) ? lo_pri : hi_pri));
         P2G_CU(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
         P2G_CU(cudaEventCreateWithFlags(&c.ev_h16k, cudaEventDisableTiming));
         for (auto& ev : c.ev_join) P2G_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        for (auto& ev : c.ev_band) P2G_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         P2G_CU(upload_tables());
         P2G_CU(c.err.ensure(64));
         P2G_CU(c.h_err.ensure(64));
@@ -132,6 +142,40 @@ static p2g_status ensure_ready(Context& c) {
     return P2G_OK;
 }
 
+// Optional stage timeline (P2G_TRACE=1): timing events recorded after each
+// stage on its stream, printed to stderr relative to the job start when the
+// job is joined.  Off by default; costs nothing when off.
+struct Tracer {
+    bool on = false;
+    cudaEvent_t t0 = nullptr;
+    std::vector<std::pair<std::string, cudaEvent_t>> marks;
+    void start(cudaStream_t s) {
+        on = getenv("P2G_TRACE") != nullptr;
+        if (!on) return;
+        cudaEventCreate(&t0);
+        cudaEventRecord(t0, s);
+    }
+    void mark(const char* what, cudaStream_t s) {
+        if (!on) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        marks.push_back({what, e});
+    }
+    void finish() {
+        if (!on) return;
+        for (auto& m : marks) {
+            cudaEventSynchronize(m.second);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, t0, m.second);
+            fprintf(stderr, "[p2g trace] %8.3f ms  %s\n", ms, m.first.c_str());
+            cudaEventDestroy(m.second);
+        }
+        cudaEventDestroy(t0);
+        marks.clear();
+    }
+};
+
 // Fork the side streams off `caller`, join them back.
 static p2g_status fork_from(Context& c, cudaStream_t caller) {
     P2G_CU(cudaEventRecord(c.ev_fork, caller));
@@ -139,7 +183,7 @@ static p2g_status fork_from(Context& c, cudaStream_t caller) {
     return P2G_OK;
 }
 static p2g_status join_into(Context& c, cudaStream_t caller) {
-    for (int i = 0; i < 5; ++i) {
+    for (int i = 0; i < Context::kStreams; ++i) {
         P2G_CU(cudaEventRecord(c.ev_join[i], c.st[i]));
         P2G_CU(cudaStreamWaitEvent(caller, c.ev_join[i], 0));
     }
@@ -231,6 +275,8 @@ static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) 
     const uint32_t n = (uint32_t)j.files.size();
     const uint32_t RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
     P2G_TRY(fork_from(c, caller));
+    Tracer tr;
+    tr.start(caller);
     cudaStream_t s_enc = c.st[0], s_files = c.st[1], s_md5 = c.st[2], s_crc = c.st[3], s_full = c.st[4];
     P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s_enc));
 
@@ -251,15 +297,24 @@ static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) 
             P2G_CU(cudaMemcpyAsync(c.h_h16k.p, j.d_h16k, 16 * n, cudaMemcpyDeviceToHost, s_files));
         }
         P2G_CU(cudaEventRecord(c.ev_h16k, s_files));
+        tr.mark("hash16k + D2H", s_files);
         if (j.d_hfull) {
             P2G_CU(cudaStreamWaitEvent(s_full, c.ev_h16k, 0));  // spans uploaded
             P2G_CU(launch_md5_files(j.d_src, c.spans.as<FileSpan>() + n, n, j.d_hfull, s_full));
+            tr.mark("hash_full", s_full);
         }
     }
     if (j.d_checks && j.S) {
         P2G_CU(launch_md5_slices(j.d_src, j.slice, j.S, j.slice, j.d_checks, s_md5));
-        P2G_CU(launch_crc_slices(j.d_src, j.slice, j.S, j.slice, j.d_checks, s_crc));
+        tr.mark("slice md5", s_md5);
+        // CRC32 is light but shared-memory and ALU heavy: run it after the
+        // last encode band (see below), alongside the final packet-MD5 step.
     }
+    // Banded encode: band b covers a contiguous symbol range of every row, so
+    // the recovery-packet MD5 chains (one per row, src/format.rs:33-54) can
+    // follow band by band while later bands are still encoding.
+    EncodePlan plan;
+    cudaStream_t s_enc2 = c.st[5], s_pkt = c.st[6];
     if (j.R && j.S) {
         P2G_CU(c.basis.ensure(basis_bytes(j.S, RG)));
         P2G_CU(launch_basis(c.basis.as<uint16_t>(), j.S, RG, j.R, j.first_exp, s_enc));
@@ -271,8 +326,35 @@ static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) 
             P2G_CU(launch_realign(j.d_src, j.slice, c.src_al.as<uint8_t>(), estride, j.S, j.slice, s_enc));
             esrc = c.src_al.as<uint8_t>();
         }
-        P2G_CU(launch_encode(esrc, estride, j.S, c.basis.as<uint16_t>(), RG, j.R, j.slice, j.d_rec, j.rec_stride,
-                             c.err.as<int>(), s_enc));
+        // slice-MD5 (and device whole-file MD5) blocks each hold an SM for
+        // about chain-length x 0.72 us per 64-byte block
+        uint32_t reserve = hash_blocks(j.d_checks ? j.S : 0) + hash_blocks(j.d_h16k ? n : 0);
+        double reserve_ms = j.d_checks ? (double)(j.slice / 64) * 7.2e-4 : 0.0;
+        if (j.d_hfull) {
+            uint64_t mx = 0;
+            for (const auto& f : j.files) mx = std::max(mx, f.length);
+            reserve += hash_blocks(n);
+            reserve_ms = std::max(reserve_ms, (double)(mx / 64) * 7.2e-4);
+        }
+        plan = plan_encode(j.slice, j.S, RG, j.d_pkt != nullptr, reserve, reserve_ms);
+        if (plan.bands.size() > (size_t)Context::kBandEvents) plan = plan_encode(j.slice, j.S, RG, false, 0, 0.0);
+        tr.mark("basis", s_enc);
+        P2G_CU(cudaEventRecord(c.ev_band[0], s_enc));  // basis (and realign) done
+        P2G_CU(cudaStreamWaitEvent(s_enc2, c.ev_band[0], 0));
+        for (uint32_t b = 0; b < (uint32_t)plan.bands.size(); ++b) {
+            // one stream: band b+1 starts when band b's wave drains, so bands
+            // complete in order and each packet-MD5 step can start early
+            cudaStream_t sb = s_enc;
+            P2G_CU(launch_encode_band(plan, b, esrc, estride, j.S, c.basis.as<uint16_t>(), RG, j.R, j.d_rec,
+                                      j.rec_stride, c.err.as<int>(), sb));
+            P2G_CU(cudaEventRecord(c.ev_band[b], sb));
+            tr.mark("encode band", sb);
+        }
+    }
+    if (j.d_checks && j.S) {
+        if (j.R) P2G_CU(cudaStreamWaitEvent(s_crc, c.ev_band[plan.bands.size() - 1], 0));
+        P2G_CU(launch_crc_slices(j.d_src, j.slice, j.S, j.slice, j.d_checks, s_crc));
+        tr.mark("slice crc32", s_crc);
     }
     if (!j.have_set_id) {
         // set id = MD5(main packet body) over the sorted file ids
@@ -287,10 +369,28 @@ static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) 
         std::vector<uint8_t> mp;
         j.set_id = build_main_packet(j.slice, j.file_ids, mp);
     }
-    if (j.R && j.d_pkt)
+    if (j.R && j.S && j.d_pkt) {
+        P2G_CU(c.md5_state.ensure(16 * (size_t)j.R));
+        const uint64_t total = 36 + j.slice;
+        const uint64_t nblocks = (total + 8) / 64 + 1;
+        uint64_t done = 0;
+        for (uint32_t b = 0; b < (uint32_t)plan.bands.size(); ++b) {
+            P2G_CU(cudaStreamWaitEvent(s_pkt, c.ev_band[b], 0));
+            const bool final = b + 1 == plan.bands.size();
+            const uint64_t complete = std::min<uint64_t>(j.slice, 2ull * plan.bands[b].end);
+            const uint64_t upto = final ? nblocks : (36 + complete) / 64;
+            P2G_CU(launch_md5_recovery_range(j.d_rec, j.rec_stride, j.R, j.slice, j.set_id.data(), j.first_exp,
+                                             c.md5_state.as<uint32_t>(), done, upto, final, j.d_pkt, s_pkt));
+            tr.mark("packet md5 band", s_pkt);
+            done = upto;
+        }
+    } else if (j.R && j.d_pkt) {  // S == 0: all-zero recovery rows
         P2G_CU(launch_md5_recovery(j.d_rec, j.rec_stride, j.R, j.slice, j.set_id.data(), j.first_exp, j.d_pkt, s_enc));
+    }
     P2G_CU(cudaMemcpyAsync(c.h_err.p, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, s_enc));
     P2G_TRY(join_into(c, caller));
+    tr.mark("joined", caller);
+    tr.finish();
     return P2G_OK;
 }
 

@@ -5,12 +5,12 @@
 #include <errno.h>
 #include <fcntl.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
 #include <algorithm>
-#include <mutex>
 
 namespace p2g {
 
@@ -56,39 +56,54 @@ namespace p2g {
 // ---------------------------------------------------------------------------
 static inline uint32_t rol(uint32_t x, int s) { return (x << s) | (x >> (32 - s)); }
 
-static const uint32_t kMd5T[64] = {
-    0xd76aa478, 0xe8c7b756, 0x242070db, 0xc1bdceee, 0xf57c0faf, 0x4787c62a, 0xa8304613, 0xfd469501,
-    0x698098d8, 0x8b44f7af, 0xffff5bb1, 0x895cd7be, 0x6b901122, 0xfd987193, 0xa679438e, 0x49b40821,
-    0xf61e2562, 0xc040b340, 0x265e5a51, 0xe9b6c7aa, 0xd62f105d, 0x02441453, 0xd8a1e681, 0xe7d3fbc8,
-    0x21e1cde6, 0xc33707d6, 0xf4d50d87, 0x455a14ed, 0xa9e3e905, 0xfcefa3f8, 0x676f02d9, 0x8d2a4c8a,
-    0xfffa3942, 0x8771f681, 0x6d9d6122, 0xfde5380c, 0xa4beea44, 0x4bdecfa9, 0xf6bb4b60, 0xbebfbc70,
-    0x289b7ec6, 0xeaa127fa, 0xd4ef3085, 0x04881d05, 0xd9d4d039, 0xe6db99e5, 0x1fa27cf8, 0xc4ac5665,
-    0xf4292244, 0x432aff97, 0xab9423a7, 0xfc93a039, 0x655b59c3, 0x8f0ccc92, 0xffeff47d, 0x85845dd1,
-    0x6fa87e4f, 0xfe2ce6e0, 0xa3014314, 0x4e0811a1, 0xf7537e82, 0xbd3af235, 0x2ad7d2bb, 0xeb86d391};
-static const int kMd5S[4][4] = {{7, 12, 17, 22}, {5, 9, 14, 20}, {4, 11, 16, 23}, {6, 10, 15, 21}};
+
+// Fully unrolled compression: the round functions use the shortest
+// dependent forms (z ^ (x & (y ^ z)) etc.) so one core runs the serial
+// chain of a whole-file hash as fast as plain C allows.
+#define HM_F(x, y, z) ((z) ^ ((x) & ((y) ^ (z))))
+#define HM_G(x, y, z) ((y) ^ ((z) & ((x) ^ (y))))
+#define HM_H(x, y, z) ((x) ^ (y) ^ (z))
+#define HM_I(x, y, z) ((y) ^ ((x) | ~(z)))
+#define HM_STEP(f, a, b, c, d, x, t, s) \
+    (a) += f((b), (c), (d)) + (x) + (t); \
+    (a) = rol((a), (s)) + (b);
 
 static void md5_block(uint32_t st[4], const uint8_t* p) {
     uint32_t m[16];
-    for (int i = 0; i < 16; ++i)
-        m[i] = (uint32_t)p[4 * i] | ((uint32_t)p[4 * i + 1] << 8) | ((uint32_t)p[4 * i + 2] << 16) |
-               ((uint32_t)p[4 * i + 3] << 24);
+    memcpy(m, p, 64);  // little-endian host
     uint32_t a = st[0], b = st[1], c = st[2], d = st[3];
-    for (int i = 0; i < 64; ++i) {
-        const int round = i / 16;
-        uint32_t f;
-        int g;
-        switch (round) {
-        case 0: f = (b & c) | (~b & d); g = i; break;
-        case 1: f = (b & d) | (c & ~d); g = (5 * i + 1) & 15; break;
-        case 2: f = b ^ c ^ d; g = (3 * i + 5) & 15; break;
-        default: f = c ^ (b | ~d); g = (7 * i) & 15; break;
-        }
-        const uint32_t tmp = d;
-        d = c;
-        c = b;
-        b = b + rol(a + f + kMd5T[i] + m[g], kMd5S[round][i & 3]);
-        a = tmp;
-    }
+    HM_STEP(HM_F, a, b, c, d, m[0], 0xd76aa478, 7) HM_STEP(HM_F, d, a, b, c, m[1], 0xe8c7b756, 12)
+    HM_STEP(HM_F, c, d, a, b, m[2], 0x242070db, 17) HM_STEP(HM_F, b, c, d, a, m[3], 0xc1bdceee, 22)
+    HM_STEP(HM_F, a, b, c, d, m[4], 0xf57c0faf, 7) HM_STEP(HM_F, d, a, b, c, m[5], 0x4787c62a, 12)
+    HM_STEP(HM_F, c, d, a, b, m[6], 0xa8304613, 17) HM_STEP(HM_F, b, c, d, a, m[7], 0xfd469501, 22)
+    HM_STEP(HM_F, a, b, c, d, m[8], 0x698098d8, 7) HM_STEP(HM_F, d, a, b, c, m[9], 0x8b44f7af, 12)
+    HM_STEP(HM_F, c, d, a, b, m[10], 0xffff5bb1, 17) HM_STEP(HM_F, b, c, d, a, m[11], 0x895cd7be, 22)
+    HM_STEP(HM_F, a, b, c, d, m[12], 0x6b901122, 7) HM_STEP(HM_F, d, a, b, c, m[13], 0xfd987193, 12)
+    HM_STEP(HM_F, c, d, a, b, m[14], 0xa679438e, 17) HM_STEP(HM_F, b, c, d, a, m[15], 0x49b40821, 22)
+    HM_STEP(HM_G, a, b, c, d, m[1], 0xf61e2562, 5) HM_STEP(HM_G, d, a, b, c, m[6], 0xc040b340, 9)
+    HM_STEP(HM_G, c, d, a, b, m[11], 0x265e5a51, 14) HM_STEP(HM_G, b, c, d, a, m[0], 0xe9b6c7aa, 20)
+    HM_STEP(HM_G, a, b, c, d, m[5], 0xd62f105d, 5) HM_STEP(HM_G, d, a, b, c, m[10], 0x02441453, 9)
+    HM_STEP(HM_G, c, d, a, b, m[15], 0xd8a1e681, 14) HM_STEP(HM_G, b, c, d, a, m[4], 0xe7d3fbc8, 20)
+    HM_STEP(HM_G, a, b, c, d, m[9], 0x21e1cde6, 5) HM_STEP(HM_G, d, a, b, c, m[14], 0xc33707d6, 9)
+    HM_STEP(HM_G, c, d, a, b, m[3], 0xf4d50d87, 14) HM_STEP(HM_G, b, c, d, a, m[8], 0x455a14ed, 20)
+    HM_STEP(HM_G, a, b, c, d, m[13], 0xa9e3e905, 5) HM_STEP(HM_G, d, a, b, c, m[2], 0xfcefa3f8, 9)
+    HM_STEP(HM_G, c, d, a, b, m[7], 0x676f02d9, 14) HM_STEP(HM_G, b, c, d, a, m[12], 0x8d2a4c8a, 20)
+    HM_STEP(HM_H, a, b, c, d, m[5], 0xfffa3942, 4) HM_STEP(HM_H, d, a, b, c, m[8], 0x8771f681, 11)
+    HM_STEP(HM_H, c, d, a, b, m[11], 0x6d9d6122, 16) HM_STEP(HM_H, b, c, d, a, m[14], 0xfde5380c, 23)
+    HM_STEP(HM_H, a, b, c, d, m[1], 0xa4beea44, 4) HM_STEP(HM_H, d, a, b, c, m[4], 0x4bdecfa9, 11)
+    HM_STEP(HM_H, c, d, a, b, m[7], 0xf6bb4b60, 16) HM_STEP(HM_H, b, c, d, a, m[10], 0xbebfbc70, 23)
+    HM_STEP(HM_H, a, b, c, d, m[13], 0x289b7ec6, 4) HM_STEP(HM_H, d, a, b, c, m[0], 0xeaa127fa, 11)
+    HM_STEP(HM_H, c, d, a, b, m[3], 0xd4ef3085, 16) HM_STEP(HM_H, b, c, d, a, m[6], 0x04881d05, 23)
+    HM_STEP(HM_H, a, b, c, d, m[9], 0xd9d4d039, 4) HM_STEP(HM_H, d, a, b, c, m[12], 0xe6db99e5, 11)
+    HM_STEP(HM_H, c, d, a, b, m[15], 0x1fa27cf8, 16) HM_STEP(HM_H, b, c, d, a, m[2], 0xc4ac5665, 23)
+    HM_STEP(HM_I, a, b, c, d, m[0], 0xf4292244, 6) HM_STEP(HM_I, d, a, b, c, m[7], 0x432aff97, 10)
+    HM_STEP(HM_I, c, d, a, b, m[14], 0xab9423a7, 15) HM_STEP(HM_I, b, c, d, a, m[5], 0xfc93a039, 21)
+    HM_STEP(HM_I, a, b, c, d, m[12], 0x655b59c3, 6) HM_STEP(HM_I, d, a, b, c, m[3], 0x8f0ccc92, 10)
+    HM_STEP(HM_I, c, d, a, b, m[10], 0xffeff47d, 15) HM_STEP(HM_I, b, c, d, a, m[1], 0x85845dd1, 21)
+    HM_STEP(HM_I, a, b, c, d, m[8], 0x6fa87e4f, 6) HM_STEP(HM_I, d, a, b, c, m[15], 0xfe2ce6e0, 10)
+    HM_STEP(HM_I, c, d, a, b, m[6], 0xa3014314, 15) HM_STEP(HM_I, b, c, d, a, m[13], 0x4e0811a1, 21)
+    HM_STEP(HM_I, a, b, c, d, m[4], 0xf7537e82, 6) HM_STEP(HM_I, d, a, b, c, m[11], 0xbd3af235, 10)
+    HM_STEP(HM_I, c, d, a, b, m[2], 0x2ad7d2bb, 15) HM_STEP(HM_I, b, c, d, a, m[9], 0xeb86d391, 21)
     st[0] += a;
     st[1] += b;
     st[2] += c;

@@ -11,6 +11,7 @@
 //
 // GF(2^16) arithmetic follows src/galois.rs: polynomial 0x1100B, generator
 // 2, symbols are little-endian u16 pairs of bytes.
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <vector>
@@ -105,6 +106,12 @@ __device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
+// x*m + y as one IMAD (m a run-time value keeps ptxas from rewriting it)
+__device__ __forceinline__ uint32_t mad1(uint32_t x, uint32_t m, uint32_t y) {
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(m), "r"(y));
+    return r;
+}
 __device__ __forceinline__ uint4 lds128(uint32_t addr) {
     uint4 v;
     asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
@@ -125,8 +132,10 @@ __device__ __forceinline__ uint32_t lds32(uint32_t addr) {
 // Coefficient basis.  c(r,s) = base_s^(first_exp+r) = 2^(logbase_s*(first_exp+r)
 // mod 65535) (RsEncoder::coefficient + gf_pow, src/reedsolomon.rs:56-60,
 // src/galois.rs:74-87); the basis entry j is c*2^j = antilog[log c + j].
-// Layout [s][rg][j][32 rows] u16: one contiguous 1 KiB block per (s, rg).
-// Rows r >= R get 0 (their tables are all-zero and never stored).
+// Layout [s][rg][jj][hi][32 rows] u16 (j = 8*hi + jj): one contiguous 1 KiB
+// block per (s, rg), ordered so that a warp's basis loads in the table build
+// (lane = row pair + 16*hi) hit 32 distinct banks.  Rows r >= R get 0 (their
+// tables are all-zero and never stored).
 // ---------------------------------------------------------------------------
 __global__ void basis_kernel(uint16_t* __restrict__ basis, uint32_t S, uint32_t RG, uint32_t R,
                              uint32_t first_exp) {
@@ -134,7 +143,9 @@ __global__ void basis_kernel(uint16_t* __restrict__ basis, uint32_t S, uint32_t 
     for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t rl = (uint32_t)(idx & 31);
-        const uint32_t j = (uint32_t)((idx >> 5) & 15);
+        const uint32_t hi = (uint32_t)((idx >> 5) & 1);
+        const uint32_t jj = (uint32_t)((idx >> 6) & 7);
+        const uint32_t j = 8 * hi + jj;
         const uint64_t sg = idx >> 9;
         const uint32_t rg = (uint32_t)(sg % RG);
         const uint32_t s = (uint32_t)(sg / RG);
@@ -174,6 +185,7 @@ __global__ void basis_kernel(uint16_t* __restrict__ basis, uint32_t S, uint32_t 
 // separates table builds (double-buffered) from lookups.
 // ---------------------------------------------------------------------------
 constexpr int kTabBytes = 256 * 128;
+__device__ uint32_t d_row_bytes = 128;
 
 __host__ __device__ constexpr int ctz5(int u) {
     return (u & 1) ? 0 : (u & 2) ? 1 : (u & 4) ? 2 : (u & 8) ? 3 : 4;
@@ -188,10 +200,11 @@ __host__ __device__ constexpr size_t encode_smem_bytes() {
 template <int NCH>
 __global__ void __launch_bounds__(kEncThreads, 1)
     encode_lut_kernel(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S,
-                      const uint16_t* __restrict__ basis, uint32_t RG, uint32_t R, uint32_t Np,
-                      uint8_t* __restrict__ rec, uint64_t rec_stride, int* __restrict__ err) {
+                      const uint16_t* __restrict__ basis, uint32_t RG, uint32_t R, uint32_t sym_begin,
+                      uint32_t sym_end, uint32_t TS, uint8_t* __restrict__ rec, uint64_t rec_stride,
+                      int* __restrict__ err) {
     constexpr int WARPS = kEncThreads / 32;
-    constexpr int NT = WARPS * NCH * 64;  // symbols per tile
+    constexpr int NT = WARPS * NCH * 64;  // symbol capacity of a tile (TS <= NT)
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* tabs = smem;
     uint8_t* src_st = smem + 2 * kTabBytes;
@@ -200,8 +213,9 @@ __global__ void __launch_bounds__(kEncThreads, 1)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x / RG, rg = blockIdx.x % RG;
-    const uint32_t n0 = tile * NT;
-    const uint32_t tile_syms = min((uint32_t)NT, Np - n0);
+    const uint32_t n0 = sym_begin + tile * TS;
+    if (n0 >= sym_end) return;  // uniform: empty tile at the end of a band
+    const uint32_t tile_syms = min(TS, sym_end - n0);
     const uint32_t tile_bytes = tile_syms * 2;
 
     if (tid == 0) {
@@ -219,21 +233,28 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     if (tid == 0)
         for (int st = 0; st < kEncStages && (uint32_t)st < S; ++st) issue(st, st);
 
-    // Table build: thread (word column wc = lane, v-block = warp) writes the
-    // 32 entries v = 32*warp + u of its column with a Gray-code walk.
+    // Table build: the 256 table rows are 16 blocks of 16; warp w builds
+    // blocks w, w+WARPS, ...  Thread (word column wc = lane) writes the 16
+    // entries v = 16*block + u of its column with a Gray-code walk over the
+    // low 4 bits of v; the high 4 bits select the starting XOR.
     const uint32_t bas_u32 = smem_u32(bas_st), tab_u32 = smem_u32(tabs);
     auto build = [&](int t, int st) {
         const int p = lane & 15, h = lane >> 4;
         uint32_t b[8];
 #pragma unroll
-        for (int jj = 0; jj < 8; ++jj) b[jj] = lds32(bas_u32 + st * 1024 + ((8 * h + jj) * 16 + p) * 4);
-        uint32_t e = ((warp & 1) ? b[5] : 0u) ^ ((warp & 2) ? b[6] : 0u) ^ ((warp & 4) ? b[7] : 0u);
-        const uint32_t row0 = tab_u32 + t * kTabBytes + (uint32_t)(warp * 32) * 128 + lane * 4;
-        sts32(row0, e);
+        for (int jj = 0; jj < 8; ++jj) b[jj] = lds32(bas_u32 + st * 1024 + (jj * 32 + h * 16 + p) * 4);
+        for (int blk = warp; blk < 16; blk += WARPS) {
+            uint32_t e = 0;
 #pragma unroll
-        for (int u = 1; u < 32; ++u) {
-            e ^= b[ctz5(u)];
-            sts32(row0 + (uint32_t)(u ^ (u >> 1)) * 128, e);
+            for (int jj = 4; jj < 8; ++jj)
+                if ((blk >> (jj - 4)) & 1) e ^= b[jj];
+            const uint32_t row0 = tab_u32 + t * kTabBytes + (uint32_t)(blk * 16) * 128 + lane * 4;
+            sts32(row0, e);
+#pragma unroll
+            for (int u = 1; u < 16; ++u) {
+                e ^= b[ctz5(u)];
+                sts32(row0 + (uint32_t)(u ^ (u >> 1)) * 128, e);
+            }
         }
     };
 
@@ -243,6 +264,9 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     const uint32_t selA0 = odd ? 0x4441u : 0x4440u, selB0 = odd ? 0x4440u : 0x4441u;
     const uint32_t selA1 = odd ? 0x4443u : 0x4442u, selB1 = odd ? 0x4442u : 0x4443u;
     const uint32_t src_u32 = smem_u32(src_st) + (uint32_t)(warp * NCH * 8 + g) * 16;
+    // 128 = bytes per table row; read at run time so the address multiply-add
+    // stays an IMAD (FMA pipe) instead of integer-ALU shift+add
+    const uint32_t row_bytes = *reinterpret_cast<volatile const uint32_t*>(&d_row_bytes);
 
     uint32_t acc[NCH][8][4];
 #pragma unroll
@@ -278,6 +302,7 @@ __global__ void __launch_bounds__(kEncThreads, 1)
         const uint32_t sbase = src_u32 + st * NT * 2;
 #pragma unroll
         for (int j = 0; j < NCH; ++j) {
+            if ((uint32_t)(warp * NCH * 8 + j * 8 + g) * 8 >= tile_syms) continue;  // chunk outside the tile
             const uint4 w4 = lds128(sbase + j * 128);
             const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
@@ -286,8 +311,8 @@ __global__ void __launch_bounds__(kEncThreads, 1)
                 for (int hh = 0; hh < 2; ++hh) {
                     const uint32_t bA = __byte_perm(ws[m], 0u, hh ? selA1 : selA0);
                     const uint32_t bB = __byte_perm(ws[m], 0u, hh ? selB1 : selB0);
-                    const uint4 A = lds128(baseA + (bA << 7));
-                    const uint4 B = lds128(baseB + (bB << 7));
+                    const uint4 A = lds128(mad1(bA, row_bytes, baseA));
+                    const uint4 B = lds128(mad1(bB, row_bytes, baseB));
                     const int i = 2 * m + hh;
                     acc[j][i][0] ^= A.x ^ B.x;
                     acc[j][i][1] ^= A.y ^ B.y;
@@ -314,7 +339,7 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     for (int j = 0; j < NCH; ++j) {
         const uint32_t chunk = (uint32_t)(warp * NCH * 8 + j * 8 + g);
         const uint32_t n = n0 + chunk * 8;
-        if (n < Np) {
+        if (chunk * 8 < tile_syms) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const uint32_t re = rg * kRowsPerGroup + 8 * k + 2 * q;
@@ -493,50 +518,164 @@ __device__ uint32_t md5_stream_word(const uint32_t* pre, uint32_t pre_bytes, con
     return w;
 }
 
+// Blocks [b_from, b_to) of the padded message prefix ‖ data.
 template <bool VEC>
-__device__ void md5_stream(uint32_t st[4], const uint32_t* pre, uint32_t pre_bytes, const uint8_t* data,
-                           uint64_t len) {
-    st[0] = 0x67452301u;
-    st[1] = 0xefcdab89u;
-    st[2] = 0x98badcfeu;
-    st[3] = 0x10325476u;
+__device__ void md5_range(uint32_t st[4], const uint32_t* pre, uint32_t pre_bytes, const uint8_t* data, uint64_t len,
+                          uint64_t b_from, uint64_t b_to) {
     const uint64_t total = pre_bytes + len;
     const uint64_t nblocks = (total + 8) / 64 + 1;
     const uint64_t last_start = (nblocks - 1) * 64;
     const uint64_t fb0 = (pre_bytes + 63) / 64;  // first block wholly after the prefix
     const uint64_t fb1 = total / 64;             // blocks below this hold no padding
-    uint64_t b = 0;
+    if (b_to > nblocks) b_to = nblocks;
+    uint64_t b = b_from;
     uint32_t m[16];
-    for (; b < fb0 && b < nblocks; ++b) {
+    for (; b < fb0 && b < b_to; ++b) {
 #pragma unroll
         for (int i = 0; i < 16; ++i) m[i] = md5_stream_word(pre, pre_bytes, data, len, total, last_start, 64 * b + 4 * i);
         md5_compress(st, m);
     }
-    if (b < fb1) {
+    const uint64_t fast_end = fb1 < b_to ? fb1 : b_to;
+    if (b < fast_end) {
         md5_load_block<VEC>(m, data + 64 * b - pre_bytes);
-        for (; b < fb1; ++b) {
+        for (; b < fast_end; ++b) {
             uint32_t nx[16];
-            const uint64_t nb = b + 1 < fb1 ? b + 1 : b;
+            const uint64_t nb = b + 1 < fast_end ? b + 1 : b;
             md5_load_block<VEC>(nx, data + 64 * nb - pre_bytes);
             md5_compress(st, m);
 #pragma unroll
             for (int i = 0; i < 16; ++i) m[i] = nx[i];
         }
     }
-    for (; b < nblocks; ++b) {
+    for (; b < b_to; ++b) {
 #pragma unroll
         for (int i = 0; i < 16; ++i) m[i] = md5_stream_word(pre, pre_bytes, data, len, total, last_start, 64 * b + 4 * i);
         md5_compress(st, m);
     }
 }
 
+__device__ __forceinline__ void md5_init(uint32_t st[4]) {
+    st[0] = 0x67452301u;
+    st[1] = 0xefcdab89u;
+    st[2] = 0x98badcfeu;
+    st[3] = 0x10325476u;
+}
+
 template <bool VEC>
-__global__ void md5_slices_kernel(const uint8_t* __restrict__ src, uint64_t stride, uint32_t count,
-                                  uint64_t slice_size, p2g_slice_checksum* __restrict__ out) {
+__device__ void md5_stream(uint32_t st[4], const uint32_t* pre, uint32_t pre_bytes, const uint8_t* data,
+                           uint64_t len) {
+    md5_init(st);
+    md5_range<VEC>(st, pre, pre_bytes, data, len, 0, ~0ull);
+}
+
+// ---------------------------------------------------------------------------
+// Staged MD5 streams.  With 32 lanes of a warp each hashing a different
+// stream, direct global loads leave every block waiting on 32 scattered
+// cache lines.  Instead each lane pulls its stream through a private ring of
+// kRingUnits 64-byte units in shared memory with cp.async, kRingAhead units
+// ahead of the block being compressed, and reads message words back with
+// 128-bit shared loads.  PW = prefix words (the message is PW prefix words
+// ‖ data); data must be 16-byte aligned when VEC (else 4-byte copies).
+// Blocks that contain prefix words, padding, or data past the last whole
+// copy unit take the direct (generic) path.
+// ---------------------------------------------------------------------------
+constexpr int kHashThreads = 256;  // 8 warps: two MD5 warps per SM sub-partition keep full chain speed
+constexpr int kRingUnits = 8;
+constexpr int kRingAhead = 4;
+constexpr int kRingLaneBytes = kRingUnits * 64 + 16;  // +16: lanes land on distinct bank groups
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int PW, bool VEC>
+__device__ void md5_range_ring(uint32_t st[4], const uint32_t* pre, const uint8_t* data, uint64_t len,
+                               uint64_t b_from, uint64_t b_to, uint32_t ring) {
+    constexpr uint32_t pre_bytes = 4 * PW;
+    constexpr int SH = (4 - (PW & 3)) & 3;  // word offset of a block's first word in its aligned quad
+    constexpr int NQ = SH ? 5 : 4;          // quads touched per block
+    const uint64_t total = pre_bytes + len;
+    const uint64_t nblocks = (total + 8) / 64 + 1;
+    const uint64_t last_start = (nblocks - 1) * 64;
+    if (b_to > nblocks) b_to = nblocks;
+    // whole 64-byte units that can go through the ring
+    const uint64_t fetch_bytes = VEC ? (len & ~15ull) : (len & ~3ull);
+    const uint64_t n_units = fetch_bytes / 64;
+    // ring-eligible blocks: no prefix word, all data words inside whole units
+    const uint64_t rb0 = (pre_bytes + 63) / 64;
+    const uint64_t rb1 = n_units * 16 >= 16 - PW ? (n_units * 16 + PW) / 16 : 0;  // blocks b with 16b+16-PW <= 16*n_units
+    uint64_t b = b_from;
+    uint32_t m[16];
+    auto generic = [&](uint64_t blk) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) m[i] = md5_stream_word(pre, pre_bytes, data, len, total, last_start, 64 * blk + 4 * i);
+        md5_compress(st, m);
+    };
+    for (; b < b_to && (b < rb0 || b >= rb1); ++b) generic(b);
+    const uint64_t fast_end = rb1 < b_to ? rb1 : b_to;
+    if (b < fast_end) {
+        auto fetch = [&](uint64_t u) {  // one unit = one commit group (possibly empty)
+            if (u < n_units) {
+                const uint8_t* g = data + 64 * u;
+                const uint32_t d = ring + (uint32_t)(u % kRingUnits) * 64;
+                if (VEC) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) cp_async16(d + 16 * q, g + 16 * q);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) cp_async4(d + 4 * q, g + 4 * q);
+                }
+            }
+            cp_async_commit();
+        };
+        // units of block b: [lo(b), hi(b)] with hi(b) = floor((16b + 15 - PW) / 16)
+        const uint64_t first_w = 16 * b - PW;
+        const uint64_t u_lo = first_w / 16;
+        const uint64_t u_hi0 = (first_w + 15) / 16;
+        for (uint64_t u = u_lo; u < u_hi0 + kRingAhead; ++u) fetch(u);
+        for (; b < fast_end; ++b) {
+            const uint64_t u_hi = (16 * b + 15 - PW) / 16;
+            fetch(u_hi + kRingAhead);
+            cp_async_wait<kRingAhead>();
+            const uint64_t w0 = (16 * b - PW) & ~3ull;  // aligned quad holding the first word
+            uint32_t q[NQ * 4];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) {
+                const uint32_t widx = (uint32_t)((w0 + 4 * i) % (16 * kRingUnits));
+                const uint4 v = lds128(ring + widx * 4);
+                q[4 * i] = v.x;
+                q[4 * i + 1] = v.y;
+                q[4 * i + 2] = v.z;
+                q[4 * i + 3] = v.w;
+            }
+#pragma unroll
+            for (int i = 0; i < 16; ++i) m[i] = q[SH + i];
+            md5_compress(st, m);
+        }
+        cp_async_wait<0>();
+    }
+    for (; b < b_to; ++b) generic(b);
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(kHashThreads) md5_slices_kernel(const uint8_t* __restrict__ src, uint64_t stride,
+                                                                  uint32_t count, uint64_t slice_size,
+                                                                  p2g_slice_checksum* __restrict__ out) {
+    extern __shared__ __align__(16) uint8_t ring[];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     uint32_t st[4];
-    md5_stream<VEC>(st, nullptr, 0, src + (size_t)i * stride, slice_size);
+    md5_init(st);
+    md5_range_ring<0, VEC>(st, nullptr, src + (size_t)i * stride, slice_size, 0, ~0ull,
+                           smem_u32(ring) + threadIdx.x * kRingLaneBytes);
     uint32_t* o = reinterpret_cast<uint32_t*>(&out[i]);
     o[0] = st[0];
     o[1] = st[1];
@@ -545,13 +684,17 @@ __global__ void md5_slices_kernel(const uint8_t* __restrict__ src, uint64_t stri
 }
 
 template <bool VEC>
-__global__ void md5_files_kernel(const uint8_t* __restrict__ base, const FileSpan* __restrict__ spans,
-                                 uint32_t n, uint8_t* __restrict__ out16) {
+__global__ void __launch_bounds__(kHashThreads) md5_files_kernel(const uint8_t* __restrict__ base,
+                                                                 const FileSpan* __restrict__ spans, uint32_t n,
+                                                                 uint8_t* __restrict__ out16) {
+    extern __shared__ __align__(16) uint8_t ring[];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t st[4];
     const FileSpan sp = spans[i];
-    md5_stream<VEC>(st, nullptr, 0, base + sp.offset, sp.length);
+    md5_init(st);
+    md5_range_ring<0, VEC>(st, nullptr, base + sp.offset, sp.length, 0, ~0ull,
+                           smem_u32(ring) + threadIdx.x * kRingLaneBytes);
     uint32_t* o = reinterpret_cast<uint32_t*>(out16 + 16 * (size_t)i);
     o[0] = st[0];
     o[1] = st[1];
@@ -563,7 +706,8 @@ struct RecvPrefix {
     uint32_t w[8];  // set_id ‖ "PAR 2.0\0RecvSlic"
 };
 
-__global__ void md5_recovery_kernel(const uint8_t* __restrict__ rec, uint64_t stride, uint32_t count,
+template <bool VEC>
+__global__ void __launch_bounds__(kHashThreads) md5_recovery_kernel(const uint8_t* __restrict__ rec, uint64_t stride, uint32_t count,
                                     uint64_t slice_size, RecvPrefix pfx, uint32_t first_exp,
                                     uint8_t* __restrict__ out16) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -572,13 +716,54 @@ __global__ void md5_recovery_kernel(const uint8_t* __restrict__ rec, uint64_t st
 #pragma unroll
     for (int i = 0; i < 8; ++i) pre[i] = pfx.w[i];
     pre[8] = first_exp + r;  // exponent as le32 (src/packet/recovery.rs:15)
+    extern __shared__ __align__(16) uint8_t ring[];
     uint32_t st[4];
-    md5_stream<false>(st, pre, 36, rec + (size_t)r * stride, slice_size);
+    md5_init(st);
+    md5_range_ring<9, VEC>(st, pre, rec + (size_t)r * stride, slice_size, 0, ~0ull,
+                            smem_u32(ring) + threadIdx.x * kRingLaneBytes);
     uint32_t* o = reinterpret_cast<uint32_t*>(out16 + 16 * (size_t)r);
     o[0] = st[0];
     o[1] = st[1];
     o[2] = st[2];
     o[3] = st[3];
+}
+
+// Continuation form: blocks [b_from, b_to) of each row's packet message,
+// with the chain state kept in `state` (4 words per row) between calls.
+// b_from == 0 starts a chain; `final` writes the digest instead of the state.
+template <bool VEC>
+__global__ void __launch_bounds__(kHashThreads) md5_recovery_range_kernel(const uint8_t* __restrict__ rec, uint64_t stride, uint32_t count,
+                                          uint64_t slice_size, RecvPrefix pfx, uint32_t first_exp,
+                                          uint32_t* __restrict__ state, uint64_t b_from, uint64_t b_to, int final,
+                                          uint8_t* __restrict__ out16) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= count) return;
+    uint32_t pre[9];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) pre[i] = pfx.w[i];
+    pre[8] = first_exp + r;
+    extern __shared__ __align__(16) uint8_t ring[];
+    uint32_t st[4];
+    if (b_from == 0) {
+        md5_init(st);
+    } else {
+        const uint4 v = reinterpret_cast<const uint4*>(state)[r];
+        st[0] = v.x;
+        st[1] = v.y;
+        st[2] = v.z;
+        st[3] = v.w;
+    }
+    md5_range_ring<9, VEC>(st, pre, rec + (size_t)r * stride, slice_size, b_from, b_to,
+                            smem_u32(ring) + threadIdx.x * kRingLaneBytes);
+    if (final) {
+        uint32_t* o = reinterpret_cast<uint32_t*>(out16 + 16 * (size_t)r);
+        o[0] = st[0];
+        o[1] = st[1];
+        o[2] = st[2];
+        o[3] = st[3];
+    } else {
+        reinterpret_cast<uint4*>(state)[r] = make_uint4(st[0], st[1], st[2], st[3]);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -615,7 +800,7 @@ __device__ uint32_t x_pow_8n(uint64_t n) {
 }
 
 template <bool VEC>
-__global__ void __launch_bounds__(256) crc_slices_kernel(const uint8_t* __restrict__ src, uint64_t stride,
+__global__ void __launch_bounds__(64) crc_slices_kernel(const uint8_t* __restrict__ src, uint64_t stride,
                                                          uint32_t count, uint64_t slice_size,
                                                          p2g_slice_checksum* __restrict__ out) {
     __shared__ uint32_t T[4][256];
@@ -691,6 +876,32 @@ static int sm_count() {
     return n;
 }
 
+// Tile size for Np symbol positions and RG row groups on `sms` SMs (one CTA
+// each).  Per input slice a CTA spends about one shared-memory wavefront per
+// symbol of its tile on lookups plus a fixed ~384 on building its tables, so
+// pick the tile count minimising ceil(tiles*RG/sms) * (tile + 384): the
+// fewest, fullest waves.
+void choose_tiles(uint32_t Np, uint32_t RG, uint32_t sms, uint32_t* ts_out, uint32_t* tiles_out) {
+    constexpr uint64_t kBuildCost = 384;
+    const uint32_t tmin = (Np + kEncTileSymbols - 1) / kEncTileSymbols;
+    uint64_t best_cost = ~0ull;
+    uint32_t best_ts = kEncTileSymbols, best_t = tmin;
+    for (uint32_t t = tmin; t <= 4 * tmin + 8; ++t) {
+        const uint32_t ts = ((Np + t - 1) / t + 7) & ~7u;
+        if (ts == 0 || ts > (uint32_t)kEncTileSymbols) continue;
+        const uint32_t tt = (Np + ts - 1) / ts;
+        const uint64_t waves = ((uint64_t)tt * RG + sms - 1) / sms;
+        const uint64_t cost = waves * (ts + kBuildCost);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best_ts = ts;
+            best_t = tt;
+        }
+    }
+    *ts_out = best_ts;
+    *tiles_out = best_t;
+}
+
 cudaError_t launch_basis(uint16_t* basis, uint32_t S, uint32_t RG, uint32_t R, uint32_t first_exp,
                          cudaStream_t st) {
     const uint64_t total = (uint64_t)S * RG * 512;
@@ -702,28 +913,117 @@ cudaError_t launch_basis(uint16_t* basis, uint32_t S, uint32_t RG, uint32_t R, u
     return cudaGetLastError();
 }
 
-cudaError_t launch_encode(const uint8_t* src, uint64_t src_stride, uint32_t S, const uint16_t* basis,
-                          uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec, uint64_t rec_stride,
-                          int* err, cudaStream_t st) {
-    constexpr int NCH = kEncChunks;
-    constexpr size_t smem = encode_smem_bytes<NCH>();
+static cudaError_t encode_attr() {
+    constexpr size_t smem = encode_smem_bytes<kEncChunks>();
     static bool attr_set[256] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 256 || !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(encode_lut_kernel<NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(encode_lut_kernel<kEncChunks>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 256) attr_set[dev] = true;
     }
-    const uint32_t Np = (uint32_t)(((slice_size + 15) & ~15ull) / 2);
-    const uint32_t n_tiles = (Np + kEncTileSymbols - 1) / kEncTileSymbols;
-    const uint64_t grid = (uint64_t)n_tiles * RG;
-    if (!grid || !R) return cudaSuccess;
-    encode_lut_kernel<NCH><<<(unsigned)grid, kEncThreads, smem, st>>>(src, src_stride, S, basis, RG, R, Np, rec,
-                                                                      rec_stride, err);
+    return cudaSuccess;
+}
+
+// Band plan.  The symbol range is cut into bands of whole waves so bands
+// finish in order and the recovery-packet MD5 chains can follow band by band
+// (one SM kept free for them).  While the slice-MD5 blocks run (`reserve`
+// SMs for about `reserve_ms`), bands are sized to leave those SMs alone;
+// the plan keeps that only when it beats sharing SMs with them (which slows
+// the bands involved about twofold).  Per input slice a CTA spends ~1 shared-
+// memory wavefront per tile symbol plus ~384 on its tables; 0.78 of the peak
+// wavefront rate at ~1.9 GHz estimates band times.
+static double est_band_ms(uint32_t S, uint32_t ts, uint32_t waves) {
+    return (double)S * (ts + 384.0) * waves / (0.78 * 1.9e6);
+}
+
+static void split_even(EncodePlan& pl, uint32_t begin, uint32_t RG, uint32_t budget, double* ms, uint32_t S) {
+    if (begin >= pl.Np) return;
+    const uint32_t tiles = RG <= budget ? budget / RG : 1;
+    const uint32_t waves = RG <= budget ? 1 : (RG + budget - 1) / budget;
+    const uint64_t rem = pl.Np - begin;
+    const uint64_t per = (uint64_t)tiles * kEncTileSymbols;
+    const uint32_t B = (uint32_t)((rem + per - 1) / per);
+    const uint32_t ts = (uint32_t)(((rem + (uint64_t)B * tiles - 1) / ((uint64_t)B * tiles) + 7) & ~7ull);
+    for (uint32_t b = 0; b < B; ++b) {
+        const uint64_t s0 = begin + (uint64_t)b * tiles * ts;
+        if (s0 >= pl.Np) break;
+        const uint32_t s1 = (uint32_t)std::min<uint64_t>(pl.Np, s0 + (uint64_t)tiles * ts);
+        pl.bands.push_back({(uint32_t)s0, s1, ts});
+        if (ms) *ms += est_band_ms(S, ts, waves);
+    }
+}
+
+EncodePlan plan_encode(uint64_t slice_size, uint32_t S, uint32_t RG, bool banded, uint32_t reserve,
+                       double reserve_ms) {
+    EncodePlan pl;
+    pl.Np = (uint32_t)(((slice_size + 15) & ~15ull) / 2);
+    const uint32_t sms = (uint32_t)sm_count();
+    uint32_t ts1 = 0, t1 = 0;
+    choose_tiles(pl.Np, RG, sms, &ts1, &t1);
+    EncodePlan c = pl;  // C: one launch, packet MD5 after it
+    c.bands.push_back({0, pl.Np, ts1});
+    if (!banded || sms < 4) return c;
+    const double chain_ms_per_byte = 7.2e-4 / 64;  // one MD5 chain: ~0.72 us per 64-byte block
+    const uint32_t waves1 = (uint32_t)(((uint64_t)t1 * RG + sms - 1) / sms);
+    const double ms_c = est_band_ms(S, ts1, waves1) + 2.0 * pl.Np * chain_ms_per_byte + reserve_ms;
+    auto tail = [&](const EncodePlan& p) {  // last band's packet-MD5 step + per-band launch/drain
+        const EncodeBand& l = p.bands.back();
+        return 2.0 * (l.end - l.begin) * chain_ms_per_byte + 0.02 * p.bands.size();
+    };
+    // A: bands with one SM kept for the packet MD5; slice MD5 shares SMs
+    EncodePlan a = pl;
+    double ms_a = 0;
+    split_even(a, 0, RG, sms - 1, &ms_a, S);
+    ms_a += std::min(reserve_ms, ms_a) + tail(a);  // bands overlapping the slice MD5 run ~2x slower
+    // B: early bands leave the slice-MD5 SMs alone, later bands use them
+    EncodePlan b = pl;
+    double ms_b = 1e30;
+    if (reserve && reserve + 2 < sms) {
+        const uint32_t budget = sms - reserve - 1;
+        const uint32_t tiles = RG <= budget ? budget / RG : 1;
+        const uint32_t waves = RG <= budget ? 1 : (RG + budget - 1) / budget;
+        uint32_t sym = 0;
+        ms_b = 0;
+        while (sym < pl.Np && ms_b < reserve_ms) {
+            const uint32_t s1 = (uint32_t)std::min<uint64_t>(pl.Np, sym + (uint64_t)tiles * kEncTileSymbols);
+            b.bands.push_back({sym, s1, (uint32_t)kEncTileSymbols});
+            ms_b += est_band_ms(S, kEncTileSymbols, waves);
+            sym = s1;
+        }
+        split_even(b, sym, RG, sms - 1, &ms_b, S);
+        ms_b += tail(b);
+    }
+    const size_t kMaxBands = 64;
+    if (a.bands.size() > kMaxBands) ms_a = 1e30;
+    if (b.bands.size() > kMaxBands) ms_b = 1e30;
+    if (ms_c <= ms_a && ms_c <= ms_b) return c;
+    return ms_b < ms_a ? b : a;
+}
+
+cudaError_t launch_encode_band(const EncodePlan& pl, uint32_t band, const uint8_t* src, uint64_t src_stride,
+                               uint32_t S, const uint16_t* basis, uint32_t RG, uint32_t R, uint8_t* rec,
+                               uint64_t rec_stride, int* err, cudaStream_t st) {
+    constexpr size_t smem = encode_smem_bytes<kEncChunks>();
+    cudaError_t e = encode_attr();
+    if (e != cudaSuccess) return e;
+    if (band >= pl.bands.size() || !R) return cudaSuccess;
+    const EncodeBand& bd = pl.bands[band];
+    if (bd.begin >= bd.end) return cudaSuccess;
+    const uint32_t tiles = (bd.end - bd.begin + bd.ts - 1) / bd.ts;
+    encode_lut_kernel<kEncChunks><<<tiles * RG, kEncThreads, smem, st>>>(src, src_stride, S, basis, RG, R, bd.begin,
+                                                                         bd.end, bd.ts, rec, rec_stride, err);
     count_launch();
     return cudaGetLastError();
+}
+
+cudaError_t launch_encode(const uint8_t* src, uint64_t src_stride, uint32_t S, const uint16_t* basis,
+                          uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec, uint64_t rec_stride,
+                          int* err, cudaStream_t st) {
+    const EncodePlan pl = plan_encode(slice_size, S, RG, false, 0, 0.0);
+    return launch_encode_band(pl, 0, src, src_stride, S, basis, RG, R, rec, rec_stride, err, st);
 }
 
 cudaError_t launch_gf_mul_xor(uint16_t coeff, const uint8_t* in, uint8_t* out, size_t len, cudaStream_t st) {
@@ -736,15 +1036,52 @@ cudaError_t launch_gf_mul_xor(uint16_t coeff, const uint8_t* in, uint8_t* out, s
     return cudaGetLastError();
 }
 
+// Hash blocks run long serial chains; any long-running warp sharing an SM
+// with an encode CTA slows that CTA (its per-slice barrier waits for the
+// slowest warp) and with it the whole band.  So hash blocks claim almost all
+// of an SM's shared memory: nothing else can be resident beside them.
+static int exclusive_smem() {
+    static int v = 0;
+    if (!v) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (v <= 0) v = 48 * 1024;
+    }
+    return v;
+}
+template <class K>
+static cudaError_t allow_exclusive(K kernel) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, exclusive_smem());
+}
+struct HashGrid {
+    unsigned blocks, threads;
+    size_t smem;
+};
+static HashGrid hash_grid(uint32_t streams) {
+    const unsigned warps = (streams + 31) / 32;
+    const unsigned wpb = warps < (unsigned)(kHashThreads / 32) ? warps : (unsigned)(kHashThreads / 32);
+    HashGrid g;
+    g.threads = wpb * 32;
+    g.blocks = (streams + g.threads - 1) / g.threads;
+    g.smem = (size_t)exclusive_smem();
+    return g;
+}
+uint32_t hash_blocks(uint32_t streams) { return streams ? hash_grid(streams).blocks : 0; }
+
 cudaError_t launch_md5_slices(const uint8_t* src, uint64_t stride, uint32_t count, uint64_t slice_size,
                               p2g_slice_checksum* out, cudaStream_t st) {
     if (!count) return cudaSuccess;
-    const unsigned tpb = 64, blocks = (count + tpb - 1) / tpb;
+    const HashGrid g = hash_grid(count);
     const bool vec = ((uintptr_t)src % 16 == 0) && (stride % 16 == 0);
-    if (vec)
-        md5_slices_kernel<true><<<blocks, tpb, 0, st>>>(src, stride, count, slice_size, out);
-    else
-        md5_slices_kernel<false><<<blocks, tpb, 0, st>>>(src, stride, count, slice_size, out);
+    cudaError_t e;
+    if (vec) {
+        if ((e = allow_exclusive(md5_slices_kernel<true>)) != cudaSuccess) return e;
+        md5_slices_kernel<true><<<g.blocks, g.threads, g.smem, st>>>(src, stride, count, slice_size, out);
+    } else {
+        if ((e = allow_exclusive(md5_slices_kernel<false>)) != cudaSuccess) return e;
+        md5_slices_kernel<false><<<g.blocks, g.threads, g.smem, st>>>(src, stride, count, slice_size, out);
+    }
     count_launch();
     return cudaGetLastError();
 }
@@ -752,7 +1089,7 @@ cudaError_t launch_md5_slices(const uint8_t* src, uint64_t stride, uint32_t coun
 cudaError_t launch_crc_slices(const uint8_t* src, uint64_t stride, uint32_t count, uint64_t slice_size,
                               p2g_slice_checksum* out, cudaStream_t st) {
     if (!count) return cudaSuccess;
-    const unsigned tpb = 256, wpb = tpb / 32;
+    const unsigned tpb = 64, wpb = tpb / 32;
     const uint64_t want = (count + wpb - 1) / wpb;
     const unsigned blocks = (unsigned)(want < (uint64_t)sm_count() * 8 ? want : (uint64_t)sm_count() * 8);
     const bool vec = ((uintptr_t)src % 16 == 0) && (stride % 16 == 0) && (slice_size % 16 == 0);
@@ -767,18 +1104,16 @@ cudaError_t launch_crc_slices(const uint8_t* src, uint64_t stride, uint32_t coun
 cudaError_t launch_md5_files(const uint8_t* base, const FileSpan* spans, uint32_t n, uint8_t* out16,
                              cudaStream_t st) {
     if (!n) return cudaSuccess;
-    const unsigned tpb = 64, blocks = (n + tpb - 1) / tpb;
-    // spans are device memory; the vector path is chosen by the caller-visible
-    // guarantee that every file starts 16-byte aligned (checked on the host side
-    // through `base`), so use the 4-byte path unless base alignment allows.
-    md5_files_kernel<false><<<blocks, tpb, 0, st>>>(base, spans, n, out16);
+    const HashGrid g = hash_grid(n);
+    cudaError_t e = allow_exclusive(md5_files_kernel<false>);
+    if (e != cudaSuccess) return e;
+    // file starts are only known to be 4-byte aligned: 4-byte ring copies
+    md5_files_kernel<false><<<g.blocks, g.threads, g.smem, st>>>(base, spans, n, out16);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_md5_recovery(const uint8_t* rec, uint64_t stride, uint32_t count, uint64_t slice_size,
-                                const uint8_t set_id[16], uint32_t first_exp, uint8_t* out16, cudaStream_t st) {
-    if (!count) return cudaSuccess;
+static RecvPrefix recv_prefix(const uint8_t set_id[16]) {
     RecvPrefix pfx;
     static const uint8_t kType[16] = {'P', 'A', 'R', ' ', '2', '.', '0', 0, 'R', 'e', 'c', 'v', 'S', 'l', 'i', 'c'};
     uint8_t raw[32];
@@ -787,8 +1122,43 @@ cudaError_t launch_md5_recovery(const uint8_t* rec, uint64_t stride, uint32_t co
     for (int i = 0; i < 8; ++i)
         pfx.w[i] = (uint32_t)raw[4 * i] | ((uint32_t)raw[4 * i + 1] << 8) | ((uint32_t)raw[4 * i + 2] << 16) |
                    ((uint32_t)raw[4 * i + 3] << 24);
-    const unsigned tpb = 32, blocks = (count + tpb - 1) / tpb;
-    md5_recovery_kernel<<<blocks, tpb, 0, st>>>(rec, stride, count, slice_size, pfx, first_exp, out16);
+    return pfx;
+}
+
+cudaError_t launch_md5_recovery(const uint8_t* rec, uint64_t stride, uint32_t count, uint64_t slice_size,
+                                const uint8_t set_id[16], uint32_t first_exp, uint8_t* out16, cudaStream_t st) {
+    if (!count) return cudaSuccess;
+    const HashGrid g = hash_grid(count);
+    cudaError_t e;
+    // 16-byte ring copies only when every row starts 16-byte aligned
+    if ((uintptr_t)rec % 16 == 0 && stride % 16 == 0) {
+        if ((e = allow_exclusive(md5_recovery_kernel<true>)) != cudaSuccess) return e;
+        md5_recovery_kernel<true><<<g.blocks, g.threads, g.smem, st>>>(rec, stride, count, slice_size,
+                                                                        recv_prefix(set_id), first_exp, out16);
+    } else {
+        if ((e = allow_exclusive(md5_recovery_kernel<false>)) != cudaSuccess) return e;
+        md5_recovery_kernel<false><<<g.blocks, g.threads, g.smem, st>>>(rec, stride, count, slice_size,
+                                                                         recv_prefix(set_id), first_exp, out16);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_md5_recovery_range(const uint8_t* rec, uint64_t stride, uint32_t count, uint64_t slice_size,
+                                      const uint8_t set_id[16], uint32_t first_exp, uint32_t* state,
+                                      uint64_t b_from, uint64_t b_to, bool final, uint8_t* out16, cudaStream_t st) {
+    if (!count || (b_from >= b_to && !final)) return cudaSuccess;
+    const HashGrid g = hash_grid(count);
+    cudaError_t e;
+    if ((uintptr_t)rec % 16 == 0 && stride % 16 == 0) {
+        if ((e = allow_exclusive(md5_recovery_range_kernel<true>)) != cudaSuccess) return e;
+        md5_recovery_range_kernel<true><<<g.blocks, g.threads, g.smem, st>>>(
+            rec, stride, count, slice_size, recv_prefix(set_id), first_exp, state, b_from, b_to, final ? 1 : 0, out16);
+    } else {
+        if ((e = allow_exclusive(md5_recovery_range_kernel<false>)) != cudaSuccess) return e;
+        md5_recovery_range_kernel<false><<<g.blocks, g.threads, g.smem, st>>>(
+            rec, stride, count, slice_size, recv_prefix(set_id), first_exp, state, b_from, b_to, final ? 1 : 0, out16);
+    }
     count_launch();
     return cudaGetLastError();
 }

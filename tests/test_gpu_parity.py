@@ -149,6 +149,20 @@ def test_create_in_memory_bit_exact(p2g, oracle, gpu, case):
         assert [(c.md5, c.crc32) for c in sf.slice_checksums] == cks
 
 
+@pytest.mark.parametrize("n_slices,R", [(3, 40), (2, 200), (5, 7)])
+def test_banded_encode_and_packet_md5(p2g, oracle, gpu, n_slices, R):
+    """Large slices split the encode into symbol bands and chain the packet
+    MD5 band by band; the files must still match the oracle byte for byte."""
+    slice_ = 524288
+    data = file_bytes(n_slices * 31 + R, n_slices * slice_ - 1000).tobytes()
+    opts = p2g.CreateOptions(output="recovery.par2", slice_size=slice_, recovery_block_count=R,
+                             volume_scheme=p2g.VolumeScheme.Exponential())
+    got = p2g.create_in_memory(opts, [(b"band.bin", data)])
+    want = oracle.create([(b"band.bin", data)], slice_, R, kind=oracle.SCHEME_EXPONENTIAL)
+    assert [n for n, _ in got] == [n for n, _ in want]
+    assert all(a == b for (_, a), (_, b) in zip(got, want))
+
+
 def test_single_16m_bit_exact(p2g, oracle, gpu):
     """16,777,216 B, slice 65,536, R 32, Single: every output byte vs the oracle."""
     data = file_bytes(0x16, 16_777_216)
