@@ -236,6 +236,22 @@ typedef struct p2g_encode_job {
 } p2g_encode_job;
 p2g_status p2g_encode(const p2g_encode_job *job);
 
+/* p2g_encode without any allocation by the library.  No counterpart in the
+ * reference: it exists for callers that must own all device memory (a
+ * caching allocator or memory pool that accounts for every byte, a hard
+ * memory cap, or a latency-critical path where cudaMalloc/cudaFree would
+ * synchronise the device), and so cannot let the library call cudaMalloc.
+ * Device pointers only (P2G_DEVICE_POINTERS), same alignment rules as
+ * p2g_encode.  Its scratch is a fixed 8 MiB array inside the library
+ * (present on every GPU that loads it, until exit), which limits a call to
+ * input_count * ceil(recovery_count/32) <= 8192; larger jobs get
+ * P2G_ERR_INVALID_ARGUMENT.  The first call on a device uploads tables and
+ * looks up the scratch address; make that first call before any stream
+ * capture.  All calls share the one scratch array, so calls whose work
+ * overlaps on the GPU (other streams, other threads) race: order them on one
+ * stream or synchronise between them.  Work is enqueued on `stream`. */
+p2g_status p2g_encode_noalloc(const p2g_encode_job *job);
+
 /* The per-slice half of scan_via_mmap, src/source.rs:165-220: MD5 and
  * CRC32 of `count` slices (slice i at src + i*src_stride, slice_size bytes,
  * already zero-padded). */

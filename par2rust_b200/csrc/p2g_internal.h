@@ -85,6 +85,12 @@ uint32_t hash_blocks(uint32_t streams);
 // symbols, RG row groups and `sms` SMs.
 void choose_tiles(uint32_t Np, uint32_t RG, uint32_t sms, uint32_t* ts_out, uint32_t* tiles_out);
 
+// Heap-free variants used by the allocation-free entry point.
+cudaError_t upload_tables_noheap();
+cudaError_t launch_encode_noheap(const uint8_t* src, uint64_t src_stride, uint32_t S, const uint16_t* basis,
+                                 uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec, uint64_t rec_stride,
+                                 int* err, cudaStream_t st);
+
 // Size in bytes of the coefficient-basis scratch for S slices and RG groups.
 inline size_t basis_bytes(uint32_t S, uint32_t RG) { return (size_t)S * RG * 512 * sizeof(uint16_t); }
 

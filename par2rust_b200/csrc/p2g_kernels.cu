@@ -1174,4 +1174,54 @@ cudaError_t launch_realign(const uint8_t* src, uint64_t src_stride, uint8_t* dst
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Heap-free helpers for the allocation-free entry point (p2g_noalloc.cu):
+// same tables and the same single-launch encode as above, but without any
+// host or device allocation.
+// ---------------------------------------------------------------------------
+cudaError_t upload_tables_noheap() {
+    static uint16_t lg[65536], al[65536], lb[32768];
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    uint32_t b = 1;
+    for (uint32_t l = 0; l < kFieldLimit; l++) {
+        lg[b] = (uint16_t)l;
+        al[l] = (uint16_t)b;
+        b <<= 1;
+        if (b & 0x10000u) b ^= kFieldGenerator;
+    }
+    lg[0] = (uint16_t)kFieldLimit;
+    al[kFieldLimit] = 0;
+    uint32_t n = 0;
+    for (uint32_t l = 0; l < kFieldLimit && n < 32768; l++) {
+        uint32_t x = kFieldLimit, y = l;
+        while (y) {
+            const uint32_t t = x % y;
+            x = y;
+            y = t;
+        }
+        if (x == 1) lb[n++] = (uint16_t)l;
+    }
+    cudaError_t e;
+    if ((e = cudaMemcpyToSymbol(d_log, lg, sizeof lg)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(d_antilog, al, sizeof al)) != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(d_logbase, lb, sizeof lb);
+}
+
+cudaError_t launch_encode_noheap(const uint8_t* src, uint64_t src_stride, uint32_t S, const uint16_t* basis,
+                                 uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec, uint64_t rec_stride,
+                                 int* err, cudaStream_t st) {
+    constexpr size_t smem = encode_smem_bytes<kEncChunks>();
+    cudaError_t e = encode_attr();
+    if (e != cudaSuccess) return e;
+    const uint32_t Np = (uint32_t)(((slice_size + 15) & ~15ull) / 2);
+    uint32_t ts = 0, tiles = 0;
+    choose_tiles(Np, RG, (uint32_t)sm_count(), &ts, &tiles);
+    if (!R || !tiles) return cudaSuccess;
+    encode_lut_kernel<kEncChunks><<<tiles * RG, kEncThreads, smem, st>>>(src, src_stride, S, basis, RG, R, 0, Np, ts,
+                                                                         rec, rec_stride, err);
+    count_launch();
+    return cudaGetLastError();
+}
+
 }  // namespace p2g
