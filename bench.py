@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the device MD5-chain rate probe")
+    ap.add_argument("--only-encode", action="store_true",
+                    help="profiling aid: run only the single-launch encode kernel loop (no JSON line)")
     return ap.parse_args()
 
 
@@ -220,6 +222,13 @@ def main():
     def barrier():
         if world > 1:
             dist.barrier()
+
+    if args.only_encode:  # profiling aid: the encode kernel alone, warmup + steps launches
+        for _ in range(args.warmup + args.steps):
+            p2g.encode_device(src.data_ptr(), slice_, S, slice_, R, bufs.recovery.data_ptr(), bufs.rec_stride,
+                              stream.cuda_stream)
+        torch.cuda.synchronize()
+        return 0
 
     # ---- value: device-resident job ----
     for _ in range(args.warmup):

@@ -18,7 +18,7 @@ constexpr uint32_t kFieldGenerator = 0x1100Bu;
 // Encode kernel geometry: 32 recovery rows per CTA ("row group"), 512
 // threads, NCH chunks of 8 symbols per lane.
 constexpr int kRowsPerGroup = 32;
-constexpr int kEncThreads = 448;  // 14 warps x 128 regs leaves 8K registers/SM for MD5 blocks
+constexpr int kEncThreads = 512;  // 16 warps: one 16-row block of each table build per warp
 constexpr int kEncChunks = 2;
 constexpr int kEncTileSymbols = (kEncThreads / 32) * kEncChunks * 64;  // 2048
 constexpr int kEncStages = 4;
