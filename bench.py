@@ -274,7 +274,7 @@ def main():
     sm_mhz = clk.get("sm_mhz") or 1965.0
     lut_peak = 32 * 148 * 1965e6  # 2 shared-memory u16 lookups per MAC at 128 B/clk/SM, max clock
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "encode_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "encode_lut_kernel_traffic.json")
     if os.path.exists(tp):
         try:
             traffic = json.load(open(tp)).get(args.workload)

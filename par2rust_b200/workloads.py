@@ -140,11 +140,18 @@ def many_2000(seed: int = 3) -> Job:
             return j
 
 
-def batch_256(seed: int = 4, cap: int = 24 << 30) -> List[Job]:
+def batch_256(seed: int = 4, cap: int = 24 << 30, n_jobs: int = 256) -> List[Job]:
+    """n_jobs jobs (256 by default) whose total source stays within `cap`;
+    a draw that would exceed the cap (or 32,768 slices) is redrawn, so the
+    cap must leave room for n_jobs jobs (~57 MB each on average)."""
     m = Meta(seed ^ 0xA5A5A5A5A5A5A5A5)
     jobs, total = [], 0
     slices = [16384, 65536, 262144, 1048576]
-    while len(jobs) < 256:
+    draws = 0
+    while len(jobs) < n_jobs:
+        draws += 1
+        if draws > 100 * n_jobs:
+            raise ValueError(f"cannot fit {n_jobs} jobs under a {cap}-byte cap")
         nf = m.randint(1, 16)
         lens = [m.log_uniform(4096, 64 << 20) for _ in range(nf)]
         ss = slices[m.randint(0, 3)]
@@ -157,3 +164,24 @@ def batch_256(seed: int = 4, cap: int = 24 << 30) -> List[Job]:
         jobs.append(Job(ss, R, lens, [file_seed(seed, jid, i) for i in range(nf)], "single"))
         total += sum(lens)
     return jobs
+
+
+def job_cost(job: Job) -> int:
+    """Relative device cost of a create job: GF multiply-accumulates
+    (input slices x recovery rows x symbols per slice) plus the bytes hashed."""
+    return job.slices * max(job.recovery, 1) * (job.slice_size // 2) + 4 * job.source_bytes
+
+
+def shard_jobs(jobs: List[Job], rank: int, world: int) -> List[int]:
+    """Indices of the jobs rank `rank` of `world` runs.  Jobs are independent,
+    so GPUs share no data: greedy longest-processing-time assignment by
+    job_cost, deterministic on every rank (ties broken by job index)."""
+    if world <= 1:
+        return list(range(len(jobs)))
+    load = [0] * world
+    owner = [0] * len(jobs)
+    for i in sorted(range(len(jobs)), key=lambda k: (-job_cost(jobs[k]), k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += job_cost(jobs[i])
+    return [i for i in range(len(jobs)) if owner[i] == rank]
