@@ -45,6 +45,8 @@ WORKLOADS = {
     "single_16m": dict(length=16_777_216, slice=65_536, R=32, scheme="single", seed=1),
     # profiling case: same slice size and recovery count, 256 slices (134 MB > L2)
     "prof_256x512k": dict(length=256 * 524_288, slice=524_288, R=200, scheme="exponential", seed=2),
+    # 256 independent jobs in one persistent launch vs the plain per-job path
+    "batch_256": dict(batch=True, n_jobs=256, seed=4),
 }
 
 
@@ -59,6 +61,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the device MD5-chain rate probe")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-vs-plain section of the default (single-file) run")
+    ap.add_argument("--batch-jobs", type=int, default=256, help="jobs in the batched comparison")
     ap.add_argument("--only-encode", action="store_true",
                     help="profiling aid: run only the single-launch encode kernel loop (no JSON line)")
     return ap.parse_args()
@@ -181,6 +186,159 @@ def run_reference(args, wl):
     return 0
 
 
+def batch_specs(dev, n_jobs=256, seed=4):
+    """The mixed batch on the device: each job's files generated in place
+    (seeded splitmix64 bytes), slice-padded, with its output buffers."""
+    import torch
+
+    import par2rust_b200 as p2g
+    from par2rust_b200 import workloads as W
+
+    jobs = W.batch_256(seed=seed, n_jobs=n_jobs)
+    specs = []
+    for k, j in enumerate(jobs):
+        src = torch.zeros(j.slices * j.slice_size, dtype=torch.uint8, device=dev)
+        off = 0
+        for n, sd in zip(j.file_lengths, j.seeds):
+            src[off:off + n] = W.file_bytes_torch(sd, n, device=dev)
+            off += (n + j.slice_size - 1) // j.slice_size * j.slice_size
+        names = [f"job{k:03d}_file{i:02d}.bin".encode() for i in range(len(j.file_lengths))]
+        bufs = p2g.DeviceJobBuffers(j.slices, len(names), j.slice_size, j.recovery, dev)
+        specs.append(p2g.BatchJobSpec(src, list(j.file_lengths), names, j.slice_size, j.recovery, bufs))
+    return jobs, specs
+
+
+def bench_batch(dev, steps, warmup, plain_steps=1, n_jobs=256, e2e_steps=0):
+    """Batched persistent launch vs the same jobs run one after another through
+    the plain per-job device path (p2g_run_device_job), both with the sources
+    resident in HBM and hash_full left to the host; outputs compared."""
+    import torch
+
+    import par2rust_b200 as p2g
+
+    jobs, specs = batch_specs(dev, n_jobs)
+    total = sum(j.source_bytes for j in jobs)
+    macs = sum(j.slices * j.recovery * (j.slice_size // 2) for j in jobs)
+    stream = torch.cuda.current_stream(dev)
+    t0 = time.perf_counter()
+    batch = p2g.Batch(specs)
+    plan_s = time.perf_counter() - t0
+    info = batch.info()
+    for _ in range(warmup):
+        batch.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    batch.check()
+    l0 = p2g.kernel_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        batch.launch(stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    batch.check()
+    launches = (p2g.kernel_launch_count() - l0) // max(steps, 1)
+    ms = ev0.elapsed_time(ev1) / steps
+    snap = [(s.bufs.recovery.clone(), s.bufs.checksums.clone(), s.bufs.hash16k.clone(), s.bufs.packet_md5.clone(),
+             bytes(s.bufs.set_id_device.cpu().numpy())) for s in specs]
+
+    def plain_step():
+        for s in specs:
+            p2g.run_device_job(s.src, s.file_lengths, s.names, s.slice_size, s.recovery_count, s.bufs,
+                               stream=stream.cuda_stream, skip_hash_full=True)
+
+    plain_step()  # warm: first-call scratch growth
+    torch.cuda.synchronize()
+    pl0 = p2g.kernel_launch_count()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(plain_steps):
+        plain_step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    plain_launches = (p2g.kernel_launch_count() - pl0) // max(plain_steps, 1)
+    plain_ms = a.elapsed_time(b) / plain_steps
+    same = True
+    for s, (rec, ck, h16, pkt, sid) in zip(specs, snap):
+        R = s.recovery_count
+        rs = s.bufs.rec_stride
+        same &= torch.equal(rec.view(-1, rs)[:R, :s.slice_size], s.bufs.recovery.view(-1, rs)[:R, :s.slice_size])
+        same &= torch.equal(ck, s.bufs.checksums) and torch.equal(h16, s.bufs.hash16k)
+        same &= torch.equal(pkt[:16 * R], s.bufs.packet_md5[:16 * R]) and sid == s.bufs.set_id
+    out = {
+        "workload": f"batch_{n_jobs} (mixed jobs: 1-16 files log-uniform in [4 KiB, 64 MiB], slice in "
+                    "{16K,64K,256K,1M}, R 1-20% of slices, seed 4)",
+        "jobs": n_jobs, "files": sum(len(j.file_lengths) for j in jobs), "source_bytes": total,
+        "recovery_bytes": sum(j.recovery * j.slice_size for j in jobs), "gf_macs": macs,
+        "batched_gbs": total / (ms * 1e-3) / 1e9, "batched_ms": ms,
+        "plain_gbs": total / (plain_ms * 1e-3) / 1e9, "plain_ms": plain_ms,
+        "batched_over_plain": plain_ms / ms, "identical_to_plain": bool(same),
+        "batched_launches_per_step": launches, "plain_launches_per_step": plain_launches,
+        "lut_frac": macs / (ms * 1e-3) / (32 * 148 * 1965e6),
+        "plan": {"items": info.items, "encode_items": info.encode_items, "scan_items": info.scan_items,
+                 "ctas": info.ctas, "predicted_ms": info.predicted_ms, "plan_and_capture_s": plan_s,
+                 "scratch_bytes": info.device_bytes},
+        "hash_full": "not on the device in either arm (the host hashes whole files while reading them)",
+    }
+    if e2e_steps:
+        # pinned host sources -> H2D -> batched launch -> D2H of every output
+        hosts = [torch.empty(s.src.numel(), dtype=torch.uint8, pin_memory=True) for s in specs]
+        for h, s in zip(hosts, specs):
+            h.copy_(s.src)
+        outs = [(torch.empty(s.bufs.recovery.numel(), dtype=torch.uint8, pin_memory=True),
+                 torch.empty(s.bufs.checksums.numel(), dtype=torch.uint8, pin_memory=True),
+                 torch.empty(s.bufs.packet_md5.numel(), dtype=torch.uint8, pin_memory=True),
+                 torch.empty(s.bufs.hash16k.numel(), dtype=torch.uint8, pin_memory=True),
+                 torch.empty(16, dtype=torch.uint8, pin_memory=True)) for s in specs]
+        h2d = sum(h.numel() for h in hosts)
+        d2h = sum(sum(t.numel() for t in o) for o in outs)
+
+        def e2e_step():
+            for h, s in zip(hosts, specs):
+                s.src.copy_(h, non_blocking=True)
+            batch.launch(stream.cuda_stream)
+            for o, s in zip(outs, specs):
+                for t, d in zip(o, (s.bufs.recovery, s.bufs.checksums, s.bufs.packet_md5, s.bufs.hash16k,
+                                    s.bufs.set_id_device)):
+                    t.copy_(d, non_blocking=True)
+            torch.cuda.synchronize()
+
+        e2e_step()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        es = (time.perf_counter() - t0) / e2e_steps
+        batch.check()
+        out["e2e"] = {"value": total / es / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                      "seconds_per_step": es,
+                      "api": "p2g_batch_launch with pinned host sources (H2D) and pinned output copies (D2H)"}
+    batch.close()
+    del specs, snap
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_reference_batch(args, wl):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    per_step = max(1.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    cb = None
+    for _ in range(args.steps):
+        cb, spent = batch_cpu_baseline(per_step)
+        vals.append(spent)
+    line = {
+        "metric": "encode source GB/s (batched)", "value": cb["value"], "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(vals) / len(vals) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "impl": "reference", "config": {"workload": "batch_256", "parallelism": "host threads"},
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def config_dict(args, wl):
     S = (wl["length"] + wl["slice"] - 1) // wl["slice"]
     return {"workload": args.workload, "file_bytes": wl["length"], "files": 1, "slice_size": wl["slice"],
@@ -189,11 +347,89 @@ def config_dict(args, wl):
             "l2": "inputs larger than L2: each step reads the whole padded source"}
 
 
+def batch_cpu_baseline(target_s, threads=0):
+    """The CPU port on whole jobs of the mixed batch, in batch order, until
+    about target_s seconds of CPU work (each job's files as one buffer)."""
+    import numpy as np
+
+    from oracle import oracle as orc
+    from par2rust_b200 import workloads as W
+
+    done_bytes, spent, jobs_done = 0, 0.0, 0
+    for j in W.batch_256():
+        data = np.concatenate([W.file_bytes(sd, n) for n, sd in zip(j.file_lengths, j.seeds)])
+        t, *_ = orc.create_timed(data, j.slice_size, j.recovery, threads)
+        done_bytes += len(data)
+        spent += t
+        jobs_done += 1
+        if spent >= target_s:
+            break
+    return {"value": done_bytes / spent / 1e9, "unit": "GB/s", "cores": threads or orc.max_threads(), "kind": "port",
+            "sample": f"the first {jobs_done} jobs of the batch ({done_bytes} B), each job's files hashed and encoded "
+                      "as one buffer (scan + encode + packet MD5s)", "seconds": spent}, spent
+
+
+def run_batch(args, wl):
+    """--workload batch_256: the batched launch is the measured step."""
+    import torch
+    import torch.distributed as dist
+
+    import par2rust_b200 as p2g
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    clocks = ClockSampler(local)
+    clocks.start()
+    res = bench_batch(dev, args.steps, args.warmup, plain_steps=1, n_jobs=wl["n_jobs"],
+                      e2e_steps=args.e2e_steps)
+    clk = clocks.stop()
+    t = torch.tensor([res["batched_ms"]], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * res["source_bytes"] / (ms_max * 1e-3) / 1e9
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb, _ = batch_cpu_baseline(args.cpu_seconds)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    hbm_peak, peak_kind = measured_peaks()
+    alg = res["source_bytes"] + res["recovery_bytes"]
+    line = {
+        "metric": "encode source GB/s (batched)", "value": value, "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": res["workload"], "jobs": res["jobs"], "files": res["files"],
+                   "source_bytes": res["source_bytes"], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (14.7 GB of sources per step)"},
+        "batched": res,
+        "e2e": res.get("e2e"),
+        "roofline": {"bound": "hbm", "achieved": alg / (ms_max * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": alg / (ms_max * 1e-3) / 1e9 / hbm_peak, "traffic": None, "peak_source": peak_kind,
+                     "kernel": "batch_kernel (whole step)", "algorithmic_bytes": alg},
+        "lut_roofline": {"achieved": res["gf_macs"] / (ms_max * 1e-3), "peak": 32 * 148 * 1965e6,
+                         "unit": "GF(2^16) MAC/s", "frac": res["lut_frac"]},
+        "cpu_baseline": cb, "clocks": clk, "gpu_launches": res["batched_launches_per_step"] * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
+        if wl.get("batch"):
+            return run_reference_batch(args, wl)
         return run_reference(args, wl)
+    if wl.get("batch"):
+        return run_batch(args, wl)
 
     import numpy as np
     import torch
@@ -313,6 +549,11 @@ def main():
         torch.cuda.synchronize()
         chain_gbs = 64 * 1024 * 1024 / (time.perf_counter() - t0) / 1e9
 
+    # ---- batched persistent launch vs the plain path on the mixed batch ----
+    batched = None
+    if world == 1 and not args.no_batch:
+        batched = bench_batch(dev, args.steps, args.warmup, plain_steps=1, n_jobs=args.batch_jobs)
+
     # ---- CPU baseline (rank 0, N=1) ----
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -342,6 +583,7 @@ def main():
         "clocks": clk,
         "gpu_launches": launches,
         "file_md5_device_chain_gbs": chain_gbs,
+        "batched": batched,
         "device": info,
         "baseline_note": "vs_baseline divides by the reference's published end-to-end create rate for this "
                          "shape (0.0975 GB/s, Apple M4, 10 threads)",

@@ -305,6 +305,74 @@ typedef struct p2g_device_job {
 } p2g_device_job;
 p2g_status p2g_run_device_job(p2g_device_job *job);
 
+/* ---- batched create (no counterpart in par2rust, which runs one create
+ * at a time: run_create, src/creator.rs:188-321) ------------------------
+ * Many independent create jobs, each described like p2g_device_job, run in
+ * one persistent launch: one CTA per SM pops (job, row group, symbol tile)
+ * encode items and (job, 256-slice) scan items off a device queue; the CTA
+ * that completes a job's last encode item derives that job's hash16k, file
+ * ids, set id (on the device) and recovery-packet MD5s.  Per job the device
+ * outputs are byte-identical to p2g_run_device_job with
+ * P2G_JOB_SKIP_HASH_FULL (hash_full stays with the caller, who usually hashes
+ * it on the host while reading the files).  An autotuner picks each job's
+ * tile width and the queue order by simulating the launch with a cost model.
+ * The launch sequence (queue reset, coefficient bases, any realignment, the
+ * persistent kernel) is captured once into a CUDA graph and replayed. */
+typedef struct p2g_batch_job {
+    const uint8_t *src;                 /* device, 16-byte aligned; layout as in p2g_device_job */
+    uint32_t file_count;
+    const uint64_t *file_lengths;       /* host array */
+    const uint8_t *const *names;        /* host array of display names */
+    const size_t *name_lens;
+    uint64_t slice_size;
+    uint32_t recovery_count;
+    uint8_t *recovery;                  /* device, 16-byte aligned */
+    uint64_t recovery_stride;           /* multiple of 16, >= slice_size rounded up to 16 */
+    p2g_slice_checksum *checksums;      /* device, one per input slice */
+    uint8_t *hash16k;                   /* device, 16 per file */
+    uint8_t *packet_md5;                /* device, 16 per recovery row */
+    uint8_t *set_id;                    /* device, 16 bytes, 4-byte aligned */
+} p2g_batch_job;
+
+typedef struct p2g_batch p2g_batch;     /* opaque */
+
+typedef struct p2g_batch_info {
+    uint32_t jobs, items;
+    uint32_t encode_items, scan_items, finish_items;
+    uint32_t ctas;                      /* persistent CTAs (one per SM) */
+    double predicted_ms;                /* the autotuner's makespan estimate */
+    uint64_t device_bytes;              /* scratch the batch holds (bases, tables, queue) */
+} p2g_batch_info;
+
+/* Shape of one job, for the host-only planner. */
+typedef struct p2g_batch_shape {
+    uint64_t slice_size;
+    uint32_t input_slices;
+    uint32_t recovery_count;
+    uint32_t file_count;
+} p2g_batch_shape;
+
+#define P2G_BATCH_NO_GRAPH 1u           /* launch directly instead of replaying a CUDA graph */
+#define P2G_BATCH_NO_AUTOTUNE 2u        /* widest tiles and cost order, no tile search */
+
+/* Validate the jobs (the checks of p2g_run_device_job), plan the items and
+ * allocate the batch's device scratch.  The job buffers must stay valid
+ * while the batch is used; contents may change between launches. */
+p2g_status p2g_batch_create(const p2g_batch_job *jobs, uint32_t n, uint32_t flags, p2g_batch **out);
+/* Enqueue one run of the whole batch on `stream` (one run at a time per batch). */
+p2g_status p2g_batch_launch(p2g_batch *batch, void *stream);
+/* After the run's stream has been synchronised: P2G_ERR_TIMEOUT when a
+ * bounded device wait gave up, else P2G_OK. */
+p2g_status p2g_batch_check(p2g_batch *batch);
+p2g_status p2g_batch_get_info(const p2g_batch *batch, p2g_batch_info *out);
+/* Tile width (symbols) the autotuner chose for job `job`; 0 if out of range. */
+uint32_t p2g_batch_job_tile(const p2g_batch *batch, uint32_t job);
+void p2g_batch_destroy(p2g_batch *batch);
+/* The planner alone (no device): items and predicted makespan for `ctas`
+ * CTAs; tiles_out (optional, n entries) receives each job's tile width. */
+p2g_status p2g_batch_plan(const p2g_batch_shape *shapes, uint32_t n, uint32_t ctas, uint32_t flags,
+                          p2g_batch_info *info, uint32_t *tiles_out);
+
 /* ---- host helpers of the reference's public format/packet modules ----- */
 
 /* generate_input_bases, src/reedsolomon.rs:130-149 */

@@ -72,6 +72,10 @@ def lib() -> C.CDLL:
                                 C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
         L.or_gfni_matrices.argtypes = [C.c_uint16, C.c_void_p]
         L.or_gfni_apply.argtypes = [C.c_void_p, C.c_uint8, C.c_uint8, C.c_void_p, C.c_void_p]
+        L.or_build_main_packet.restype = C.c_size_t
+        L.or_build_main_packet.argtypes = [C.c_uint64, C.c_char_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        L.or_build_recovery_packet.restype = C.c_size_t
+        L.or_build_recovery_packet.argtypes = [C.c_char_p, C.c_uint16, C.c_void_p, C.c_uint64, C.c_void_p]
         L.cb_encode.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_void_p, C.c_int]
         L.cb_scan.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.cb_create_timed.restype = C.c_double
@@ -211,6 +215,24 @@ def file_id(hash16k: bytes, length: int, name: bytes) -> bytes:
     out = (C.c_uint8 * 16)()
     lib().or_file_id(hash16k, length, name, len(name), out)
     return bytes(out)
+
+
+def set_id(slice_size: int, file_ids) -> bytes:
+    """Recovery set id: MD5 of the main-packet body over the sorted file ids
+    (or_build_main_packet, main_packet.rs:25-42)."""
+    out = (C.c_uint8 * 16)()
+    lib().or_build_main_packet(slice_size, b"".join(file_ids), len(file_ids), out, None)
+    return bytes(out)
+
+
+def recovery_packet_md5(set_id_: bytes, exponent: int, row) -> bytes:
+    """Packet MD5 (header bytes 16..32) of the recovery packet of one row
+    (or_build_recovery_packet, recovery.rs:11-19)."""
+    a, p = _addr(row)
+    n = lib().or_build_recovery_packet(set_id_, exponent, p, len(a), None)
+    buf = (C.c_uint8 * n)()
+    lib().or_build_recovery_packet(set_id_, exponent, p, len(a), buf)
+    return bytes(buf)[16:32]
 
 
 def _scheme_c(kind, count=0, cap=0, inner=None, sizes=None, keep=None):

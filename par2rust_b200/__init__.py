@@ -520,6 +520,7 @@ class DeviceJobBuffers:
         self.hash_full = torch.empty(max(n_files, 1) * 16, dtype=torch.uint8, device=device)
         self.hash16k = torch.empty(max(n_files, 1) * 16, dtype=torch.uint8, device=device)
         self.packet_md5 = torch.empty(max(recovery_count, 1) * 16, dtype=torch.uint8, device=device)
+        self.set_id_device = torch.empty(16, dtype=torch.uint8, device=device)  # written by batched runs
         self.set_id = b""
 
 
@@ -563,6 +564,117 @@ def run_device_job(src, file_lengths: Sequence[int], names: Sequence[bytes], sli
     _check(lib().p2g_run_device_job(C.byref(job)))
     bufs.set_id = bytes(job.set_id_out)
     return bufs
+
+
+# ---------------------------------------------------------------------------
+# Batched create (no counterpart in the reference, which creates one set at a
+# time): many jobs in one persistent, graph-captured launch.
+# ---------------------------------------------------------------------------
+BATCH_NO_GRAPH = 1
+BATCH_NO_AUTOTUNE = 2
+
+
+@dataclass
+class BatchJobSpec:
+    """One job of a batch: a device source laid out as for run_device_job and
+    the buffers its outputs go to."""
+    src: object
+    file_lengths: Sequence[int]
+    names: Sequence[bytes]
+    slice_size: int
+    recovery_count: int
+    bufs: DeviceJobBuffers
+
+    @property
+    def input_slices(self) -> int:
+        return sum((n + self.slice_size - 1) // self.slice_size for n in self.file_lengths)
+
+
+@dataclass
+class BatchInfo:
+    jobs: int
+    items: int
+    encode_items: int
+    scan_items: int
+    finish_items: int
+    ctas: int
+    predicted_ms: float
+    device_bytes: int
+
+
+def _batch_info(ci: "_ffi.p2g_batch_info") -> BatchInfo:
+    return BatchInfo(ci.jobs, ci.items, ci.encode_items, ci.scan_items, ci.finish_items, ci.ctas,
+                     ci.predicted_ms, ci.device_bytes)
+
+
+class Batch:
+    """A planned batch of create jobs (p2g_batch_create).  ``launch`` enqueues
+    one run of every job on a stream; after synchronising, ``check`` raises
+    DeviceTimeout if a bounded device wait gave up.  Per job the outputs equal
+    run_device_job(..., skip_hash_full=True); the set id lands in
+    ``bufs.set_id_device``."""
+
+    def __init__(self, jobs: Sequence[BatchJobSpec], flags: int = 0):
+        self._keep = []
+        arr = (_ffi.p2g_batch_job * len(jobs))()
+        for i, j in enumerate(jobs):
+            n = len(j.file_lengths)
+            lens = (C.c_uint64 * max(n, 1))(*j.file_lengths)
+            nbufs = [C.create_string_buffer(bytes(x), len(x)) for x in j.names]
+            nptrs = (C.c_void_p * max(n, 1))(*[C.addressof(b) for b in nbufs])
+            nlens = (C.c_size_t * max(n, 1))(*[len(x) for x in j.names])
+            self._keep += [lens, nbufs, nptrs, nlens]
+            b = j.bufs
+            arr[i] = _ffi.p2g_batch_job(src=j.src.data_ptr(), file_count=n, file_lengths=lens, names=nptrs,
+                                        name_lens=nlens, slice_size=j.slice_size, recovery_count=j.recovery_count,
+                                        recovery=b.recovery.data_ptr(), recovery_stride=b.rec_stride,
+                                        checksums=b.checksums.data_ptr(), hash16k=b.hash16k.data_ptr(),
+                                        packet_md5=b.packet_md5.data_ptr(), set_id=b.set_id_device.data_ptr())
+        self.jobs = list(jobs)
+        h = C.c_void_p()
+        _check(lib().p2g_batch_create(arr, len(jobs), flags, C.byref(h)))
+        self._h = h
+
+    def launch(self, stream: Optional[int] = None) -> None:
+        import torch
+
+        if stream is None:
+            stream = torch.cuda.current_stream().cuda_stream
+        _check(lib().p2g_batch_launch(self._h, stream))
+
+    def check(self) -> None:
+        _check(lib().p2g_batch_check(self._h))
+
+    def info(self) -> BatchInfo:
+        ci = _ffi.p2g_batch_info()
+        _check(lib().p2g_batch_get_info(self._h, C.byref(ci)))
+        return _batch_info(ci)
+
+    def tile(self, job: int) -> int:
+        return lib().p2g_batch_job_tile(self._h, job)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().p2g_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_plan(shapes: Sequence[Tuple[int, int, int, int]], ctas: int = 148, flags: int = 0
+               ) -> Tuple[BatchInfo, List[int]]:
+    """The batch planner alone (no device): shapes are (slice_size,
+    input_slices, recovery_count, file_count); returns the plan summary and
+    each job's tile width (0 for jobs without recovery rows)."""
+    arr = (_ffi.p2g_batch_shape * len(shapes))(*[_ffi.p2g_batch_shape(*s) for s in shapes])
+    ci = _ffi.p2g_batch_info()
+    tiles = (C.c_uint32 * max(len(shapes), 1))()
+    _check(lib().p2g_batch_plan(arr, len(shapes), ctas, flags, C.byref(ci), tiles))
+    return _batch_info(ci), list(tiles[:len(shapes)])
 
 
 # ---------------------------------------------------------------------------
@@ -646,5 +758,6 @@ __all__ = [
     "run_create_with_progress", "run_create_fused", "write_index_file", "create_in_memory", "gf_mul_xor", "encode",
     "encode_device", "slice_checksums", "file_hashes", "recovery_packet_md5", "input_bases", "gf_mul", "gf_pow",
     "resolve_volume_sizes", "volume_filename", "build_packet", "build_main_packet", "compute_file_id", "md5",
-    "kernel_launch_count", "device_info", "DeviceJobBuffers", "run_device_job",
+    "kernel_launch_count", "device_info", "DeviceJobBuffers", "run_device_job", "BATCH_NO_GRAPH",
+    "BATCH_NO_AUTOTUNE", "BatchJobSpec", "BatchInfo", "Batch", "batch_plan",
 ]

@@ -138,6 +138,46 @@ class p2g_device_job(C.Structure):
     ]
 
 
+class p2g_batch_job(C.Structure):
+    _fields_ = [
+        ("src", C.c_void_p),
+        ("file_count", C.c_uint32),
+        ("file_lengths", C.POINTER(C.c_uint64)),
+        ("names", C.POINTER(C.c_void_p)),
+        ("name_lens", C.POINTER(C.c_size_t)),
+        ("slice_size", C.c_uint64),
+        ("recovery_count", C.c_uint32),
+        ("recovery", C.c_void_p),
+        ("recovery_stride", C.c_uint64),
+        ("checksums", C.c_void_p),
+        ("hash16k", C.c_void_p),
+        ("packet_md5", C.c_void_p),
+        ("set_id", C.c_void_p),
+    ]
+
+
+class p2g_batch_info(C.Structure):
+    _fields_ = [
+        ("jobs", C.c_uint32),
+        ("items", C.c_uint32),
+        ("encode_items", C.c_uint32),
+        ("scan_items", C.c_uint32),
+        ("finish_items", C.c_uint32),
+        ("ctas", C.c_uint32),
+        ("predicted_ms", C.c_double),
+        ("device_bytes", C.c_uint64),
+    ]
+
+
+class p2g_batch_shape(C.Structure):
+    _fields_ = [
+        ("slice_size", C.c_uint64),
+        ("input_slices", C.c_uint32),
+        ("recovery_count", C.c_uint32),
+        ("file_count", C.c_uint32),
+    ]
+
+
 # (name, restype, argtypes) for every entry point of include/par2gpu.h
 SIGNATURES = [
     ("p2g_last_error_message", C.c_char_p, []),
@@ -173,6 +213,15 @@ SIGNATURES = [
     ("p2g_recovery_packet_md5", C.c_int,
      [C.c_char_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint16, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("p2g_run_device_job", C.c_int, [C.POINTER(p2g_device_job)]),
+    ("p2g_batch_create", C.c_int, [C.POINTER(p2g_batch_job), C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("p2g_batch_launch", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("p2g_batch_check", C.c_int, [C.c_void_p]),
+    ("p2g_batch_get_info", C.c_int, [C.c_void_p, C.POINTER(p2g_batch_info)]),
+    ("p2g_batch_job_tile", C.c_uint32, [C.c_void_p, C.c_uint32]),
+    ("p2g_batch_destroy", None, [C.c_void_p]),
+    ("p2g_batch_plan", C.c_int,
+     [C.POINTER(p2g_batch_shape), C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(p2g_batch_info),
+      C.POINTER(C.c_uint32)]),
     ("p2g_input_bases", C.c_int, [C.c_uint32, C.POINTER(C.c_uint16)]),
     ("p2g_gf_mul", C.c_uint16, [C.c_uint16, C.c_uint16]),
     ("p2g_gf_pow", C.c_uint16, [C.c_uint16, C.c_uint32]),

@@ -1,0 +1,498 @@
+// p2g_batch.cpp -- batched create: many independent create jobs in one
+// persistent, graph-captured launch (p2g_batch_* in include/par2gpu.h).
+//
+// Planning.  Each job becomes work items: scan items (slice MD5 + CRC32 of
+// up to kScanSlices slices), encode items (one row group x one symbol tile
+// over all of the job's input slices) and, for a job without recovery rows,
+// one finish item.  A job's finish step (hash16k, file ids, set id, packet
+// MD5s) runs on the CTA that completes its last encode item.
+//
+// Autotuning.  Items are popped in a fixed order by whichever CTA is free,
+// so the launch is list scheduling.  The planner simulates it with a cost
+// model (per-slice encode cost ~ tile + 384 shared-memory wavefronts at 78%
+// of peak, ~0.72 us per 64-byte MD5 block of a chain) for the queue order
+// "longest item + tail first", then searches each large job's tile width
+// (1x, 2x, 4x, 8x its minimum tile count) for the shortest simulated makespan.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <queue>
+#include <vector>
+
+#include "p2g_host_util.h"
+#include "p2g_internal.h"
+
+namespace p2g {
+namespace {
+
+constexpr double kEncRate = 0.78 * 1.9e6;  // tile-symbol wavefronts per ms per CTA
+constexpr double kBuildCost = 384.0;       // table build per slice, in wavefronts
+constexpr double kChainMs = 7.2e-4;        // one MD5 chain step of 64 bytes
+constexpr double kItemMs = 0.003;          // pop, descriptor loads, pipeline fill
+
+inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+inline double md5_ms(uint64_t bytes) { return (double)((bytes + 8) / 64 + 1) * kChainMs; }
+
+struct PlanJob {
+    uint64_t slice = 0;
+    uint32_t S = 0, R = 0, n = 0, RG = 0, Np = 0;
+    uint32_t ts = 0, tiles = 0;  // chosen tiling
+    double finish = 0;           // finish-step estimate
+};
+
+double finish_ms(const PlanJob& j) {
+    const double files = ceil(j.n / 256.0) * (md5_ms(P2G_HASH16K_LEN) + md5_ms(24 + 256));
+    const double sort = (double)j.n * j.n / 512.0 * 4e-6;
+    const double body = md5_ms(12 + 16ull * j.n);
+    const double pkt = ceil(j.R / 256.0) * md5_ms(36 + j.slice);
+    return files + sort + body + pkt + kItemMs;
+}
+inline double encode_ms(const PlanJob& j, uint32_t syms) {
+    return (double)j.S * (round_up(syms, 8) + kBuildCost) / kEncRate + kItemMs;
+}
+inline double scan_ms(const PlanJob& j, uint32_t count) {
+    // MD5 lanes run in parallel; the CRC warps take count/8 slices each at
+    // about 6 shared loads per 4 bytes per lane, mostly hidden behind them
+    const double crc = ceil(count / 8.0) * (double)j.slice / 128.0 * 6.0 / 1.9e6;
+    return std::max(md5_ms(j.slice), crc) + kItemMs;
+}
+
+void set_tiling(PlanJob& j, uint32_t tiles) {
+    const uint32_t ts = (uint32_t)std::min<uint64_t>(round_up((j.Np + tiles - 1) / tiles, 8), kEncTileSymbols);
+    j.ts = ts;
+    j.tiles = (j.Np + ts - 1) / ts;
+}
+inline uint32_t min_tiles(const PlanJob& j) { return (j.Np + kEncTileSymbols - 1) / kEncTileSymbols; }
+
+struct Plan {
+    std::vector<BatchItem> items;
+    std::vector<uint32_t> enc_items;  // per job
+    uint32_t n_scan = 0, n_enc = 0, n_fin = 0;
+    double makespan = 0;
+};
+
+// Items of all jobs in queue order (stable: key descending, then job, then
+// generation order, which is tile-major so a tile's row groups run together
+// and share its source reads in L2).
+Plan build_items(const std::vector<PlanJob>& jobs) {
+    struct Keyed {
+        double key;
+        uint32_t seq;
+        BatchItem it;
+    };
+    std::vector<Keyed> v;
+    Plan p;
+    p.enc_items.assign(jobs.size(), 0);
+    uint32_t seq = 0;
+    for (uint32_t ji = 0; ji < (uint32_t)jobs.size(); ++ji) {
+        const PlanJob& j = jobs[ji];
+        for (uint32_t s = 0; s < j.S; s += kScanSlices) {
+            const uint32_t cnt = std::min(kScanSlices, j.S - s);
+            v.push_back({scan_ms(j, cnt), seq++, {ji, kItemScan, s, cnt}});
+            p.n_scan++;
+        }
+        if (j.R) {
+            for (uint32_t t = 0; t < j.tiles; ++t) {
+                const uint32_t n0 = t * j.ts, syms = std::min(j.ts, j.Np - n0);
+                const double key = encode_ms(j, syms) + j.finish;
+                for (uint32_t rg = 0; rg < j.RG; ++rg) v.push_back({key, seq++, {ji, kItemEncode | (rg << 8), n0, syms}});
+            }
+            p.enc_items[ji] = j.tiles * j.RG;
+            p.n_enc += j.tiles * j.RG;
+        } else {
+            v.push_back({j.finish, seq++, {ji, kItemFinish, 0, 0}});
+            p.n_fin++;
+        }
+    }
+    std::stable_sort(v.begin(), v.end(), [](const Keyed& a, const Keyed& b) {
+        if (a.key != b.key) return a.key > b.key;
+        if (a.it.job != b.it.job) return a.it.job < b.it.job;
+        return a.seq < b.seq;
+    });
+    p.items.reserve(v.size());
+    for (const Keyed& k : v) p.items.push_back(k.it);
+    return p;
+}
+
+double item_ms(const PlanJob& j, const BatchItem& it) {
+    switch (it.kind_rg & 0xFF) {
+    case kItemScan: return scan_ms(j, it.b);
+    case kItemEncode: return encode_ms(j, it.b);
+    default: return j.finish;
+    }
+}
+
+// List-scheduling simulation: each item goes to the CTA that frees first;
+// the CTA that runs a job's last encode item also runs its finish step.
+double simulate(const std::vector<PlanJob>& jobs, const Plan& p, uint32_t ctas) {
+    std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+    for (uint32_t c = 0; c < ctas; ++c) free_at.push(0.0);
+    std::vector<uint32_t> left = p.enc_items;
+    double end = 0;
+    for (const BatchItem& it : p.items) {
+        double t = free_at.top();
+        free_at.pop();
+        const PlanJob& j = jobs[it.job];
+        t += item_ms(j, it);
+        if ((it.kind_rg & 0xFF) == kItemEncode && --left[it.job] == 0) t += j.finish;
+        end = std::max(end, t);
+        free_at.push(t);
+    }
+    return end;
+}
+
+Plan plan_batch(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
+    for (PlanJob& j : jobs) {
+        j.RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
+        j.Np = (uint32_t)(round_up(j.slice, 16) / 2);
+        j.finish = finish_ms(j);
+        set_tiling(j, min_tiles(j));
+    }
+    Plan best = build_items(jobs);
+    best.makespan = simulate(jobs, best, ctas);
+    if (flags & P2G_BATCH_NO_AUTOTUNE) return best;
+    // lower bound at the widest tiles: all work spread evenly over the CTAs
+    double total = 0;
+    for (const PlanJob& j : jobs) {
+        total += j.finish;
+        total += ceil((double)j.S / kScanSlices) * scan_ms(j, std::min(j.S, kScanSlices));
+        if (j.R) total += (double)j.tiles * j.RG * encode_ms(j, j.ts);
+    }
+    const double bound = total / ctas;
+    if (best.makespan <= 1.02 * bound) return best;
+    // try finer tilings for the jobs with the longest encode items
+    std::vector<uint32_t> order;
+    for (uint32_t i = 0; i < (uint32_t)jobs.size(); ++i)
+        if (jobs[i].R) order.push_back(i);
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        return encode_ms(jobs[a], jobs[a].ts) > encode_ms(jobs[b], jobs[b].ts);
+    });
+    if (order.size() > 24) order.resize(24);
+    for (uint32_t ji : order) {
+        PlanJob& j = jobs[ji];
+        const uint32_t base = min_tiles(j), keep = j.tiles;
+        uint32_t best_tiles = keep;
+        for (uint32_t mult : {2u, 4u, 8u}) {
+            const uint32_t t = base * mult;
+            if ((j.Np + t - 1) / t < 64) continue;  // tiles too small to pay for their table builds
+            set_tiling(j, t);
+            Plan p = build_items(jobs);
+            p.makespan = simulate(jobs, p, ctas);
+            if (p.makespan < best.makespan * 0.999) {
+                best = std::move(p);
+                best_tiles = j.tiles;
+            }
+        }
+        set_tiling(j, best_tiles);
+        if (best.makespan <= 1.02 * bound) break;
+    }
+    return best;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// The batch object
+// ---------------------------------------------------------------------------
+}  // namespace p2g
+
+struct p2g_batch {
+    int device = -1;
+    uint32_t flags = 0;
+    uint32_t n_jobs = 0, n_items = 0, ctas = 0;
+    p2g::Plan plan;
+    std::vector<p2g::PlanJob> shape;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    p2g::BatchJob* d_jobs = nullptr;
+    p2g::BatchItem* d_items = nullptr;
+    uint32_t* d_ctl = nullptr;  // queue head, per-job counters, then the error word
+    size_t ctl_bytes = 0;
+    uint64_t max_basis_words = 0;
+    struct Realign {
+        const uint8_t* src;
+        uint8_t* dst;
+        uint64_t slice, estride;
+        uint32_t S;
+    };
+    std::vector<Realign> realigns;
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t kernels_per_run = 0;
+};
+
+namespace p2g {
+namespace {
+
+p2g_status enqueue_run(p2g_batch* b, cudaStream_t st) {
+    int* err = reinterpret_cast<int*>(b->d_ctl + 1 + b->n_jobs);
+    P2G_CU(cudaMemsetAsync(b->d_ctl, 0, b->ctl_bytes, st));
+    P2G_CU(launch_basis_batch(b->d_jobs, b->n_jobs, b->max_basis_words, st));
+    for (const auto& r : b->realigns) P2G_CU(launch_realign(r.src, r.slice, r.dst, r.estride, r.S, r.slice, st));
+    P2G_CU(launch_batch(b->d_jobs, b->d_items, b->n_items, b->d_ctl, err, b->ctas, st));
+    return P2G_OK;
+}
+
+void release(p2g_batch* b) {
+    if (!b) return;
+    if (b->device >= 0) cudaSetDevice(b->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    if (b->arena) cudaFree(b->arena);
+    delete b;
+}
+
+void fill_info(const p2g_batch* b, p2g_batch_info* out) {
+    out->jobs = b->n_jobs;
+    out->items = b->n_items;
+    out->encode_items = b->plan.n_enc;
+    out->scan_items = b->plan.n_scan;
+    out->finish_items = b->plan.n_fin;
+    out->ctas = b->ctas;
+    out->predicted_ms = b->plan.makespan;
+    out->device_bytes = b->arena_bytes;
+}
+
+}  // namespace
+}  // namespace p2g
+
+using namespace p2g;
+
+extern "C" p2g_status p2g_batch_plan(const p2g_batch_shape* shapes, uint32_t n, uint32_t ctas, uint32_t flags,
+                                     p2g_batch_info* info, uint32_t* tiles_out) {
+    clear_error();
+    if (!shapes || !n || !ctas) return set_error(P2G_ERR_INVALID_ARGUMENT, "batch plan needs shapes and ctas > 0");
+    std::vector<PlanJob> jobs(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        P2G_TRY(check_common(std::max(1u, shapes[i].file_count), shapes[i].recovery_count, shapes[i].slice_size));
+        if (!shapes[i].input_slices || shapes[i].input_slices > P2G_MAX_INPUT_BLOCKS)
+            return set_error(P2G_ERR_INVALID_ARGUMENT, "job %u: input slice count must be in [1, 32768]", i);
+        jobs[i].slice = shapes[i].slice_size;
+        jobs[i].S = shapes[i].input_slices;
+        jobs[i].R = shapes[i].recovery_count;
+        jobs[i].n = std::max(1u, shapes[i].file_count);
+    }
+    const Plan p = plan_batch(jobs, ctas, flags);
+    if (info) {
+        p2g_batch tmp;
+        tmp.n_jobs = n;
+        tmp.n_items = (uint32_t)p.items.size();
+        tmp.ctas = ctas;
+        tmp.plan = p;
+        fill_info(&tmp, info);
+    }
+    if (tiles_out)
+        for (uint32_t i = 0; i < n; ++i) tiles_out[i] = jobs[i].R ? jobs[i].ts : 0;
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, uint32_t flags, p2g_batch** out) {
+    clear_error();
+    if (!out) return set_error(P2G_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!jobs || !n) return set_error(P2G_ERR_INVALID_ARGUMENT, "a batch needs at least one job");
+    if (n > 65535) return set_error(P2G_ERR_INVALID_ARGUMENT, "a batch holds at most 65535 jobs");
+    // ---- validation (as p2g_run_device_job) ----
+    std::vector<PlanJob> shape(n);
+    uint64_t total_files = 0, names_bytes = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const p2g_batch_job& jb = jobs[i];
+        P2G_TRY(check_common(jb.file_count, jb.recovery_count, jb.slice_size));
+        if (!jb.src || (uintptr_t)jb.src % 16 || !jb.checksums || !jb.hash16k || !jb.set_id ||
+            (uintptr_t)jb.set_id % 4 || !jb.file_lengths || !jb.names || !jb.name_lens)
+            return set_error(P2G_ERR_INVALID_ARGUMENT,
+                             "batch job %u: src (16-byte aligned), checksums, hash16k, set_id (4-byte aligned), "
+                             "file lengths and names are required", i);
+        if (jb.recovery_count && (!jb.recovery || !jb.packet_md5 || (uintptr_t)jb.recovery % 16 ||
+                                  jb.recovery_stride % 16 || jb.recovery_stride < round_up(jb.slice_size, 16)))
+            return set_error(P2G_ERR_INVALID_ARGUMENT,
+                             "batch job %u: recovery rows need a 16-byte aligned buffer, recovery_stride a multiple "
+                             "of 16 and >= round_up(slice,16), and packet_md5", i);
+        uint64_t S = 0, total = 0;
+        for (uint32_t f = 0; f < jb.file_count; ++f) {
+            P2G_TRY(check_name(jb.names[f], jb.name_lens[f], ""));
+            if (jb.file_lengths[f] == 0) return set_error(P2G_ERR_EMPTY_FILE, "batch job %u: input file %u is empty", i, f);
+            S += (jb.file_lengths[f] + jb.slice_size - 1) / jb.slice_size;
+            total += jb.file_lengths[f];
+            names_bytes += round_up(jb.name_lens[f], 4);
+        }
+        P2G_TRY(check_total_blocks(S, total, jb.slice_size));
+        total_files += jb.file_count;
+        shape[i].slice = jb.slice_size;
+        shape[i].S = (uint32_t)S;
+        shape[i].R = jb.recovery_count;
+        shape[i].n = jb.file_count;
+    }
+    P2G_TRY(ensure_device_ready());
+    p2g_batch* b = new p2g_batch();
+    cudaGetDevice(&b->device);
+    b->flags = flags;
+    b->n_jobs = n;
+    b->ctas = (uint32_t)device_sm_count();
+    b->plan = plan_batch(shape, b->ctas, flags);
+    b->shape = shape;
+    b->n_items = (uint32_t)b->plan.items.size();
+
+    // ---- device arena: descriptors, items, queue, tables, scratch, bases ----
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = round_up(off + bytes, 256);
+        return o;
+    };
+    const size_t o_jobs = take(sizeof(BatchJob) * n);
+    const size_t o_items = take(sizeof(BatchItem) * b->n_items);
+    b->ctl_bytes = sizeof(uint32_t) * (1 + n) + sizeof(int);
+    const size_t o_ctl = take(b->ctl_bytes);
+    const size_t o_files = take(16 * total_files);
+    const size_t o_noff = take(8 * total_files);
+    const size_t o_names = take(names_bytes);
+    std::vector<size_t> o_scratch(n), o_basis(n), o_real(n, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        o_scratch[i] = take(32ull * shape[i].n + 12);
+        o_basis[i] = shape[i].R ? take(basis_bytes(shape[i].S, shape[i].RG)) : 0;
+        if (shape[i].R && jobs[i].slice_size % 16) o_real[i] = take(round_up(jobs[i].slice_size, 16) * shape[i].S);
+    }
+    b->arena_bytes = off;
+    cudaError_t e = cudaMalloc(&b->arena, off);
+    if (e != cudaSuccess) {
+        release(b);
+        return cuda_fail(e, "batch arena");
+    }
+    uint8_t* A = static_cast<uint8_t*>(b->arena);
+    b->d_jobs = reinterpret_cast<BatchJob*>(A + o_jobs);
+    b->d_items = reinterpret_cast<BatchItem*>(A + o_items);
+    b->d_ctl = reinterpret_cast<uint32_t*>(A + o_ctl);
+
+    // ---- host images of the tables ----
+    std::vector<BatchJob> hj(n);
+    std::vector<uint64_t> hfiles(2 * total_files);
+    std::vector<uint32_t> hnoff(2 * total_files);
+    std::vector<uint8_t> hnames(names_bytes, 0);
+    uint64_t fcur = 0, ncur = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const p2g_batch_job& jb = jobs[i];
+        BatchJob& d = hj[i];
+        memset(&d, 0, sizeof d);
+        d.src = jb.src;
+        d.slice = jb.slice_size;
+        d.S = shape[i].S;
+        d.R = jb.recovery_count;
+        d.RG = shape[i].RG;
+        d.n_files = jb.file_count;
+        d.rec = jb.recovery;
+        d.rec_stride = jb.recovery_stride;
+        d.checks = jb.checksums;
+        d.h16k = jb.hash16k;
+        d.pkt = jb.packet_md5;
+        d.set_id = jb.set_id;
+        d.files = reinterpret_cast<const uint64_t*>(A + o_files) + 2 * fcur;
+        d.name_off = reinterpret_cast<const uint32_t*>(A + o_noff) + 2 * fcur;
+        d.names = A + o_names;
+        d.scratch = A + o_scratch[i];
+        d.enc_items = b->plan.enc_items[i];
+        d.first_exp = 0;
+        d.vec = jb.slice_size % 16 == 0 ? 1u : 0u;
+        d.basis = d.R ? reinterpret_cast<uint16_t*>(A + o_basis[i]) : nullptr;
+        if (d.R && jb.slice_size % 16) {
+            d.esrc = A + o_real[i];
+            d.estride = round_up(jb.slice_size, 16);
+            b->realigns.push_back({jb.src, A + o_real[i], jb.slice_size, d.estride, d.S});
+        } else {
+            d.esrc = jb.src;
+            d.estride = jb.slice_size;
+        }
+        if (d.R) b->max_basis_words = std::max<uint64_t>(b->max_basis_words, (uint64_t)d.S * d.RG * 512);
+        uint64_t first = 0;
+        for (uint32_t f = 0; f < jb.file_count; ++f, ++fcur) {
+            hfiles[2 * fcur] = first * jb.slice_size;
+            hfiles[2 * fcur + 1] = jb.file_lengths[f];
+            first += (jb.file_lengths[f] + jb.slice_size - 1) / jb.slice_size;
+            hnoff[2 * fcur] = (uint32_t)ncur;
+            hnoff[2 * fcur + 1] = (uint32_t)jb.name_lens[f];
+            memcpy(hnames.data() + ncur, jb.names[f], jb.name_lens[f]);
+            ncur += round_up(jb.name_lens[f], 4);
+        }
+    }
+    auto up = [&](size_t o, const void* src, size_t bytes) {
+        return bytes ? cudaMemcpy(A + o, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+    };
+    if ((e = up(o_jobs, hj.data(), sizeof(BatchJob) * n)) != cudaSuccess ||
+        (e = up(o_items, b->plan.items.data(), sizeof(BatchItem) * b->n_items)) != cudaSuccess ||
+        (e = up(o_files, hfiles.data(), 8 * hfiles.size())) != cudaSuccess ||
+        (e = up(o_noff, hnoff.data(), 4 * hnoff.size())) != cudaSuccess ||
+        (e = up(o_names, hnames.data(), hnames.size())) != cudaSuccess) {
+        release(b);
+        return cuda_fail(e, "batch tables upload");
+    }
+    b->kernels_per_run = 2 + (uint32_t)b->realigns.size();
+
+    // ---- capture the run into a CUDA graph ----
+    if (!(flags & P2G_BATCH_NO_GRAPH)) {
+        if ((e = prepare_batch_kernel()) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking)) != cudaSuccess) {
+            release(b);
+            return cuda_fail(e, "batch graph stream");
+        }
+        if ((e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+            release(b);
+            return cuda_fail(e, "batch graph capture");
+        }
+        const p2g_status s = enqueue_run(b, b->cap);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(b->cap, &g);
+        b->graph = g;
+        if (s != P2G_OK) {
+            release(b);
+            return s;
+        }
+        if (e != cudaSuccess || (e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess) {
+            release(b);
+            return cuda_fail(e, "batch graph instantiate");
+        }
+    }
+    *out = b;
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_batch_launch(p2g_batch* b, void* stream) {
+    clear_error();
+    if (!b) return set_error(P2G_ERR_INVALID_ARGUMENT, "batch is NULL");
+    P2G_CU(cudaSetDevice(b->device));
+    const cudaStream_t st = (cudaStream_t)stream;
+    if (b->exec) {
+        P2G_CU(cudaGraphLaunch(b->exec, st));
+        add_launches(b->kernels_per_run);
+        return P2G_OK;
+    }
+    return enqueue_run(b, st);
+}
+
+extern "C" p2g_status p2g_batch_check(p2g_batch* b) {
+    clear_error();
+    if (!b) return set_error(P2G_ERR_INVALID_ARGUMENT, "batch is NULL");
+    P2G_CU(cudaSetDevice(b->device));
+    int h = 0;
+    P2G_CU(cudaMemcpy(&h, b->d_ctl + 1 + b->n_jobs, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) return set_error(P2G_ERR_TIMEOUT, "a bounded device wait gave up in the batch kernel (TMA stage never completed)");
+    return P2G_OK;
+}
+
+extern "C" p2g_status p2g_batch_get_info(const p2g_batch* b, p2g_batch_info* out) {
+    clear_error();
+    if (!b || !out) return set_error(P2G_ERR_INVALID_ARGUMENT, "batch or out is NULL");
+    fill_info(b, out);
+    return P2G_OK;
+}
+
+extern "C" uint32_t p2g_batch_job_tile(const p2g_batch* b, uint32_t job) {
+    if (!b || job >= b->n_jobs || !b->shape[job].R) return 0;
+    return b->shape[job].ts;
+}
+
+extern "C" void p2g_batch_destroy(p2g_batch* b) { release(b); }

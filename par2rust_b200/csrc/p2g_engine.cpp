@@ -32,22 +32,12 @@
 
 namespace p2g {
 
-static p2g_status cuda_fail(cudaError_t e, const char* what) {
+p2g_status cuda_fail(cudaError_t e, const char* what) {
     cudaGetLastError();  // clear a sticky-free error so later calls can proceed
     if (e == cudaErrorMemoryAllocation)
         return set_error(P2G_ERR_OOM, "device allocation failed: %s (%s)", cudaGetErrorString(e), what);
     return set_error(P2G_ERR_CUDA, "CUDA error: %s (%s)", cudaGetErrorString(e), what);
 }
-#define P2G_CU(call)                                            \
-    do {                                                        \
-        cudaError_t _e = (call);                                \
-        if (_e != cudaSuccess) return cuda_fail(_e, #call);     \
-    } while (0)
-#define P2G_TRY(expr)                       \
-    do {                                    \
-        p2g_status _s = (expr);             \
-        if (_s != P2G_OK) return _s;        \
-    } while (0)
 
 static inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
@@ -145,6 +135,12 @@ static p2g_status ensure_ready(Context& c) {
 // Optional stage timeline (P2G_TRACE=1): timing events recorded after each
 // stage on its stream, printed to stderr relative to the job start when the
 // job is joined.  Off by default; costs nothing when off.
+p2g_status ensure_device_ready() {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    return ensure_ready(c);
+}
+
 struct Tracer {
     bool on = false;
     cudaEvent_t t0 = nullptr;
@@ -397,41 +393,6 @@ static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) 
 static p2g_status check_device_error(Context& c) {
     if (*c.h_err.as<int>() != 0)
         return set_error(P2G_ERR_TIMEOUT, "a bounded device wait gave up (TMA stage never completed)");
-    return P2G_OK;
-}
-
-// ---------------------------------------------------------------------------
-// Validation shared by the create entry points (src/creator.rs:193-218,
-// :461-508, src/source.rs:65-75).
-// ---------------------------------------------------------------------------
-static p2g_status check_common(uint32_t n, uint32_t R, uint64_t slice) {
-    if (n == 0) return set_error(P2G_ERR_NO_INPUT_FILES, "no input files supplied");
-    if (n > P2G_MAX_FILES)
-        return set_error(P2G_ERR_TOO_MANY_FILES, "too many input files (%u); PAR2 limit is 32768", n);
-    if (R > P2G_MAX_RECOVERY_BLOCKS)
-        return set_error(P2G_ERR_TOO_MANY_RECOVERY_BLOCKS, "recovery block count %u exceeds PAR2 limit of 65535", R);
-    if (slice == 0 || slice % 4)
-        return set_error(P2G_ERR_INVALID_SLICE_SIZE, "invalid slice size %llu: must be > 0 and a multiple of 4",
-                         (unsigned long long)slice);
-    return P2G_OK;
-}
-static p2g_status check_name(const uint8_t* name, size_t len, const char* path) {
-    if (len == 0 || !name || memchr(name, 0, len))
-        return set_error(P2G_ERR_INVALID_FILE_NAME,
-                         "filename \"%s\" is empty or contains a NUL byte; PAR2 does not permit either",
-                         path ? path : "");
-    return P2G_OK;
-}
-static p2g_status check_total_blocks(uint64_t total_blocks, uint64_t total_bytes, uint64_t slice) {
-    if (total_blocks > P2G_MAX_INPUT_BLOCKS) {
-        const uint64_t raw = (total_bytes + P2G_MAX_INPUT_BLOCKS - 1) / P2G_MAX_INPUT_BLOCKS;
-        const uint64_t suggested = (raw + 3) / 4 * 4;
-        set_error_detail(total_blocks, slice, suggested);
-        return set_error(P2G_ERR_TOO_MANY_INPUT_BLOCKS,
-                         "too many input blocks (%llu) at slice_size %llu; PAR2 caps total slices at 32768 — retry "
-                         "with slice_size >= %llu",
-                         (unsigned long long)total_blocks, (unsigned long long)slice, (unsigned long long)suggested);
-    }
     return P2G_OK;
 }
 

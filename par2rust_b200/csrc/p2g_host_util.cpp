@@ -355,6 +355,41 @@ Md5 file_id_of(const uint8_t hash16k[16], uint64_t length, const uint8_t* name, 
 }
 
 // ---------------------------------------------------------------------------
+// Validation shared by the create entry points (src/creator.rs:193-218,
+// :461-508, src/source.rs:65-75).
+// ---------------------------------------------------------------------------
+p2g_status check_common(uint32_t n, uint32_t R, uint64_t slice) {
+    if (n == 0) return set_error(P2G_ERR_NO_INPUT_FILES, "no input files supplied");
+    if (n > P2G_MAX_FILES)
+        return set_error(P2G_ERR_TOO_MANY_FILES, "too many input files (%u); PAR2 limit is 32768", n);
+    if (R > P2G_MAX_RECOVERY_BLOCKS)
+        return set_error(P2G_ERR_TOO_MANY_RECOVERY_BLOCKS, "recovery block count %u exceeds PAR2 limit of 65535", R);
+    if (slice == 0 || slice % 4)
+        return set_error(P2G_ERR_INVALID_SLICE_SIZE, "invalid slice size %llu: must be > 0 and a multiple of 4",
+                         (unsigned long long)slice);
+    return P2G_OK;
+}
+p2g_status check_name(const uint8_t* name, size_t len, const char* path) {
+    if (len == 0 || !name || memchr(name, 0, len))
+        return set_error(P2G_ERR_INVALID_FILE_NAME,
+                         "filename \"%s\" is empty or contains a NUL byte; PAR2 does not permit either",
+                         path ? path : "");
+    return P2G_OK;
+}
+p2g_status check_total_blocks(uint64_t total_blocks, uint64_t total_bytes, uint64_t slice) {
+    if (total_blocks > P2G_MAX_INPUT_BLOCKS) {
+        const uint64_t raw = (total_bytes + P2G_MAX_INPUT_BLOCKS - 1) / P2G_MAX_INPUT_BLOCKS;
+        const uint64_t suggested = (raw + 3) / 4 * 4;
+        set_error_detail(total_blocks, slice, suggested);
+        return set_error(P2G_ERR_TOO_MANY_INPUT_BLOCKS,
+                         "too many input blocks (%llu) at slice_size %llu; PAR2 caps total slices at 32768 — retry "
+                         "with slice_size >= %llu",
+                         (unsigned long long)total_blocks, (unsigned long long)slice, (unsigned long long)suggested);
+    }
+    return P2G_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Volumes
 // ---------------------------------------------------------------------------
 p2g_status resolve_volume_sizes(const p2g_volume_scheme& sc, uint32_t total, std::vector<uint32_t>& out) {

@@ -62,6 +62,12 @@ Md5 file_id_of(const uint8_t hash16k[16], uint64_t length, const uint8_t* name, 
 p2g_status resolve_volume_sizes(const p2g_volume_scheme& sc, uint32_t total, std::vector<uint32_t>& out);
 std::string volume_filename(const std::string& index_path, uint16_t first_exp, uint32_t count);
 
+// ---- validation shared by the create entry points (src/creator.rs:193-218,
+// :461-508, src/source.rs:65-75); each sets the error message ----
+p2g_status check_common(uint32_t n, uint32_t R, uint64_t slice);
+p2g_status check_name(const uint8_t* name, size_t len, const char* path);
+p2g_status check_total_blocks(uint64_t total_blocks, uint64_t total_bytes, uint64_t slice);
+
 // ---- filesystem ----
 p2g_status write_atomic(const std::string& path, const std::vector<std::pair<const uint8_t*, size_t>>& pieces);
 

@@ -11,6 +11,24 @@
 
 namespace p2g {
 
+// CUDA error -> status (P2G_ERR_OOM for allocation failures, else
+// P2G_ERR_CUDA) with the message set; clears the runtime's last error.
+p2g_status cuda_fail(cudaError_t e, const char* what);
+#define P2G_CU(call)                                                \
+    do {                                                            \
+        cudaError_t _e = (call);                                    \
+        if (_e != cudaSuccess) return ::p2g::cuda_fail(_e, #call);  \
+    } while (0)
+#define P2G_TRY(expr)                \
+    do {                             \
+        p2g_status _s = (expr);      \
+        if (_s != P2G_OK) return _s; \
+    } while (0)
+
+// Select the engine's device, check it is sm_100 and upload the GF tables
+// (idempotent; serialised with the engine's other calls).
+p2g_status ensure_device_ready();
+
 // GF(2^16) constants of src/galois.rs:15-18.
 constexpr uint32_t kFieldLimit = 65535u;
 constexpr uint32_t kFieldGenerator = 0x1100Bu;
@@ -34,8 +52,10 @@ struct FileSpan {
 // __device__ arrays of the current device (idempotent per device).
 cudaError_t upload_tables();
 
-// Number of kernels launched so far (all wrappers bump it).
+// Number of kernels launched so far (all wrappers bump it; graph replays
+// add their kernel count with add_launches).
 uint64_t launch_count();
+void add_launches(uint64_t n);
 
 cudaError_t launch_basis(uint16_t* basis, uint32_t S, uint32_t RG, uint32_t R, uint32_t first_exp,
                          cudaStream_t st);
@@ -93,5 +113,57 @@ cudaError_t launch_encode_noheap(const uint8_t* src, uint64_t src_stride, uint32
 
 // Size in bytes of the coefficient-basis scratch for S slices and RG groups.
 inline size_t basis_bytes(uint32_t S, uint32_t RG) { return (size_t)S * RG * 512 * sizeof(uint16_t); }
+
+// ---------------------------------------------------------------------------
+// Batched create (p2g_batch.cpp): the work items of many jobs run in one
+// persistent launch, one CTA per SM popping items off a device queue.
+// ---------------------------------------------------------------------------
+enum BatchItemKind : uint32_t {
+    kItemScan = 0,    // slice MD5 + CRC32 of up to kScanSlices slices
+    kItemEncode = 1,  // one (row group, symbol tile) of the accumulator
+    kItemFinish = 2,  // hash16k, set id and packet MD5s of a job without encode items
+};
+constexpr uint32_t kScanSlices = 256;  // one slice per MD5 lane
+
+struct BatchItem {
+    uint32_t job;
+    uint32_t kind_rg;  // kind in bits 0-7, row group in bits 8-31
+    uint32_t a, b;     // scan: first slice, count; encode: first symbol, symbol count
+};
+
+// Device descriptor of one job.  The CTA that completes a job's last encode
+// item (or runs its finish item) also derives the job's hash16k values, file
+// ids, set id and recovery-packet MD5s.
+struct BatchJob {
+    const uint8_t* src;        // files back to back, each on a slice boundary, zero-padded
+    const uint8_t* esrc;       // encode source: src, or a copy with 16-byte aligned slices
+    uint16_t* basis;           // [s][row group][16][32] coefficient basis
+    uint8_t* rec;              // recovery row r at rec + r*rec_stride
+    p2g_slice_checksum* checks;
+    uint8_t* h16k;             // 16 bytes per file
+    uint8_t* pkt;              // 16 bytes per recovery row
+    uint8_t* set_id;           // 16 bytes
+    const uint64_t* files;     // 2 per file: byte offset in src, length
+    const uint8_t* names;      // display names, each starting 4-byte aligned
+    const uint32_t* name_off;  // 2 per file: offset into names, length
+    uint8_t* scratch;          // 16*n file ids, then the 12+16*n main-packet body
+    uint64_t slice, estride, rec_stride;
+    uint32_t S, R, RG, n_files;
+    uint32_t enc_items, first_exp;
+    uint32_t vec;  // slices and file starts of src are 16-byte aligned
+    uint32_t pad;
+};
+
+// Shared memory of one batch CTA.
+size_t batch_smem_bytes();
+// Fills every job's basis (one launch; blockIdx.y = job).
+cudaError_t launch_basis_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_words, cudaStream_t st);
+// The persistent kernel: `ctas` CTAs; ctl[0] queue head, ctl[1+j] completed
+// encode items of job j (zeroed before each launch).
+// Sets the batch kernel's shared-memory attribute (call before stream capture).
+cudaError_t prepare_batch_kernel();
+cudaError_t launch_batch(const BatchJob* jobs, const BatchItem* items, uint32_t n_items, uint32_t* ctl, int* err,
+                         uint32_t ctas, cudaStream_t st);
+int device_sm_count();
 
 }  // namespace p2g

@@ -29,6 +29,7 @@ __device__ uint16_t d_logbase[32768];
 static std::atomic<uint64_t> g_launches{0};
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 static inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void add_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 cudaError_t upload_tables() {
     static std::mutex mu;
@@ -137,11 +138,10 @@ __device__ __forceinline__ uint32_t lds32(uint32_t addr) {
 // (lane = row pair + 16*hi) hit 32 distinct banks.  Rows r >= R get 0 (their
 // tables are all-zero and never stored).
 // ---------------------------------------------------------------------------
-__global__ void basis_kernel(uint16_t* __restrict__ basis, uint32_t S, uint32_t RG, uint32_t R,
-                             uint32_t first_exp) {
+__device__ __forceinline__ void basis_fill(uint16_t* __restrict__ basis, uint32_t S, uint32_t RG, uint32_t R,
+                                           uint32_t first_exp, uint64_t start, uint64_t step) {
     const uint64_t total = (uint64_t)S * RG * 512;
-    for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t idx = start; idx < total; idx += step) {
         const uint32_t rl = (uint32_t)(idx & 31);
         const uint32_t hi = (uint32_t)((idx >> 5) & 1);
         const uint32_t jj = (uint32_t)((idx >> 6) & 7);
@@ -160,6 +160,12 @@ __global__ void basis_kernel(uint16_t* __restrict__ basis, uint32_t S, uint32_t 
         }
         basis[idx] = v;
     }
+}
+
+__global__ void basis_kernel(uint16_t* __restrict__ basis, uint32_t S, uint32_t RG, uint32_t R,
+                             uint32_t first_exp) {
+    basis_fill(basis, S, RG, R, first_exp, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
+               (uint64_t)gridDim.x * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -197,32 +203,29 @@ __host__ __device__ constexpr size_t encode_smem_bytes() {
            kEncStages * sizeof(uint64_t);
 }
 
+// One (row group, symbol tile) work unit of the accumulator: 32 rows x
+// tile_syms symbols from n0, over all S input slices.  `phase` holds the
+// mbarrier parity of each stage's next use, so a persistent CTA can run
+// tiles back to back on the same barriers; it is advanced on return.
+// Returns false (uniformly over the CTA) when a bounded TMA wait gave up;
+// copies still in flight have then been waited for.
 template <int NCH>
-__global__ void __launch_bounds__(kEncThreads, 1)
-    encode_lut_kernel(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S,
-                      const uint16_t* __restrict__ basis, uint32_t RG, uint32_t R, uint32_t sym_begin,
-                      uint32_t sym_end, uint32_t TS, uint8_t* __restrict__ rec, uint64_t rec_stride,
-                      int* __restrict__ err) {
+__device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S,
+                                            const uint16_t* __restrict__ basis, uint32_t RG, uint32_t rg,
+                                            uint32_t R, uint32_t n0, uint32_t tile_syms,
+                                            uint8_t* __restrict__ rec, uint64_t rec_stride, uint8_t* smem,
+                                            uint32_t& phase) {
     constexpr int WARPS = kEncThreads / 32;
-    constexpr int NT = WARPS * NCH * 64;  // symbol capacity of a tile (TS <= NT)
-    extern __shared__ __align__(128) uint8_t smem[];
+    constexpr int NT = WARPS * NCH * 64;  // symbol capacity of a tile (tile_syms <= NT)
     uint8_t* tabs = smem;
     uint8_t* src_st = smem + 2 * kTabBytes;
     uint8_t* bas_st = src_st + kEncStages * NT * 2;
     uint64_t* bars = reinterpret_cast<uint64_t*>(bas_st + kEncStages * 1024);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t tile = blockIdx.x / RG, rg = blockIdx.x % RG;
-    const uint32_t n0 = sym_begin + tile * TS;
-    if (n0 >= sym_end) return;  // uniform: empty tile at the end of a band
-    const uint32_t tile_syms = min(TS, sym_end - n0);
     const uint32_t tile_bytes = tile_syms * 2;
-
-    if (tid == 0) {
-        for (int st = 0; st < kEncStages; ++st) mbar_init(&bars[st], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
+    const uint32_t ph = phase;
+    auto parity = [&](uint32_t s) { return ((ph >> (s % kEncStages)) ^ (s / kEncStages)) & 1u; };
 
     auto issue = [&](uint32_t s, int st) {
         mbar_arrive_expect_tx(&bars[st], tile_bytes + 1024);
@@ -278,15 +281,13 @@ __global__ void __launch_bounds__(kEncThreads, 1)
 
     int bad = 0;
     if (S > 0) {
-        if (!mbar_wait_bounded(&bars[0], 0)) bad = 1;
+        if (!mbar_wait_bounded(&bars[0], parity(0))) bad = 1;
         build(0, 0);
     }
     if (__syncthreads_or(bad)) {
-        if (tid == 0) {
-            atomicOr(err, 1);
-            for (uint32_t s2 = 1; s2 < S && s2 < (uint32_t)kEncStages; ++s2) mbar_wait_bounded(&bars[s2], 0);
-        }
-        return;
+        if (tid == 0)
+            for (uint32_t s2 = 1; s2 < S && s2 < (uint32_t)kEncStages; ++s2) mbar_wait_bounded(&bars[s2], parity(s2));
+        return false;
     }
 
     for (uint32_t s = 0; s < S; ++s) {
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(kEncThreads, 1)
         const int t = (int)(s & 1);
         if (s + 1 < S) {
             const int st1 = (int)((s + 1) % kEncStages);
-            if (!mbar_wait_bounded(&bars[st1], ((s + 1) / kEncStages) & 1)) bad = 1;
+            if (!mbar_wait_bounded(&bars[st1], parity(s + 1))) bad = 1;
             build(t ^ 1, st1);
         }
         const uint32_t baseA = tab_u32 + t * kTabBytes + offA;
@@ -322,16 +323,19 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             }
         }
         if (__syncthreads_or(bad)) {
-            if (tid == 0) {
-                atomicOr(err, 1);
-                // drain copies still in flight before the CTA's shared memory goes away
+            if (tid == 0)  // drain copies still in flight before the CTA's shared memory goes away
                 for (uint32_t s2 = s + 1; s2 < S && s2 < s + kEncStages; ++s2)
-                    mbar_wait_bounded(&bars[s2 % kEncStages], (s2 / kEncStages) & 1);
-            }
-            return;
+                    mbar_wait_bounded(&bars[s2 % kEncStages], parity(s2));
+            return false;
         }
         if (tid == 0 && s + kEncStages < S) issue(s + kEncStages, st);
     }
+    // stage st was used ceil((S - st) / kEncStages) times: flip its parity if odd
+    uint32_t flip = 0;
+#pragma unroll
+    for (int st = 0; st < kEncStages; ++st)
+        if ((uint32_t)st < S && (((S - 1 - st) / kEncStages) & 1u) == 0) flip |= 1u << st;
+    phase = ph ^ flip;
 
     // Epilogue: transpose (symbol-major, row pairs packed) into row-major
     // 16-byte runs of 8 symbols and store.
@@ -358,6 +362,31 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             }
         }
     }
+    return true;
+}
+
+template <int NCH>
+__global__ void __launch_bounds__(kEncThreads, 1)
+    encode_lut_kernel(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S,
+                      const uint16_t* __restrict__ basis, uint32_t RG, uint32_t R, uint32_t sym_begin,
+                      uint32_t sym_end, uint32_t TS, uint8_t* __restrict__ rec, uint64_t rec_stride,
+                      int* __restrict__ err) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    constexpr int NT = (kEncThreads / 32) * NCH * 64;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * kTabBytes + kEncStages * (NT * 2 + 1024));
+    const uint32_t tile = blockIdx.x / RG, rg = blockIdx.x % RG;
+    const uint32_t n0 = sym_begin + tile * TS;
+    if (n0 >= sym_end) return;  // uniform: empty tile at the end of a band
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kEncStages; ++st) mbar_init(&bars[st], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    if (!encode_tile<NCH>(src, src_stride, S, basis, RG, rg, R, n0, min(TS, sym_end - n0), rec, rec_stride, smem,
+                          phase) &&
+        threadIdx.x == 0)
+        atomicOr(err, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -482,13 +511,15 @@ __device__ __forceinline__ void md5_compress(uint32_t st[4], const uint32_t m[16
     st[3] += d;
 }
 
-template <bool VEC>
+// CG: load through L2 only (data written earlier in the same launch by
+// other CTAs or by this one); otherwise through the read-only path.
+template <bool VEC, bool CG = false>
 __device__ __forceinline__ void md5_load_block(uint32_t m[16], const uint8_t* p) {
     if (VEC) {
         const uint4* q = reinterpret_cast<const uint4*>(p);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const uint4 v = __ldg(q + i);
+            const uint4 v = CG ? __ldcg(q + i) : __ldg(q + i);
             m[4 * i] = v.x;
             m[4 * i + 1] = v.y;
             m[4 * i + 2] = v.z;
@@ -497,7 +528,7 @@ __device__ __forceinline__ void md5_load_block(uint32_t m[16], const uint8_t* p)
     } else {
         const uint32_t* q = reinterpret_cast<const uint32_t*>(p);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) m[i] = __ldg(q + i);
+        for (int i = 0; i < 16; ++i) m[i] = CG ? __ldcg(q + i) : __ldg(q + i);
     }
 }
 
@@ -508,18 +539,19 @@ __device__ uint32_t md5_stream_word(const uint32_t* pre, uint32_t pre_bytes, con
     if (q == last_start + 60) return (uint32_t)(total >> 29);
     if (q < pre_bytes) return pre[q >> 2];
     const uint64_t d = q - pre_bytes;
-    if (d + 4 <= len) return *reinterpret_cast<const uint32_t*>(data + d);
+    // L2-only loads: the data may have been written earlier in the same launch
+    if (d + 4 <= len) return __ldcg(reinterpret_cast<const uint32_t*>(data + d));
     uint32_t w = 0;
     for (int t = 0; t < 4; ++t) {
         const uint64_t pos = d + t;
-        const uint32_t byte = pos < len ? data[pos] : (pos == len ? 0x80u : 0u);
+        const uint32_t byte = pos < len ? (uint32_t)__ldcg(data + pos) : (pos == len ? 0x80u : 0u);
         w |= byte << (8 * t);
     }
     return w;
 }
 
 // Blocks [b_from, b_to) of the padded message prefix ‖ data.
-template <bool VEC>
+template <bool VEC, bool CG = false>
 __device__ void md5_range(uint32_t st[4], const uint32_t* pre, uint32_t pre_bytes, const uint8_t* data, uint64_t len,
                           uint64_t b_from, uint64_t b_to) {
     const uint64_t total = pre_bytes + len;
@@ -537,11 +569,11 @@ __device__ void md5_range(uint32_t st[4], const uint32_t* pre, uint32_t pre_byte
     }
     const uint64_t fast_end = fb1 < b_to ? fb1 : b_to;
     if (b < fast_end) {
-        md5_load_block<VEC>(m, data + 64 * b - pre_bytes);
+        md5_load_block<VEC, CG>(m, data + 64 * b - pre_bytes);
         for (; b < fast_end; ++b) {
             uint32_t nx[16];
             const uint64_t nb = b + 1 < fast_end ? b + 1 : b;
-            md5_load_block<VEC>(nx, data + 64 * nb - pre_bytes);
+            md5_load_block<VEC, CG>(nx, data + 64 * nb - pre_bytes);
             md5_compress(st, m);
 #pragma unroll
             for (int i = 0; i < 16; ++i) m[i] = nx[i];
@@ -799,11 +831,9 @@ __device__ uint32_t x_pow_8n(uint64_t n) {
     return result;
 }
 
-template <bool VEC>
-__global__ void __launch_bounds__(64) crc_slices_kernel(const uint8_t* __restrict__ src, uint64_t stride,
-                                                         uint32_t count, uint64_t slice_size,
-                                                         p2g_slice_checksum* __restrict__ out) {
-    __shared__ uint32_t T[4][256];
+// Slicing-by-4 tables T[t][b] (T[0] the byte table) into shared memory,
+// built by all threads of the block (contains __syncthreads).
+__device__ __forceinline__ void crc_tables_build(uint32_t (*T)[256]) {
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         uint32_t c = (uint32_t)i;
         for (int b = 0; b < 8; ++b) c = (c >> 1) ^ ((c & 1u) ? kCrcPoly : 0u);
@@ -817,36 +847,66 @@ __global__ void __launch_bounds__(64) crc_slices_kernel(const uint8_t* __restric
         }
         __syncthreads();
     }
-    const int lane = threadIdx.x & 31;
-    const uint32_t wpb = blockDim.x >> 5;
+}
+
+// Lane chunk of a slice of W = slice_size/4 words: [start, end) words, and
+// K = x^(8 * bytes after the chunk) mod P that moves its partial CRC to the
+// end of the slice.
+struct CrcLane {
+    uint64_t start, end;
+    uint32_t K;
+};
+template <bool VEC>
+__device__ __forceinline__ CrcLane crc_lane(uint64_t slice_size, int lane) {
     const uint64_t W = slice_size / 4;
     uint64_t cw = (W + 31) / 32;
     if (VEC) cw = (cw + 3) & ~3ull;
-    const uint64_t start = min((uint64_t)lane * cw, W), end = min(start + cw, W);
-    const uint32_t K = x_pow_8n(slice_size - end * 4);
-    for (uint64_t s = (uint64_t)blockIdx.x * wpb + (threadIdx.x >> 5); s < count; s += (uint64_t)gridDim.x * wpb) {
-        const uint32_t* p = reinterpret_cast<const uint32_t*>(src + (size_t)s * stride);
-        uint32_t c = lane == 0 ? 0xFFFFFFFFu : 0u;
-        uint64_t w = start;
-        if (VEC) {
-            for (; w + 4 <= end; w += 4) {
-                const uint4 v = __ldg(reinterpret_cast<const uint4*>(p + w));
-                const uint32_t vv[4] = {v.x, v.y, v.z, v.w};
+    CrcLane c;
+    c.start = min((uint64_t)lane * cw, W);
+    c.end = min(c.start + cw, W);
+    c.K = x_pow_8n(slice_size - c.end * 4);
+    return c;
+}
+
+// CRC32 of one slice by one warp (all 32 lanes call it with the same p).
+template <bool VEC>
+__device__ __forceinline__ uint32_t crc_slice_warp(const uint32_t* __restrict__ p, const CrcLane& cl, int lane,
+                                                   const uint32_t (*T)[256]) {
+    uint32_t c = lane == 0 ? 0xFFFFFFFFu : 0u;
+    uint64_t w = cl.start;
+    if (VEC) {
+        for (; w + 4 <= cl.end; w += 4) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(p + w));
+            const uint32_t vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    c ^= vv[q];
-                    c = T[3][c & 0xFF] ^ T[2][(c >> 8) & 0xFF] ^ T[1][(c >> 16) & 0xFF] ^ T[0][c >> 24];
-                }
+            for (int q = 0; q < 4; ++q) {
+                c ^= vv[q];
+                c = T[3][c & 0xFF] ^ T[2][(c >> 8) & 0xFF] ^ T[1][(c >> 16) & 0xFF] ^ T[0][c >> 24];
             }
         }
-        for (; w < end; ++w) {
-            c ^= __ldg(p + w);
-            c = T[3][c & 0xFF] ^ T[2][(c >> 8) & 0xFF] ^ T[1][(c >> 16) & 0xFF] ^ T[0][c >> 24];
-        }
-        c = gf2_mulmod(c, K);
+    }
+    for (; w < cl.end; ++w) {
+        c ^= __ldg(p + w);
+        c = T[3][c & 0xFF] ^ T[2][(c >> 8) & 0xFF] ^ T[1][(c >> 16) & 0xFF] ^ T[0][c >> 24];
+    }
+    c = gf2_mulmod(c, cl.K);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) c ^= __shfl_xor_sync(0xFFFFFFFFu, c, o);
-        if (lane == 0) out[s].crc32 = c ^ 0xFFFFFFFFu;
+    for (int o = 16; o > 0; o >>= 1) c ^= __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    return c ^ 0xFFFFFFFFu;
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(64) crc_slices_kernel(const uint8_t* __restrict__ src, uint64_t stride,
+                                                         uint32_t count, uint64_t slice_size,
+                                                         p2g_slice_checksum* __restrict__ out) {
+    __shared__ uint32_t T[4][256];
+    crc_tables_build(T);
+    const int lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x >> 5;
+    const CrcLane cl = crc_lane<VEC>(slice_size, lane);
+    for (uint64_t s = (uint64_t)blockIdx.x * wpb + (threadIdx.x >> 5); s < count; s += (uint64_t)gridDim.x * wpb) {
+        const uint32_t c = crc_slice_warp<VEC>(reinterpret_cast<const uint32_t*>(src + (size_t)s * stride), cl, lane, T);
+        if (lane == 0) out[s].crc32 = c;
     }
 }
 
@@ -860,6 +920,209 @@ __global__ void realign_kernel(const uint8_t* __restrict__ src, uint64_t src_str
         reinterpret_cast<uint32_t*>(dst + s * dst_stride)[w] =
             reinterpret_cast<const uint32_t*>(src + s * src_stride)[w];
     }
+}
+
+// ---------------------------------------------------------------------------
+// Batched create.  One CTA per SM pops work items off a device queue until
+// it is empty.  Items of one job never wait for one another: the CTA whose
+// encode item completes a job (counted with an atomic after a release fence)
+// runs that job's finish step itself, so the launch has no inter-CTA waits.
+//
+// Shared memory: the encode region (tables, TMA ring, mbarriers), a cp.async
+// ring of kRingLaneBytes for each of the kHashThreads MD5 lanes, the CRC32
+// tables and a few words of per-CTA state.
+// ---------------------------------------------------------------------------
+constexpr size_t kBatchEncBytes = encode_smem_bytes<kEncChunks>();
+constexpr size_t kBatchRingBytes = (size_t)kHashThreads * kRingLaneBytes;
+constexpr size_t kBatchSmem = kBatchEncBytes + kBatchRingBytes + 4 * 256 * 4 + 64;
+static_assert(kBatchEncBytes % 16 == 0, "MD5 rings must start 16-byte aligned");
+size_t batch_smem_bytes() { return kBatchSmem; }
+
+__device__ __forceinline__ void store_digest(uint8_t* out, const uint32_t st[4]) {
+    uint32_t* o = reinterpret_cast<uint32_t*>(out);  // 4-byte aligned
+    o[0] = st[0];
+    o[1] = st[1];
+    o[2] = st[2];
+    o[3] = st[3];
+}
+
+// a < b comparing the 16 digest bytes in order (words hold them little-endian)
+__device__ __forceinline__ bool id_less(const uint4& a, const uint4& b) {
+    const uint32_t x[4] = {a.x, a.y, a.z, a.w}, y[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const uint32_t p = __byte_perm(x[i], 0u, 0x0123), q = __byte_perm(y[i], 0u, 0x0123);
+        if (p != q) return p < q;
+    }
+    return false;
+}
+__device__ __forceinline__ bool id_eq(const uint4& a, const uint4& b) {
+    return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w;
+}
+
+// Slices [first, first+count) of job J: MD5 on the kHashThreads lanes (one
+// slice each, staged through the lane's ring), CRC32 on the remaining warps
+// (one slice per warp at a time).
+template <bool VEC>
+__device__ __forceinline__ void batch_scan(const BatchJob& J, uint32_t first, uint32_t count, uint32_t ring,
+                                           const uint32_t (*T)[256]) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < kHashThreads) {
+        if ((uint32_t)tid < count) {
+            const uint32_t s = first + tid;
+            uint32_t st[4];
+            md5_init(st);
+            md5_range_ring<0, VEC>(st, nullptr, J.src + (size_t)s * J.slice, J.slice, 0, ~0ull,
+                                   ring + tid * kRingLaneBytes);
+            store_digest(J.checks[s].md5, st);
+        }
+    } else {
+        constexpr uint32_t kCrcWarps = (kEncThreads - kHashThreads) / 32;
+        const CrcLane cl = crc_lane<VEC>(J.slice, lane);
+        for (uint32_t i = (uint32_t)warp - kHashThreads / 32; i < count; i += kCrcWarps) {
+            const uint32_t s = first + i;
+            const uint32_t c =
+                crc_slice_warp<VEC>(reinterpret_cast<const uint32_t*>(J.src + (size_t)s * J.slice), cl, lane, T);
+            if (lane == 0) J.checks[s].crc32 = c;
+        }
+    }
+}
+
+// Finish step of job J (all threads of the CTA):
+//   hash16k of each file and its file id MD5(hash16k ‖ length le64 ‖ name)
+//   (src/source.rs:303-309); the main-packet body slice_size le64 ‖ count
+//   le32 ‖ file ids in byte order, whose MD5 is the set id
+//   (src/packet/main_packet.rs:25-42); then each recovery row's packet MD5
+//   over set_id ‖ "PAR 2.0\0RecvSlic" ‖ exponent le32 ‖ row
+//   (src/packet/recovery.rs:15, src/format.rs:33-54).
+template <bool VEC>
+__device__ void batch_finish(const BatchJob& J, uint32_t ring, uint32_t* sid) {
+    const int tid = threadIdx.x;
+    const uint32_t n = J.n_files;
+    uint4* ids = reinterpret_cast<uint4*>(J.scratch);
+    uint8_t* body = J.scratch + 16 * (size_t)n;
+    if (tid < kHashThreads) {
+        for (uint32_t f = tid; f < n; f += kHashThreads) {
+            const uint64_t off = J.files[2 * f], len = J.files[2 * f + 1];
+            uint32_t h[4];
+            md5_init(h);
+            md5_range_ring<0, VEC>(h, nullptr, J.src + off, len < P2G_HASH16K_LEN ? len : P2G_HASH16K_LEN, 0,
+                                   ~0ull, ring + tid * kRingLaneBytes);
+            store_digest(J.h16k + 16 * (size_t)f, h);
+            const uint32_t pre[6] = {h[0], h[1], h[2], h[3], (uint32_t)len, (uint32_t)(len >> 32)};
+            uint32_t id[4];
+            md5_init(id);
+            md5_range<false>(id, pre, 24, J.names + J.name_off[2 * f], J.name_off[2 * f + 1], 0, ~0ull);
+            __stcg(ids + f, make_uint4(id[0], id[1], id[2], id[3]));
+        }
+    }
+    __syncthreads();
+    // rank sort: ties keep file order (equal ids are interchangeable anyway)
+    for (uint32_t f = tid; f < n; f += blockDim.x) {
+        const uint4 me = __ldcg(ids + f);
+        uint32_t rank = 0;
+        for (uint32_t g = 0; g < n; ++g) {
+            const uint4 o = __ldcg(ids + g);
+            rank += (id_less(o, me) || (g < f && id_eq(o, me))) ? 1u : 0u;
+        }
+        uint32_t* d = reinterpret_cast<uint32_t*>(body + 12 + 16 * (size_t)rank);
+        __stcg(d, me.x);
+        __stcg(d + 1, me.y);
+        __stcg(d + 2, me.z);
+        __stcg(d + 3, me.w);
+    }
+    if (tid == 0) {
+        uint32_t* b = reinterpret_cast<uint32_t*>(body);
+        __stcg(b, (uint32_t)J.slice);
+        __stcg(b + 1, (uint32_t)(J.slice >> 32));
+        __stcg(b + 2, n);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t s[4];
+        md5_init(s);
+        md5_range<false, true>(s, nullptr, 0, body, 12 + 16 * (uint64_t)n, 0, ~0ull);
+        sid[0] = s[0];
+        sid[1] = s[1];
+        sid[2] = s[2];
+        sid[3] = s[3];
+        store_digest(J.set_id, s);
+    }
+    __syncthreads();
+    if (tid < kHashThreads) {
+        for (uint32_t r = tid; r < J.R; r += kHashThreads) {
+            // set id ‖ "PAR 2.0\0" "RecvSlic" as little-endian words ‖ exponent
+            const uint32_t pre[9] = {sid[0], sid[1], sid[2], sid[3], 0x20524150u, 0x00302E32u, 0x76636552u,
+                                     0x63696C53u, J.first_exp + r};
+            uint32_t st[4];
+            md5_init(st);
+            md5_range_ring<9, true>(st, pre, J.rec + (size_t)r * J.rec_stride, J.slice, 0, ~0ull,
+                                    ring + tid * kRingLaneBytes);
+            store_digest(J.pkt + 16 * (size_t)r, st);
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kEncThreads, 1)
+    batch_kernel(const BatchJob* __restrict__ jobs, const BatchItem* __restrict__ items, uint32_t n_items,
+                 uint32_t* __restrict__ ctl, int* __restrict__ err) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    constexpr int NT = (kEncThreads / 32) * kEncChunks * 64;
+    uint8_t* enc = smem;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(enc + 2 * kTabBytes + kEncStages * (NT * 2 + 1024));
+    uint8_t* ring_p = smem + kBatchEncBytes;
+    uint32_t(*T)[256] = reinterpret_cast<uint32_t(*)[256]>(ring_p + kBatchRingBytes);
+    uint32_t* misc = reinterpret_cast<uint32_t*>(ring_p + kBatchRingBytes + 4 * 256 * 4);  // [0] item [1] last [4..7] set id
+    const uint32_t ring = smem_u32(ring_p);
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int st = 0; st < kEncStages; ++st) mbar_init(&bars[st], 1);
+        fence_mbar_init();
+    }
+    crc_tables_build(T);  // ends with __syncthreads
+    uint32_t phase = 0;
+    for (;;) {
+        if (tid == 0) misc[0] = *reinterpret_cast<volatile int*>(err) ? n_items : atomicAdd(&ctl[0], 1u);
+        __syncthreads();
+        const uint32_t idx = misc[0];
+        if (idx >= n_items) break;
+        const BatchItem it = items[idx];
+        const BatchJob& J = jobs[it.job];
+        const uint32_t kind = it.kind_rg & 0xFFu;
+        if (kind == kItemScan) {
+            if (J.vec)
+                batch_scan<true>(J, it.a, it.b, ring, T);
+            else
+                batch_scan<false>(J, it.a, it.b, ring, T);
+            __syncthreads();
+            continue;
+        }
+        if (kind == kItemEncode) {
+            if (!encode_tile<kEncChunks>(J.esrc, J.estride, J.S, J.basis, J.RG, it.kind_rg >> 8, J.R, it.a, it.b,
+                                         J.rec, J.rec_stride, enc, phase)) {
+                if (tid == 0) atomicOr(err, 1);
+                break;
+            }
+            __threadfence();  // release this tile's rows before counting it
+            __syncthreads();
+            if (tid == 0) misc[1] = (atomicAdd(&ctl[1 + it.job], 1u) + 1 == J.enc_items) ? 1u : 0u;
+            __syncthreads();
+            if (!misc[1]) continue;
+            __threadfence();  // acquire: every tile of the job is visible from here on
+        }
+        if (J.vec)
+            batch_finish<true>(J, ring, misc + 4);
+        else
+            batch_finish<false>(J, ring, misc + 4);
+    }
+}
+
+__global__ void basis_batch_kernel(const BatchJob* __restrict__ jobs) {
+    const BatchJob& J = jobs[blockIdx.y];
+    if (!J.R) return;
+    basis_fill(J.basis, J.S, J.RG, J.R, J.first_exp, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
+               (uint64_t)gridDim.x * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1170,6 +1433,39 @@ cudaError_t launch_realign(const uint8_t* src, uint64_t src_stride, uint8_t* dst
     const uint64_t want = (total + 255) / 256;
     const unsigned blocks = (unsigned)(want < (uint64_t)sm_count() * 16 ? want : (uint64_t)sm_count() * 16);
     realign_kernel<<<blocks, 256, 0, st>>>(src, src_stride, dst, dst_stride, count, slice_size);
+    count_launch();
+    return cudaGetLastError();
+}
+
+int device_sm_count() { return sm_count(); }
+
+cudaError_t launch_basis_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_words, cudaStream_t st) {
+    if (!n_jobs || !max_words) return cudaSuccess;
+    const uint64_t want = (max_words + 255) / 256;
+    const unsigned bx = (unsigned)(want < (uint64_t)sm_count() * 4 ? want : (uint64_t)sm_count() * 4);
+    basis_batch_kernel<<<dim3(bx, n_jobs), 256, 0, st>>>(jobs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t prepare_batch_kernel() {
+    static bool attr_set[256] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 256 || !attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 256) attr_set[dev] = true;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_batch(const BatchJob* jobs, const BatchItem* items, uint32_t n_items, uint32_t* ctl, int* err,
+                         uint32_t ctas, cudaStream_t st) {
+    if (!n_items) return cudaSuccess;
+    cudaError_t e = prepare_batch_kernel();
+    if (e != cudaSuccess) return e;
+    batch_kernel<<<ctas, kEncThreads, kBatchSmem, st>>>(jobs, items, n_items, ctl, err);
     count_launch();
     return cudaGetLastError();
 }

@@ -1,0 +1,263 @@
+"""Batched create: many jobs in one persistent, graph-captured launch.
+
+GPU tests compare every output of every job in a heterogeneous batch with
+the oracle (recovery rows, slice MD5/CRC32, hash16k, set id, packet MD5s),
+with the plain per-job device path, and with the same job batched alone:
+results must be byte-identical however the job is mixed.  CPU tests cover
+the planner (items, tile search, predicted makespan).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from par2rust_b200.workloads import file_bytes
+
+
+def _shape_items(slice_, S, R):
+    Np = (slice_ + 15) // 16 * 16 // 2
+    tiles = math.ceil(Np / 2048)
+    return math.ceil(S / 256), (tiles * math.ceil(R / 32) if R else 0), (0 if R else 1)
+
+
+# ---- planner (CPU) -----------------------------------------------------------
+def test_plan_counts_items(p2g):
+    shapes = [(4096, 74, 48, 1), (1024, 600, 300, 3), (65536, 4, 0, 1), (1048576, 300, 20, 5), (4100, 10, 7, 2)]
+    info, tiles = p2g.batch_plan(shapes, ctas=148, flags=p2g.BATCH_NO_AUTOTUNE)
+    scan = sum(_shape_items(sl, S, R)[0] for sl, S, R, _ in shapes)
+    fin = sum(_shape_items(sl, S, R)[2] for sl, S, R, _ in shapes)
+    assert info.scan_items == scan and info.finish_items == fin
+    assert info.items == info.scan_items + info.encode_items + info.finish_items
+    for (sl, S, R, _), ts in zip(shapes, tiles):
+        Np = (sl + 15) // 16 * 16 // 2
+        if R == 0:
+            assert ts == 0
+        else:
+            assert ts % 8 == 0 and 0 < ts <= 2048 and ts >= min(Np, 64) // 8 * 8
+    assert info.predicted_ms > 0
+
+
+def test_plan_autotune_splits_tiles_of_a_lone_job(p2g):
+    # one job, 1 row group, 16 tiles of 2048: 16 of 148 CTAs busy; finer tiles
+    # spread it wider and the simulated makespan must drop
+    shapes = [(65536, 2000, 20, 1)]
+    base, t0 = p2g.batch_plan(shapes, ctas=148, flags=p2g.BATCH_NO_AUTOTUNE)
+    tuned, t1 = p2g.batch_plan(shapes, ctas=148)
+    assert t0 == [2048] and t1[0] < 2048
+    assert tuned.predicted_ms < 0.6 * base.predicted_ms
+    assert tuned.encode_items > base.encode_items
+
+
+def test_plan_large_batch_is_near_its_bound(p2g):
+    from par2rust_b200 import workloads as W
+
+    jobs = W.batch_256()
+    shapes = [(j.slice_size, j.slices, j.recovery, len(j.file_lengths)) for j in jobs]
+    info, tiles = p2g.batch_plan(shapes, ctas=148)
+    assert info.jobs == 256 and info.scan_items == sum(math.ceil(j.slices / 256) for j in jobs)
+    # the mixed batch has ~43 SM-seconds of encode work: ~290 ms on 148 SMs
+    assert 250 < info.predicted_ms < 400
+
+
+def test_plan_rejects_bad_shapes(p2g):
+    with pytest.raises(p2g.InvalidSliceSize):
+        p2g.batch_plan([(4098, 10, 5, 1)])
+    with pytest.raises(p2g.TooManyRecoveryBlocks):
+        p2g.batch_plan([(4096, 10, 70000, 1)])
+    with pytest.raises(p2g.InvalidArgument):
+        p2g.batch_plan([(4096, 0, 5, 1)])
+
+
+# ---- device (GPU) -----------------------------------------------------------
+# (files, slice, R, name prefix): ragged files, slice sizes that are and are not
+# multiples of 16, a job without recovery rows, > 256 rows (two packet-MD5
+# passes), > 256 slices (several scan items), 40 files (sorting file ids),
+# two identical files (equal file ids), a one-slice job, the smallest slice
+JOB_SET = [
+    ([300_001], 4096, 48),
+    ([5000, 70000, 1], 1024, 300),
+    ([9000, 4100 * 3], 4100, 7),
+    ([200_000], 65536, 0),
+    ([100 + 73 * i for i in range(40)], 512, 5),
+    ("dup", 256, 3),
+    ([65536], 65536, 1),
+    ([600 * 1024 - 5], 1024, 33),
+    ([40], 4, 2),
+    ([1_000_000, 2_000_003, 17], 16384, 60),
+]
+
+
+def _files(k, spec):
+    if spec == "dup":
+        d = file_bytes(991, 3000).tobytes()
+        return [(b"same.bin", d), (b"same.bin", d)]
+    return [(f"j{k}_f{i}.bin".encode(), file_bytes(k * 1000 + i + 1, n).tobytes()) for i, n in enumerate(spec)]
+
+
+def _make_job(p2g, k, spec, slice_, R):
+    import torch
+
+    files = _files(k, spec)
+    S = sum((len(d) + slice_ - 1) // slice_ for _, d in files)
+    host = np.zeros(S * slice_, np.uint8)
+    off = 0
+    for _, d in files:
+        host[off:off + len(d)] = np.frombuffer(d, np.uint8)
+        off += (len(d) + slice_ - 1) // slice_ * slice_
+    src = torch.from_numpy(host).cuda()
+    bufs = p2g.DeviceJobBuffers(S, len(files), slice_, R, src.device)
+    spec_ = p2g.BatchJobSpec(src, [len(d) for _, d in files], [n for n, _ in files], slice_, R, bufs)
+    return spec_, files, host
+
+
+def _outputs(spec):
+    b = spec.bufs
+    S, R, n = spec.input_slices, spec.recovery_count, len(spec.file_lengths)
+    rec = b.recovery.view(-1, b.rec_stride)[:R, :spec.slice_size].cpu().numpy().copy() if R else None
+    return {
+        "rec": rec,
+        "checks": b.checksums[:20 * S].cpu().numpy().copy(),
+        "h16k": b.hash16k[:16 * n].cpu().numpy().copy(),
+        "pkt": b.packet_md5[:16 * R].cpu().numpy().copy() if R else None,
+        "set_id": b.set_id_device.cpu().numpy().tobytes(),
+    }
+
+
+def _expected(oracle, files, host, slice_, R):
+    S = len(host) // slice_
+    cks, h16s, fids = [], [], []
+    for name, d in files:
+        st, c, _hf, h16, fid = oracle.scan(d, slice_, name)
+        assert st == 0
+        cks += c
+        h16s.append(h16)
+        fids.append(fid)
+    sid = oracle.set_id(slice_, fids)
+    rec = np.asarray(oracle.encode(host, S, slice_, R)).reshape(R, slice_) if R else None
+    pkt = [oracle.recovery_packet_md5(sid, r, rec[r].tobytes()) for r in range(R)] if R else []
+    return cks, h16s, sid, rec, pkt
+
+
+@pytest.fixture(scope="module")
+def batch_jobs(p2g):
+    return [_make_job(p2g, k, spec, sl, R) for k, (spec, sl, R) in enumerate(JOB_SET)]
+
+
+@pytest.mark.gpu
+def test_batch_matches_oracle(p2g, oracle, gpu, batch_jobs):
+    import torch
+
+    b = p2g.Batch([j for j, _, _ in batch_jobs])
+    b.launch()
+    torch.cuda.synchronize()
+    b.check()
+    info = b.info()
+    assert info.jobs == len(JOB_SET) and info.finish_items == 1
+    for k, (spec, files, host) in enumerate(batch_jobs):
+        got = _outputs(spec)
+        cks, h16s, sid, rec, pkt = _expected(oracle, files, host, spec.slice_size, spec.recovery_count)
+        ch = got["checks"].reshape(-1, 20)
+        assert [(bytes(r[:16]), int.from_bytes(bytes(r[16:]), "little")) for r in ch] == cks, f"job {k} checksums"
+        assert got["h16k"].tobytes() == b"".join(h16s), f"job {k} hash16k"
+        assert got["set_id"] == sid, f"job {k} set id"
+        if spec.recovery_count:
+            assert (got["rec"] == rec).all(), f"job {k} recovery rows"
+            assert got["pkt"].tobytes() == b"".join(pkt), f"job {k} packet md5"
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batch_matches_plain_device_job(p2g, gpu, batch_jobs):
+    import torch
+
+    b = p2g.Batch([j for j, _, _ in batch_jobs])
+    b.launch()
+    torch.cuda.synchronize()
+    b.check()
+    for k, (spec, _, _) in enumerate(batch_jobs):
+        got = _outputs(spec)
+        plain = p2g.run_device_job(spec.src, spec.file_lengths, spec.names, spec.slice_size, spec.recovery_count,
+                                   skip_hash_full=True)
+        torch.cuda.synchronize()
+        S, R, n = spec.input_slices, spec.recovery_count, len(spec.file_lengths)
+        assert (plain.checksums[:20 * S].cpu().numpy() == got["checks"]).all(), k
+        assert (plain.hash16k[:16 * n].cpu().numpy() == got["h16k"]).all(), k
+        assert plain.set_id == got["set_id"], k
+        if R:
+            prec = plain.recovery.view(-1, plain.rec_stride)[:R, :spec.slice_size].cpu().numpy()
+            assert (prec == got["rec"]).all(), k
+            assert (plain.packet_md5[:16 * R].cpu().numpy() == got["pkt"]).all(), k
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batch_job_alone_equals_in_mix(p2g, gpu, batch_jobs):
+    import torch
+
+    mix = p2g.Batch([j for j, _, _ in batch_jobs])
+    mix.launch()
+    torch.cuda.synchronize()
+    mix.check()
+    in_mix = [_outputs(j) for j, _, _ in batch_jobs]
+    for k, (spec, _, _) in enumerate(batch_jobs):
+        for t in (spec.bufs.recovery, spec.bufs.checksums, spec.bufs.hash16k, spec.bufs.packet_md5,
+                  spec.bufs.set_id_device):
+            t.fill_(0xA5)
+        alone = p2g.Batch([spec])
+        alone.launch()
+        torch.cuda.synchronize()
+        alone.check()
+        got = _outputs(spec)
+        for key in ("checks", "h16k", "set_id"):
+            assert np.array_equal(np.frombuffer(bytes(got[key]), np.uint8),
+                                  np.frombuffer(bytes(in_mix[k][key]), np.uint8)), (k, key)
+        if spec.recovery_count:
+            assert (got["rec"] == in_mix[k]["rec"]).all() and (got["pkt"] == in_mix[k]["pkt"]).all(), k
+        alone.close()
+    mix.close()
+
+
+@pytest.mark.gpu
+def test_batch_graph_replay_and_direct_launch_agree(p2g, gpu, batch_jobs):
+    import torch
+
+    jobs = [j for j, _, _ in batch_jobs]
+    g = p2g.Batch(jobs)
+    g.launch()
+    torch.cuda.synchronize()
+    first = [_outputs(j) for j in jobs]
+    for j in jobs:
+        j.bufs.recovery.zero_()
+        j.bufs.packet_md5.zero_()
+        j.bufs.set_id_device.zero_()
+    g.launch()
+    g.launch()  # a replay right behind another on the same stream
+    torch.cuda.synchronize()
+    g.check()
+    d = p2g.Batch(jobs, flags=p2g.BATCH_NO_GRAPH)
+    d.launch()
+    torch.cuda.synchronize()
+    d.check()
+    for k, j in enumerate(jobs):
+        o = _outputs(j)
+        assert o["set_id"] == first[k]["set_id"]
+        if j.recovery_count:
+            assert (o["rec"] == first[k]["rec"]).all() and (o["pkt"] == first[k]["pkt"]).all(), k
+    g.close()
+    d.close()
+
+
+@pytest.mark.gpu
+def test_batch_validation(p2g, gpu, batch_jobs):
+    import torch
+
+    spec = batch_jobs[0][0]
+    bad = p2g.BatchJobSpec(spec.src, [0], [b"x"], 4096, 4, spec.bufs)
+    with pytest.raises(p2g.EmptyFile):
+        p2g.Batch([bad])
+    odd = p2g.BatchJobSpec(spec.src[1:], [10], [b"x"], 4096, 4, spec.bufs)
+    with pytest.raises(p2g.InvalidArgument):
+        p2g.Batch([odd])
+    with pytest.raises(p2g.InvalidSliceSize):
+        p2g.Batch([p2g.BatchJobSpec(spec.src, [10], [b"x"], 4098, 4, spec.bufs)])
+    torch.cuda.synchronize()
