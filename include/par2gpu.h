@@ -316,8 +316,12 @@ p2g_status p2g_run_device_job(p2g_device_job *job);
  * P2G_JOB_SKIP_HASH_FULL (hash_full stays with the caller, who usually hashes
  * it on the host while reading the files).  An autotuner picks each job's
  * tile width and the queue order by simulating the launch with a cost model.
- * The launch sequence (queue reset, coefficient bases, any realignment, the
- * persistent kernel) is captured once into a CUDA graph and replayed. */
+ * Coefficient bases are precomputed into batch scratch (S x ceil(R/32) x
+ * 1 KiB per job) while the batch's total stays within 16 GiB
+ * (P2G_BATCH_BASIS_BUDGET bytes); beyond that, or with
+ * P2G_BATCH_DERIVE_BASIS, each encode item derives its basis in the kernel.
+ * The launch sequence (queue reset, bases, any realignment, the persistent
+ * kernel) is captured once into a CUDA graph and replayed. */
 typedef struct p2g_batch_job {
     const uint8_t *src;                 /* device, 16-byte aligned; layout as in p2g_device_job */
     uint32_t file_count;
@@ -354,6 +358,7 @@ typedef struct p2g_batch_shape {
 
 #define P2G_BATCH_NO_GRAPH 1u           /* launch directly instead of replaying a CUDA graph */
 #define P2G_BATCH_NO_AUTOTUNE 2u        /* widest tiles and cost order, no tile search */
+#define P2G_BATCH_DERIVE_BASIS 4u       /* no basis scratch: encode items derive their bases */
 
 /* Validate the jobs (the checks of p2g_run_device_job), plan the items and
  * allocate the batch's device scratch.  The job buffers must stay valid

@@ -572,6 +572,7 @@ def run_device_job(src, file_lengths: Sequence[int], names: Sequence[bytes], sli
 # ---------------------------------------------------------------------------
 BATCH_NO_GRAPH = 1
 BATCH_NO_AUTOTUNE = 2
+BATCH_DERIVE_BASIS = 4
 
 
 @dataclass
@@ -759,5 +760,5 @@ __all__ = [
     "encode_device", "slice_checksums", "file_hashes", "recovery_packet_md5", "input_bases", "gf_mul", "gf_pow",
     "resolve_volume_sizes", "volume_filename", "build_packet", "build_main_packet", "compute_file_id", "md5",
     "kernel_launch_count", "device_info", "DeviceJobBuffers", "run_device_job", "BATCH_NO_GRAPH",
-    "BATCH_NO_AUTOTUNE", "BatchJobSpec", "BatchInfo", "Batch", "batch_plan",
+    "BATCH_NO_AUTOTUNE", "BATCH_DERIVE_BASIS", "BatchJobSpec", "BatchInfo", "Batch", "batch_plan",
 ]

@@ -15,6 +15,7 @@
 // (1x, 2x, 4x, 8x its minimum tile count) for the shortest simulated makespan.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -34,6 +35,12 @@ constexpr double kChainMs = 7.2e-4;        // one MD5 chain step of 64 bytes
 constexpr double kItemMs = 0.003;          // pop, descriptor loads, pipeline fill
 
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+// Device bytes a batch may spend on precomputed coefficient bases
+// (P2G_BATCH_BASIS_BUDGET overrides; default 16 GiB).
+uint64_t basis_budget() {
+    const char* e = getenv("P2G_BATCH_BASIS_BUDGET");
+    return e ? strtoull(e, nullptr, 10) : (16ull << 30);
+}
 inline double md5_ms(uint64_t bytes) { return (double)((bytes + 8) / 64 + 1) * kChainMs; }
 
 struct PlanJob {
@@ -91,19 +98,20 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
         const PlanJob& j = jobs[ji];
         for (uint32_t s = 0; s < j.S; s += kScanSlices) {
             const uint32_t cnt = std::min(kScanSlices, j.S - s);
-            v.push_back({scan_ms(j, cnt), seq++, {ji, kItemScan, s, cnt}});
+            v.push_back({scan_ms(j, cnt), seq++, {ji, kItemScan, s, cnt, 0, 0}});
             p.n_scan++;
         }
         if (j.R) {
             for (uint32_t t = 0; t < j.tiles; ++t) {
                 const uint32_t n0 = t * j.ts, syms = std::min(j.ts, j.Np - n0);
                 const double key = encode_ms(j, syms) + j.finish;
-                for (uint32_t rg = 0; rg < j.RG; ++rg) v.push_back({key, seq++, {ji, kItemEncode | (rg << 8), n0, syms}});
+                for (uint32_t rg = 0; rg < j.RG; ++rg)
+                    v.push_back({key, seq++, {ji, kItemEncode | (rg << 8), n0, syms, 0, 0}});
             }
             p.enc_items[ji] = j.tiles * j.RG;
             p.n_enc += j.tiles * j.RG;
         } else {
-            v.push_back({j.finish, seq++, {ji, kItemFinish, 0, 0}});
+            v.push_back({j.finish, seq++, {ji, kItemFinish, 0, 0, 0, 0}});
             p.n_fin++;
         }
     }
@@ -118,7 +126,7 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
 }
 
 double item_ms(const PlanJob& j, const BatchItem& it) {
-    switch (it.kind_rg & 0xFF) {
+    switch (it.kind_rg & kItemKindMask) {
     case kItemScan: return scan_ms(j, it.b);
     case kItemEncode: return encode_ms(j, it.b);
     default: return j.finish;
@@ -137,7 +145,7 @@ double simulate(const std::vector<PlanJob>& jobs, const Plan& p, uint32_t ctas) 
         free_at.pop();
         const PlanJob& j = jobs[it.job];
         t += item_ms(j, it);
-        if ((it.kind_rg & 0xFF) == kItemEncode && --left[it.job] == 0) t += j.finish;
+        if ((it.kind_rg & kItemKindMask) == kItemEncode && --left[it.job] == 0) t += j.finish;
         end = std::max(end, t);
         free_at.push(t);
     }
@@ -231,7 +239,7 @@ namespace {
 p2g_status enqueue_run(p2g_batch* b, cudaStream_t st) {
     int* err = reinterpret_cast<int*>(b->d_ctl + 1 + b->n_jobs);
     P2G_CU(cudaMemsetAsync(b->d_ctl, 0, b->ctl_bytes, st));
-    P2G_CU(launch_basis_batch(b->d_jobs, b->n_jobs, b->max_basis_words, st));
+    if (b->max_basis_words) P2G_CU(launch_basis_batch(b->d_jobs, b->n_jobs, b->max_basis_words, st));
     for (const auto& r : b->realigns) P2G_CU(launch_realign(r.src, r.slice, r.dst, r.estride, r.S, r.slice, st));
     P2G_CU(launch_batch(b->d_jobs, b->d_items, b->n_items, b->d_ctl, err, b->ctas, st));
     return P2G_OK;
@@ -352,10 +360,16 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
     const size_t o_files = take(16 * total_files);
     const size_t o_noff = take(8 * total_files);
     const size_t o_names = take(names_bytes);
-    std::vector<size_t> o_scratch(n), o_basis(n), o_real(n, 0);
+    // Precomputed bases load faster (a derived basis adds ~6% to an encode
+    // item) but take S x row groups x 1 KiB each: keep them while they fit.
+    uint64_t basis_total = 0;
+    for (uint32_t i = 0; i < n; ++i)
+        if (shape[i].R) basis_total += basis_bytes(shape[i].S, shape[i].RG);
+    const bool load_basis = !(flags & P2G_BATCH_DERIVE_BASIS) && basis_total <= basis_budget();
+    std::vector<size_t> o_scratch(n), o_basis(n, 0), o_real(n, 0);
     for (uint32_t i = 0; i < n; ++i) {
         o_scratch[i] = take(32ull * shape[i].n + 12);
-        o_basis[i] = shape[i].R ? take(basis_bytes(shape[i].S, shape[i].RG)) : 0;
+        if (load_basis && shape[i].R) o_basis[i] = take(basis_bytes(shape[i].S, shape[i].RG));
         if (shape[i].R && jobs[i].slice_size % 16) o_real[i] = take(round_up(jobs[i].slice_size, 16) * shape[i].S);
     }
     b->arena_bytes = off;
@@ -398,7 +412,7 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         d.enc_items = b->plan.enc_items[i];
         d.first_exp = 0;
         d.vec = jb.slice_size % 16 == 0 ? 1u : 0u;
-        d.basis = d.R ? reinterpret_cast<uint16_t*>(A + o_basis[i]) : nullptr;
+        d.basis = load_basis && d.R ? reinterpret_cast<uint16_t*>(A + o_basis[i]) : nullptr;
         if (d.R && jb.slice_size % 16) {
             d.esrc = A + o_real[i];
             d.estride = round_up(jb.slice_size, 16);
@@ -407,7 +421,7 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
             d.esrc = jb.src;
             d.estride = jb.slice_size;
         }
-        if (d.R) b->max_basis_words = std::max<uint64_t>(b->max_basis_words, (uint64_t)d.S * d.RG * 512);
+        if (d.basis) b->max_basis_words = std::max<uint64_t>(b->max_basis_words, (uint64_t)d.S * d.RG * 512);
         uint64_t first = 0;
         for (uint32_t f = 0; f < jb.file_count; ++f, ++fcur) {
             hfiles[2 * fcur] = first * jb.slice_size;
@@ -430,7 +444,7 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         release(b);
         return cuda_fail(e, "batch tables upload");
     }
-    b->kernels_per_run = 2 + (uint32_t)b->realigns.size();
+    b->kernels_per_run = 1 + (b->max_basis_words ? 1 : 0) + (uint32_t)b->realigns.size();
 
     // ---- capture the run into a CUDA graph ----
     if (!(flags & P2G_BATCH_NO_GRAPH)) {

@@ -192,6 +192,16 @@ static p2g_status join_into(Context& c, cudaStream_t caller) {
 // the side with the smaller estimated finish time from measured chain rates
 // (overridable with P2G_FILE_HASH=device|host).
 // ---------------------------------------------------------------------------
+// Coefficient basis of the encode: precomputed by its own kernel into a
+// scratch buffer (S x row groups x 1 KiB) and loaded by TMA, unless
+// P2G_ENCODE_BASIS=derive has the encode kernel derive it (no scratch, ~6%
+// more encode time on B200: 512 extra lookups per slice in a loop that is
+// close to its issue limit).
+static bool generate_basis() {
+    const char* e = getenv("P2G_ENCODE_BASIS");
+    return e && !strcmp(e, "derive");
+}
+
 enum class FileHashMode { Device, Host };
 static double env_double(const char* name, double dflt) {
     const char* e = getenv(name);
@@ -311,9 +321,12 @@ static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) 
     // follow band by band while later bands are still encoding.
     EncodePlan plan;
     cudaStream_t s_enc2 = c.st[5], s_pkt = c.st[6];
+    const bool gen = generate_basis();
     if (j.R && j.S) {
-        P2G_CU(c.basis.ensure(basis_bytes(j.S, RG)));
-        P2G_CU(launch_basis(c.basis.as<uint16_t>(), j.S, RG, j.R, j.first_exp, s_enc));
+        if (!gen) {
+            P2G_CU(c.basis.ensure(basis_bytes(j.S, RG)));
+            P2G_CU(launch_basis(c.basis.as<uint16_t>(), j.S, RG, j.R, j.first_exp, s_enc));
+        }
         const uint8_t* esrc = j.d_src;
         uint64_t estride = j.slice;
         if (j.slice % 16) {  // the TMA tile loads need 16-byte aligned slice starts
@@ -341,8 +354,8 @@ static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) 
             // one stream: band b+1 starts when band b's wave drains, so bands
             // complete in order and each packet-MD5 step can start early
             cudaStream_t sb = s_enc;
-            P2G_CU(launch_encode_band(plan, b, esrc, estride, j.S, c.basis.as<uint16_t>(), RG, j.R, j.d_rec,
-                                      j.rec_stride, c.err.as<int>(), sb));
+            P2G_CU(launch_encode_band(plan, b, esrc, estride, j.S, gen ? nullptr : c.basis.as<uint16_t>(), RG, j.R,
+                                      j.d_rec, j.rec_stride, c.err.as<int>(), sb, j.first_exp));
             P2G_CU(cudaEventRecord(c.ev_band[b], sb));
             tr.mark("encode band", sb);
         }
@@ -768,10 +781,13 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
             P2G_CU(cudaMemset2DAsync(jb.recovery, jb.recovery_stride, 0, jb.slice_size, R, s));
             return P2G_OK;
         }
-        P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
-        P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
-        P2G_CU(launch_encode(jb.src, jb.src_stride, S, c.basis.as<uint16_t>(), RG, R, jb.slice_size, jb.recovery,
-                             jb.recovery_stride, c.err.as<int>(), s));
+        const bool gen = generate_basis();
+        if (!gen) {
+            P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
+            P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
+        }
+        P2G_CU(launch_encode(jb.src, jb.src_stride, S, gen ? nullptr : c.basis.as<uint16_t>(), RG, R, jb.slice_size,
+                             jb.recovery, jb.recovery_stride, c.err.as<int>(), s, jb.first_exponent));
         return P2G_OK;
     }
     // host pointers: stage through device buffers
@@ -782,10 +798,13 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
     P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s));
     if (S) {
         P2G_CU(cudaMemcpy2DAsync(c.src.p, stride, jb.src, jb.src_stride, jb.slice_size, S, cudaMemcpyHostToDevice, s));
-        P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
-        P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
-        P2G_CU(launch_encode(c.src.as<uint8_t>(), stride, S, c.basis.as<uint16_t>(), RG, R, jb.slice_size,
-                             c.rec.as<uint8_t>(), stride, c.err.as<int>(), s));
+        const bool gen = generate_basis();
+        if (!gen) {
+            P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
+            P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
+        }
+        P2G_CU(launch_encode(c.src.as<uint8_t>(), stride, S, gen ? nullptr : c.basis.as<uint16_t>(), RG, R,
+                             jb.slice_size, c.rec.as<uint8_t>(), stride, c.err.as<int>(), s, jb.first_exponent));
     } else {
         P2G_CU(cudaMemsetAsync(c.rec.p, 0, (size_t)stride * R, s));
     }

@@ -59,9 +59,11 @@ void add_launches(uint64_t n);
 
 cudaError_t launch_basis(uint16_t* basis, uint32_t S, uint32_t RG, uint32_t R, uint32_t first_exp,
                          cudaStream_t st);
+// basis == nullptr: the kernel derives the coefficient basis itself (from
+// first_exp); otherwise it loads the launch_basis layout.
 cudaError_t launch_encode(const uint8_t* src, uint64_t src_stride, uint32_t S, const uint16_t* basis,
                           uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec,
-                          uint64_t rec_stride, int* err, cudaStream_t st);
+                          uint64_t rec_stride, int* err, cudaStream_t st, uint32_t first_exp = 0);
 cudaError_t launch_gf_mul_xor(uint16_t coeff, const uint8_t* in, uint8_t* out, size_t len,
                               cudaStream_t st);
 cudaError_t launch_md5_slices(const uint8_t* src, uint64_t stride, uint32_t count,
@@ -97,7 +99,7 @@ EncodePlan plan_encode(uint64_t slice_size, uint32_t S, uint32_t RG, bool banded
                        double reserve_ms);
 cudaError_t launch_encode_band(const EncodePlan& pl, uint32_t band, const uint8_t* src, uint64_t src_stride,
                                uint32_t S, const uint16_t* basis, uint32_t RG, uint32_t R, uint8_t* rec,
-                               uint64_t rec_stride, int* err, cudaStream_t st);
+                               uint64_t rec_stride, int* err, cudaStream_t st, uint32_t first_exp = 0);
 // Blocks (one SM each) that a hash launch over `streams` MD5 streams occupies.
 uint32_t hash_blocks(uint32_t streams);
 
@@ -122,13 +124,19 @@ enum BatchItemKind : uint32_t {
     kItemScan = 0,    // slice MD5 + CRC32 of up to kScanSlices slices
     kItemEncode = 1,  // one (row group, symbol tile) of the accumulator
     kItemFinish = 2,  // hash16k, set id and packet MD5s of a job without encode items
+    kItemSetId = 3,   // hash16k, file ids and set id only
+    kItemPacket = 4,  // packet MD5s of recovery rows [a, a+b) (set id already written)
 };
-constexpr uint32_t kScanSlices = 256;  // one slice per MD5 lane
+constexpr uint32_t kItemKindMask = 0x7Fu;
+constexpr uint32_t kItemAccumulate = 0x80u;  // encode: XOR partial sums into zeroed rows
+constexpr uint32_t kScanSlices = 256;        // one slice per MD5 lane
 
 struct BatchItem {
     uint32_t job;
-    uint32_t kind_rg;  // kind in bits 0-7, row group in bits 8-31
-    uint32_t a, b;     // scan: first slice, count; encode: first symbol, symbol count
+    uint32_t kind_rg;  // kind in bits 0-6 (+ kItemAccumulate), row group in bits 8-31
+    uint32_t a, b;     // scan: first slice, count; encode: first symbol, symbol count;
+                       // packet: first row, row count
+    uint32_t s0, sn;   // encode: input slices [s0, s0+sn) (sn == 0: all of the job's)
 };
 
 // Device descriptor of one job.  The CTA that completes a job's last encode
@@ -137,7 +145,7 @@ struct BatchItem {
 struct BatchJob {
     const uint8_t* src;        // files back to back, each on a slice boundary, zero-padded
     const uint8_t* esrc;       // encode source: src, or a copy with 16-byte aligned slices
-    uint16_t* basis;           // [s][row group][16][32] coefficient basis
+    uint16_t* basis;           // [s][row group][16][32] precomputed basis, or null: derived per slice
     uint8_t* rec;              // recovery row r at rec + r*rec_stride
     p2g_slice_checksum* checks;
     uint8_t* h16k;             // 16 bytes per file
@@ -149,7 +157,7 @@ struct BatchJob {
     uint8_t* scratch;          // 16*n file ids, then the 12+16*n main-packet body
     uint64_t slice, estride, rec_stride;
     uint32_t S, R, RG, n_files;
-    uint32_t enc_items, first_exp;
+    uint32_t enc_items, first_exp;  // enc_items ~0u: the encode items trigger no finish step
     uint32_t vec;  // slices and file starts of src are 16-byte aligned
     uint32_t pad;
 };

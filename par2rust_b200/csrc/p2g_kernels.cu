@@ -123,6 +123,9 @@ __device__ __forceinline__ uint4 lds128(uint32_t addr) {
 __device__ __forceinline__ void sts32(uint32_t addr, uint32_t v) {
     asm volatile("st.shared.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
+__device__ __forceinline__ void sts16(uint32_t addr, uint16_t v) {
+    asm volatile("st.shared.b16 [%0], %1;" ::"r"(addr), "h"(v) : "memory");
+}
 __device__ __forceinline__ uint32_t lds32(uint32_t addr) {
     uint32_t v;
     asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
@@ -209,14 +212,39 @@ __host__ __device__ constexpr size_t encode_smem_bytes() {
 // tiles back to back on the same barriers; it is advanced on return.
 // Returns false (uniformly over the CTA) when a bounded TMA wait gave up;
 // copies still in flight have then been waited for.
-template <int NCH>
+//
+// GEN: derive the 16 basis products of each slice in the kernel instead of
+// loading them: warp w (= j) lane l (= row) looks up c*2^j =
+// antilog[(logbase_s * (first_exp + r) mod 65535 + j) mod 65535], two
+// slices ahead, into one of two 1 KiB slots (no basis buffer in HBM).
+//
+// s0 / accumulate: the tile covers input slices [s0, s0+S) only; with
+// accumulate it XORs its partial sums into the recovery rows (atomic XOR
+// reductions, so chunks of one tile may run concurrently on rows that start
+// zeroed).
+__device__ __forceinline__ uint32_t mod_field(uint32_t x) {  // x mod 65535 for x < 2^32
+    x = (x & 0xFFFFu) + (x >> 16);
+    x = (x & 0xFFFFu) + (x >> 16);
+    return x >= kFieldLimit ? x - kFieldLimit : x;
+}
+__device__ __forceinline__ void red_xor4(uint8_t* p, const uint4& v) {
+    uint32_t* q = reinterpret_cast<uint32_t*>(p);
+    asm volatile("red.global.xor.b32 [%0], %1;" ::"l"(q), "r"(v.x) : "memory");
+    asm volatile("red.global.xor.b32 [%0], %1;" ::"l"(q + 1), "r"(v.y) : "memory");
+    asm volatile("red.global.xor.b32 [%0], %1;" ::"l"(q + 2), "r"(v.z) : "memory");
+    asm volatile("red.global.xor.b32 [%0], %1;" ::"l"(q + 3), "r"(v.w) : "memory");
+}
+
+template <int NCH, bool GEN = false>
 __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S,
                                             const uint16_t* __restrict__ basis, uint32_t RG, uint32_t rg,
                                             uint32_t R, uint32_t n0, uint32_t tile_syms,
                                             uint8_t* __restrict__ rec, uint64_t rec_stride, uint8_t* smem,
-                                            uint32_t& phase) {
+                                            uint32_t& phase, uint32_t first_exp = 0, uint32_t s0 = 0,
+                                            bool accumulate = false) {
     constexpr int WARPS = kEncThreads / 32;
     constexpr int NT = WARPS * NCH * 64;  // symbol capacity of a tile (tile_syms <= NT)
+    static_assert(!GEN || WARPS == 16, "derived basis: one warp per basis product j");
     uint8_t* tabs = smem;
     uint8_t* src_st = smem + 2 * kTabBytes;
     uint8_t* bas_st = src_st + kEncStages * NT * 2;
@@ -225,16 +253,41 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile_bytes = tile_syms * 2;
     const uint32_t ph = phase;
+    src += (size_t)s0 * src_stride;
+    if (!GEN) basis += (size_t)s0 * RG * 512;
+    const uint16_t* lbase = d_logbase + s0;
     auto parity = [&](uint32_t s) { return ((ph >> (s % kEncStages)) ^ (s / kEncStages)) & 1u; };
 
     auto issue = [&](uint32_t s, int st) {
-        mbar_arrive_expect_tx(&bars[st], tile_bytes + 1024);
+        mbar_arrive_expect_tx(&bars[st], GEN ? tile_bytes : tile_bytes + 1024);
         tma_load_1d(src_st + st * NT * 2, src + (size_t)s * src_stride + (size_t)n0 * 2, tile_bytes,
                     &bars[st]);
-        tma_load_1d(bas_st + st * 1024, basis + ((size_t)s * RG + rg) * 512, 1024, &bars[st]);
+        if (!GEN) tma_load_1d(bas_st + st * 1024, basis + ((size_t)s * RG + rg) * 512, 1024, &bars[st]);
     };
     if (tid == 0)
         for (int st = 0; st < kEncStages && (uint32_t)st < S; ++st) issue(st, st);
+
+    // derived basis: this thread's (j = warp, row = lane) entry and its offset in a slot
+    const uint32_t g_row = rg * kRowsPerGroup + lane;
+    const uint32_t g_exp = first_exp + g_row;
+    const bool g_live = g_row < R;
+    const uint32_t g_off = (uint32_t)((((warp & 7) * 2 + (warp >> 3)) * 32 + lane) * 2);
+    auto gen_value = [&](uint32_t lb) -> uint16_t {
+        if (!g_live) return 0;
+        uint32_t k = mod_field(lb * g_exp) + (uint32_t)warp;
+        if (k >= kFieldLimit) k -= kFieldLimit;
+        return d_antilog[k];
+    };
+    auto gen_slot = [&](uint32_t s) { return smem_u32(bas_st) + (s & 1u) * 1024 + g_off; };
+    uint16_t g_v = 0;   // basis value of slice s+2, stored at the end of iteration s
+    uint32_t g_lb = 0;  // logbase of slice s+3
+    if (GEN) {
+        if (S > 0) sts16(gen_slot(0), gen_value(lbase[0]));
+        if (S > 1) sts16(gen_slot(1), gen_value(lbase[1]));
+        if (S > 2) g_v = gen_value(lbase[2]);
+        if (S > 3) g_lb = lbase[3];
+        __syncthreads();
+    }
 
     // Table build: the 256 table rows are 16 blocks of 16; warp w builds
     // blocks w, w+WARPS, ...  Thread (word column wc = lane) writes the 16
@@ -296,7 +349,7 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
         if (s + 1 < S) {
             const int st1 = (int)((s + 1) % kEncStages);
             if (!mbar_wait_bounded(&bars[st1], parity(s + 1))) bad = 1;
-            build(t ^ 1, st1);
+            build(t ^ 1, GEN ? (int)((s + 1) & 1) : st1);  // GEN: the slice's slot
         }
         const uint32_t baseA = tab_u32 + t * kTabBytes + offA;
         const uint32_t baseB = tab_u32 + t * kTabBytes + offB;
@@ -320,6 +373,13 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
                     acc[j][i][2] ^= A.z ^ B.z;
                     acc[j][i][3] ^= A.w ^ B.w;
                 }
+            }
+        }
+        if (GEN && s + 2 < S) {  // slot s&1 was last read by build(s), before the previous barrier
+            sts16(gen_slot(s), g_v);
+            if (s + 3 < S) {
+                g_v = gen_value(g_lb);
+                if (s + 4 < S) g_lb = lbase[s + 4];
             }
         }
         if (__syncthreads_or(bad)) {
@@ -356,21 +416,27 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
                 wo.y = __byte_perm(acc[j][2][q], acc[j][3][q], 0x7632);
                 wo.z = __byte_perm(acc[j][4][q], acc[j][5][q], 0x7632);
                 wo.w = __byte_perm(acc[j][6][q], acc[j][7][q], 0x7632);
-                if (re < R) *reinterpret_cast<uint4*>(rec + (size_t)re * rec_stride + (size_t)n * 2) = we;
-                if (re + 1 < R)
-                    *reinterpret_cast<uint4*>(rec + (size_t)(re + 1) * rec_stride + (size_t)n * 2) = wo;
+                uint8_t* pe = rec + (size_t)re * rec_stride + (size_t)n * 2;
+                uint8_t* po = pe + rec_stride;
+                if (accumulate) {
+                    if (re < R) red_xor4(pe, we);
+                    if (re + 1 < R) red_xor4(po, wo);
+                } else {
+                    if (re < R) *reinterpret_cast<uint4*>(pe) = we;
+                    if (re + 1 < R) *reinterpret_cast<uint4*>(po) = wo;
+                }
             }
         }
     }
     return true;
 }
 
-template <int NCH>
+template <int NCH, bool GEN>
 __global__ void __launch_bounds__(kEncThreads, 1)
     encode_lut_kernel(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S,
                       const uint16_t* __restrict__ basis, uint32_t RG, uint32_t R, uint32_t sym_begin,
                       uint32_t sym_end, uint32_t TS, uint8_t* __restrict__ rec, uint64_t rec_stride,
-                      int* __restrict__ err) {
+                      uint32_t first_exp, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr int NT = (kEncThreads / 32) * NCH * 64;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * kTabBytes + kEncStages * (NT * 2 + 1024));
@@ -383,8 +449,8 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     }
     __syncthreads();
     uint32_t phase = 0;
-    if (!encode_tile<NCH>(src, src_stride, S, basis, RG, rg, R, n0, min(TS, sym_end - n0), rec, rec_stride, smem,
-                          phase) &&
+    if (!encode_tile<NCH, GEN>(src, src_stride, S, basis, RG, rg, R, n0, min(TS, sym_end - n0), rec, rec_stride,
+                               smem, phase, first_exp) &&
         threadIdx.x == 0)
         atomicOr(err, 1);
 }
@@ -988,15 +1054,13 @@ __device__ __forceinline__ void batch_scan(const BatchJob& J, uint32_t first, ui
     }
 }
 
-// Finish step of job J (all threads of the CTA):
-//   hash16k of each file and its file id MD5(hash16k ‖ length le64 ‖ name)
-//   (src/source.rs:303-309); the main-packet body slice_size le64 ‖ count
-//   le32 ‖ file ids in byte order, whose MD5 is the set id
-//   (src/packet/main_packet.rs:25-42); then each recovery row's packet MD5
-//   over set_id ‖ "PAR 2.0\0RecvSlic" ‖ exponent le32 ‖ row
-//   (src/packet/recovery.rs:15, src/format.rs:33-54).
+// Set-id step of job J (all threads of the CTA): hash16k of each file and
+// its file id MD5(hash16k ‖ length le64 ‖ name) (src/source.rs:303-309); the
+// main-packet body slice_size le64 ‖ count le32 ‖ file ids in byte order,
+// whose MD5 is the set id (src/packet/main_packet.rs:25-42).  The set id
+// goes to J.set_id and to sid[0..3] (shared memory).
 template <bool VEC>
-__device__ void batch_finish(const BatchJob& J, uint32_t ring, uint32_t* sid) {
+__device__ void batch_set_id(const BatchJob& J, uint32_t ring, uint32_t* sid) {
     const int tid = threadIdx.x;
     const uint32_t n = J.n_files;
     uint4* ids = reinterpret_cast<uint4*>(J.scratch);
@@ -1046,11 +1110,22 @@ __device__ void batch_finish(const BatchJob& J, uint32_t ring, uint32_t* sid) {
         sid[1] = s[1];
         sid[2] = s[2];
         sid[3] = s[3];
-        store_digest(J.set_id, s);
+        uint32_t* o = reinterpret_cast<uint32_t*>(J.set_id);
+        __stcg(o, s[0]);
+        __stcg(o + 1, s[1]);
+        __stcg(o + 2, s[2]);
+        __stcg(o + 3, s[3]);
     }
     __syncthreads();
+}
+
+// Packet MD5 of recovery rows [r0, r1) of job J (all threads of the CTA):
+// MD5(set_id ‖ "PAR 2.0\0RecvSlic" ‖ exponent le32 ‖ row)
+// (src/packet/recovery.rs:15, src/format.rs:33-54).
+__device__ void batch_packets(const BatchJob& J, uint32_t ring, const uint32_t* sid, uint32_t r0, uint32_t r1) {
+    const int tid = threadIdx.x;
     if (tid < kHashThreads) {
-        for (uint32_t r = tid; r < J.R; r += kHashThreads) {
+        for (uint32_t r = r0 + tid; r < r1; r += kHashThreads) {
             // set id ‖ "PAR 2.0\0" "RecvSlic" as little-endian words ‖ exponent
             const uint32_t pre[9] = {sid[0], sid[1], sid[2], sid[3], 0x20524150u, 0x00302E32u, 0x76636552u,
                                      0x63696C53u, J.first_exp + r};
@@ -1089,7 +1164,7 @@ __global__ void __launch_bounds__(kEncThreads, 1)
         if (idx >= n_items) break;
         const BatchItem it = items[idx];
         const BatchJob& J = jobs[it.job];
-        const uint32_t kind = it.kind_rg & 0xFFu;
+        const uint32_t kind = it.kind_rg & kItemKindMask;
         if (kind == kItemScan) {
             if (J.vec)
                 batch_scan<true>(J, it.a, it.b, ring, T);
@@ -1098,9 +1173,30 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             __syncthreads();
             continue;
         }
+        if (kind == kItemSetId) {
+            if (J.vec)
+                batch_set_id<true>(J, ring, misc + 4);
+            else
+                batch_set_id<false>(J, ring, misc + 4);
+            continue;
+        }
+        if (kind == kItemPacket) {
+            if (tid < 4) misc[4 + tid] = __ldcg(reinterpret_cast<const uint32_t*>(J.set_id) + tid);
+            __syncthreads();
+            batch_packets(J, ring, misc + 4, it.a, it.a + it.b);
+            continue;
+        }
         if (kind == kItemEncode) {
-            if (!encode_tile<kEncChunks>(J.esrc, J.estride, J.S, J.basis, J.RG, it.kind_rg >> 8, J.R, it.a, it.b,
-                                         J.rec, J.rec_stride, enc, phase)) {
+            // the job's precomputed basis when it has one, else derived per slice
+            const uint32_t rg = it.kind_rg >> 8, sn = it.sn ? it.sn : J.S;
+            const bool acc = (it.kind_rg & kItemAccumulate) != 0;
+            const bool ok = J.basis ? encode_tile<kEncChunks, false>(J.esrc, J.estride, sn, J.basis, J.RG, rg, J.R,
+                                                                      it.a, it.b, J.rec, J.rec_stride, enc, phase,
+                                                                      J.first_exp, it.s0, acc)
+                                    : encode_tile<kEncChunks, true>(J.esrc, J.estride, sn, nullptr, J.RG, rg, J.R,
+                                                                     it.a, it.b, J.rec, J.rec_stride, enc, phase,
+                                                                     J.first_exp, it.s0, acc);
+            if (!ok) {
                 if (tid == 0) atomicOr(err, 1);
                 break;
             }
@@ -1111,16 +1207,18 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             if (!misc[1]) continue;
             __threadfence();  // acquire: every tile of the job is visible from here on
         }
+        // finish: set id, then every row's packet MD5
         if (J.vec)
-            batch_finish<true>(J, ring, misc + 4);
+            batch_set_id<true>(J, ring, misc + 4);
         else
-            batch_finish<false>(J, ring, misc + 4);
+            batch_set_id<false>(J, ring, misc + 4);
+        batch_packets(J, ring, misc + 4, 0, J.R);
     }
 }
 
 __global__ void basis_batch_kernel(const BatchJob* __restrict__ jobs) {
     const BatchJob& J = jobs[blockIdx.y];
-    if (!J.R) return;
+    if (!J.R || !J.basis) return;
     basis_fill(J.basis, J.S, J.RG, J.R, J.first_exp, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
                (uint64_t)gridDim.x * blockDim.x);
 }
@@ -1182,8 +1280,11 @@ static cudaError_t encode_attr() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 256 || !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(encode_lut_kernel<kEncChunks>,
+        cudaError_t e = cudaFuncSetAttribute(encode_lut_kernel<kEncChunks, false>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(encode_lut_kernel<kEncChunks, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 256) attr_set[dev] = true;
     }
@@ -1268,7 +1369,7 @@ EncodePlan plan_encode(uint64_t slice_size, uint32_t S, uint32_t RG, bool banded
 
 cudaError_t launch_encode_band(const EncodePlan& pl, uint32_t band, const uint8_t* src, uint64_t src_stride,
                                uint32_t S, const uint16_t* basis, uint32_t RG, uint32_t R, uint8_t* rec,
-                               uint64_t rec_stride, int* err, cudaStream_t st) {
+                               uint64_t rec_stride, int* err, cudaStream_t st, uint32_t first_exp) {
     constexpr size_t smem = encode_smem_bytes<kEncChunks>();
     cudaError_t e = encode_attr();
     if (e != cudaSuccess) return e;
@@ -1276,17 +1377,21 @@ cudaError_t launch_encode_band(const EncodePlan& pl, uint32_t band, const uint8_
     const EncodeBand& bd = pl.bands[band];
     if (bd.begin >= bd.end) return cudaSuccess;
     const uint32_t tiles = (bd.end - bd.begin + bd.ts - 1) / bd.ts;
-    encode_lut_kernel<kEncChunks><<<tiles * RG, kEncThreads, smem, st>>>(src, src_stride, S, basis, RG, R, bd.begin,
-                                                                         bd.end, bd.ts, rec, rec_stride, err);
+    if (basis)
+        encode_lut_kernel<kEncChunks, false><<<tiles * RG, kEncThreads, smem, st>>>(
+            src, src_stride, S, basis, RG, R, bd.begin, bd.end, bd.ts, rec, rec_stride, first_exp, err);
+    else  // coefficient basis derived in the kernel
+        encode_lut_kernel<kEncChunks, true><<<tiles * RG, kEncThreads, smem, st>>>(
+            src, src_stride, S, nullptr, RG, R, bd.begin, bd.end, bd.ts, rec, rec_stride, first_exp, err);
     count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_encode(const uint8_t* src, uint64_t src_stride, uint32_t S, const uint16_t* basis,
                           uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec, uint64_t rec_stride,
-                          int* err, cudaStream_t st) {
+                          int* err, cudaStream_t st, uint32_t first_exp) {
     const EncodePlan pl = plan_encode(slice_size, S, RG, false, 0, 0.0);
-    return launch_encode_band(pl, 0, src, src_stride, S, basis, RG, R, rec, rec_stride, err, st);
+    return launch_encode_band(pl, 0, src, src_stride, S, basis, RG, R, rec, rec_stride, err, st, first_exp);
 }
 
 cudaError_t launch_gf_mul_xor(uint16_t coeff, const uint8_t* in, uint8_t* out, size_t len, cudaStream_t st) {
@@ -1514,8 +1619,8 @@ cudaError_t launch_encode_noheap(const uint8_t* src, uint64_t src_stride, uint32
     uint32_t ts = 0, tiles = 0;
     choose_tiles(Np, RG, (uint32_t)sm_count(), &ts, &tiles);
     if (!R || !tiles) return cudaSuccess;
-    encode_lut_kernel<kEncChunks><<<tiles * RG, kEncThreads, smem, st>>>(src, src_stride, S, basis, RG, R, 0, Np, ts,
-                                                                         rec, rec_stride, err);
+    encode_lut_kernel<kEncChunks, false><<<tiles * RG, kEncThreads, smem, st>>>(src, src_stride, S, basis, RG, R, 0,
+                                                                                Np, ts, rec, rec_stride, 0, err);
     count_launch();
     return cudaGetLastError();
 }

@@ -218,7 +218,7 @@ def test_batch_job_alone_equals_in_mix(p2g, gpu, batch_jobs):
 
 
 @pytest.mark.gpu
-def test_batch_graph_replay_and_direct_launch_agree(p2g, gpu, batch_jobs):
+def test_batch_graph_replay_direct_launch_and_derived_basis_agree(p2g, gpu, batch_jobs):
     import torch
 
     jobs = [j for j, _, _ in batch_jobs]
@@ -234,17 +234,21 @@ def test_batch_graph_replay_and_direct_launch_agree(p2g, gpu, batch_jobs):
     g.launch()  # a replay right behind another on the same stream
     torch.cuda.synchronize()
     g.check()
-    d = p2g.Batch(jobs, flags=p2g.BATCH_NO_GRAPH)
-    d.launch()
-    torch.cuda.synchronize()
-    d.check()
-    for k, j in enumerate(jobs):
-        o = _outputs(j)
-        assert o["set_id"] == first[k]["set_id"]
-        if j.recovery_count:
-            assert (o["rec"] == first[k]["rec"]).all() and (o["pkt"] == first[k]["pkt"]).all(), k
+    for flags in (p2g.BATCH_NO_GRAPH, p2g.BATCH_DERIVE_BASIS, p2g.BATCH_NO_AUTOTUNE | p2g.BATCH_DERIVE_BASIS):
+        for j in jobs:
+            j.bufs.recovery.zero_()
+            j.bufs.packet_md5.zero_()
+        d = p2g.Batch(jobs, flags=flags)
+        d.launch()
+        torch.cuda.synchronize()
+        d.check()
+        for k, j in enumerate(jobs):
+            o = _outputs(j)
+            assert o["set_id"] == first[k]["set_id"]
+            if j.recovery_count:
+                assert (o["rec"] == first[k]["rec"]).all() and (o["pkt"] == first[k]["pkt"]).all(), (flags, k)
+        d.close()
     g.close()
-    d.close()
 
 
 @pytest.mark.gpu

@@ -45,6 +45,18 @@ def test_encode_matches_oracle(p2g, oracle, gpu, S, slice_, R):
     assert (want == got).all()
 
 
+@pytest.mark.parametrize("S,slice_,R", [(5, 4096, 33), (7, 132, 40), (2, 4100, 65), (33, 256, 97), (9, 8208, 31)])
+def test_encode_basis_loaded_or_derived_agree(p2g, oracle, gpu, monkeypatch, S, slice_, R):
+    # the encode loads a precomputed coefficient basis by default; the kernel
+    # that derives it itself (P2G_ENCODE_BASIS=derive) must give the same rows
+    src = rnd(S * 7 + R, S * slice_)
+    want = oracle.encode(src, S, slice_, R)
+    got_load = p2g.encode(src, slice_, R)
+    monkeypatch.setenv("P2G_ENCODE_BASIS", "derive")
+    got_gen = p2g.encode(src, slice_, R)
+    assert (want == got_gen).all() and (want == got_load).all()
+
+
 def test_encode_zero_source_gives_zero(p2g, gpu):
     assert not p2g.encode(np.zeros(4 * 1024, np.uint8), 1024, 70).any()
 
