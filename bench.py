@@ -47,6 +47,8 @@ WORKLOADS = {
     "prof_256x512k": dict(length=256 * 524_288, slice=524_288, R=200, scheme="exponential", seed=2),
     # 256 independent jobs in one persistent launch vs the plain per-job path
     "batch_256": dict(batch=True, n_jobs=256, seed=4),
+    # serving loop: open-loop Poisson arrivals of create requests
+    "serve": dict(serve=True, seed=5),
 }
 
 
@@ -64,6 +66,11 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-vs-plain section of the default (single-file) run")
     ap.add_argument("--batch-jobs", type=int, default=256, help="jobs in the batched comparison")
+    ap.add_argument("--requests", type=int, default=10_000, help="serving: requests per arrival rate")
+    ap.add_argument("--rates", default="", help="serving: comma-separated arrival rates (jobs/s); default "
+                                                "0.5,0.8,0.95 x the capacity measured by a closed-batch probe")
+    ap.add_argument("--probe-jobs", type=int, default=200, help="serving: jobs in the capacity probe")
+    ap.add_argument("--wave-ms", type=float, default=20.0, help="serving: target device time per wave")
     ap.add_argument("--only-encode", action="store_true",
                     help="profiling aid: run only the single-launch encode kernel loop (no JSON line)")
     return ap.parse_args()
@@ -317,6 +324,140 @@ def bench_batch(dev, steps, warmup, plain_steps=1, n_jobs=256, e2e_steps=0):
     return out
 
 
+def serve_cpu_baseline(jobs, target_s, threads=0):
+    """The CPU port on whole requests of the serving mix, in order, until
+    about target_s seconds of CPU work (each request's files as one buffer)."""
+    import numpy as np
+
+    from oracle import oracle as orc
+    from par2rust_b200 import workloads as W
+
+    done_bytes, spent, n = 0, 0.0, 0
+    for j in jobs:
+        data = np.concatenate([W.file_bytes(sd, ln) for ln, sd in zip(j.file_lengths, j.seeds)])
+        t, *_ = orc.create_timed(data, j.slice_size, j.recovery, threads)
+        done_bytes += len(data)
+        spent += t
+        n += 1
+        if spent >= target_s:
+            break
+    return {"value": done_bytes / spent / 1e9, "unit": "GB/s", "cores": threads or orc.max_threads(), "kind": "port",
+            "sample": f"the first {n} requests of the serving mix ({done_bytes} B), each request's files as one "
+                      "buffer (scan + encode + packet MD5s)", "seconds": spent}, spent
+
+
+def serve_run(srv, jobs, arrivals, p2g):
+    """Open loop: submit job i at arrivals[i] (server clock from now), a
+    poller thread reads each completed job's set id and packet MD5s back and
+    releases it.  Returns per-job latencies and totals."""
+    import threading
+
+    n = len(jobs)
+    lat, done_bytes, d2h = [], [0], [0]
+    last_done = [0.0]
+    finished = threading.Event()
+
+    errors = []
+
+    def poller():
+        got = 0
+        try:
+            while got < n:
+                for r in srv.poll(wait_ms=20):
+                    got += 1
+                    if r.status != 0:
+                        raise RuntimeError(f"request {r.tag} failed with status {r.status}")
+                    p2g.copy_to_host(r.ptr["set_id"], 16)
+                    p2g.copy_to_host(r.ptr["packet_md5"], 16 * r.recovery_count)
+                    d2h[0] += 16 + 16 * r.recovery_count
+                    srv.release(r.ticket)
+                    lat.append(r.done_s - r.submit_s)
+                    done_bytes[0] += r.source_bytes
+                    last_done[0] = max(last_done[0], r.done_s)
+        except Exception as e:  # surfaced by the submitting thread
+            errors.append(e)
+        finished.set()
+
+    th = threading.Thread(target=poller, daemon=True)
+    t0 = srv.now()
+    th.start()
+    for i, (j, at) in enumerate(zip(jobs, arrivals)):
+        while True:
+            wait = t0 + at - srv.now()
+            if wait <= 0:
+                break
+            time.sleep(min(wait, 0.002))
+        names = [f"req{i:05d}_f{k:02d}.bin".encode() for k in range(len(j.file_lengths))]
+        srv.submit_seeded(j.file_lengths, j.seeds, names, j.slice_size, j.recovery, tag=i)
+        if errors:
+            break
+    finished.wait()
+    th.join()
+    if errors:
+        raise errors[0]
+    span = last_done[0] - t0
+    lat.sort()
+    pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
+    return {"requests": n, "source_bytes": done_bytes[0], "seconds": span, "gbs": done_bytes[0] / span / 1e9,
+            "jobs_per_s": n / span, "p50_ms": pct(0.50) * 1e3, "p99_ms": pct(0.99) * 1e3,
+            "mean_ms": sum(lat) / len(lat) * 1e3, "max_ms": lat[-1] * 1e3, "d2h_bytes": d2h[0]}
+
+
+def run_serve(args, wl):
+    import torch
+
+    import par2rust_b200 as p2g
+    from par2rust_b200 import workloads as W
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    jobs = W.serve_requests(args.requests, seed=wl["seed"])
+    budget = 120_000_000_000
+    srv = p2g.Server(hbm_budget=budget, wave_ms=args.wave_ms)
+    clocks = ClockSampler(local)
+    clocks.start()
+    # capacity: a closed batch of the first probe jobs, all submitted at once
+    probe = jobs[:min(args.probe_jobs, len(jobs))]
+    pr = serve_run(srv, probe, [0.0] * len(probe), p2g)
+    cap_jobs = pr["jobs_per_s"]
+    rates = [float(x) for x in args.rates.split(",") if x] or [f * cap_jobs for f in (0.5, 0.8, 0.95)]
+    sweep = []
+    for ri, rate in enumerate(rates):
+        arr = W.poisson_arrivals(len(jobs), rate, seed=100 + ri)
+        res = serve_run(srv, jobs, arr, p2g)
+        res["rate_jobs_per_s"] = rate
+        res["offered_gbs"] = rate * sum(j.source_bytes for j in jobs) / len(jobs) / 1e9
+        st = srv.stats()
+        res["waves_total"] = st["waves"]
+        res["peak_resident_gb"] = st["peak_resident_bytes"] / 1e9
+        sweep.append(res)
+        print(json.dumps({"serve_point": res}), file=sys.stderr, flush=True)
+    clk = clocks.stop()
+    launches = srv.stats()["waves"]
+    srv.close()
+    cb = None
+    if not args.no_cpu_baseline:
+        cb, _ = serve_cpu_baseline(jobs, args.cpu_seconds)
+    top = sweep[-1]
+    line = {
+        "metric": "serving: source GB/s and p50/p99 job latency per arrival rate", "value": top["gbs"],
+        "unit": "GB/s", "n_gpus": 1, "steps": len(rates), "warmup": 1, "ms_per_step": top["seconds"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+        "data": "synthetic (request bytes generated on the device from per-file seeds)",
+        "config": {"workload": f"serve: {len(jobs)} requests, totals log-uniform [1 MiB, 2 GiB] in 1-32 files, "
+                               "slice {16K,64K,256K,1M} (smallest with <= 32768 slices), R 1-20% of slices, "
+                               "Poisson arrivals", "hbm_budget_bytes": budget, "wave_ms": args.wave_ms,
+                   "total_source_bytes": sum(j.source_bytes for j in jobs), "parallelism": "1 GPU"},
+        "capacity_probe": pr, "sweep": sweep,
+        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
+        "e2e": {"value": top["gbs"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": top["d2h_bytes"],
+                "note": "host clock from each request's submit to its completion; sources generated on the device"},
+        "roofline": None, "cpu_baseline": cb, "clocks": clk, "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference_batch(args, wl):
     rank, world, local = dist_env()
     if rank != 0:
@@ -425,11 +566,28 @@ def main():
     args = parse()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
+        if wl.get("serve"):
+            rank, _, _ = dist_env()
+            if rank != 0:
+                return 0
+            from par2rust_b200 import workloads as W
+
+            cb, spent = serve_cpu_baseline(W.serve_requests(args.requests, seed=wl["seed"]), args.cpu_seconds)
+            print(json.dumps({"metric": "serving: source GB/s and p50/p99 job latency per arrival rate",
+                              "value": cb["value"], "unit": "GB/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+                              "ms_per_step": spent * 1e3, "higher_is_better": True, "scaling": "weak",
+                              "vs_baseline": None, "dtype": "u16", "data": "synthetic", "impl": "reference",
+                              "config": {"workload": "serve"}, "cpu_baseline": cb,
+                              "e2e": {"value": cb["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+            return 0
         if wl.get("batch"):
             return run_reference_batch(args, wl)
         return run_reference(args, wl)
     if wl.get("batch"):
         return run_batch(args, wl)
+    if wl.get("serve"):
+        return run_serve(args, wl)
 
     import numpy as np
     import torch

@@ -378,6 +378,82 @@ void p2g_batch_destroy(p2g_batch *batch);
 p2g_status p2g_batch_plan(const p2g_batch_shape *shapes, uint32_t n, uint32_t ctas, uint32_t flags,
                           p2g_batch_info *info, uint32_t *tiles_out);
 
+/* ---- serving loop (no counterpart in par2rust, which runs one create at
+ * a time) ------------------------------------------------------------------
+ * A request loop with continuous batching.  Submitted create jobs wait in
+ * arrival order until their footprint (padded source + recovery rows) fits
+ * the HBM budget beside the resident jobs; admission then allocates their
+ * device memory from the stream-ordered pool and brings the source in.  The
+ * device runs back-to-back "waves" of the persistent batch kernel, each
+ * taking a fair share of work items from every resident job, so requests
+ * that arrive while others are on the GPU start in the next wave and their
+ * work overlaps.  Outputs (as for p2g_batch_job, hash_full excluded) stay in
+ * device memory until the caller releases the job.  A scheduler thread
+ * inside the library drives admission and waves; all calls are thread-safe.
+ * Each job's outputs are byte-identical to the same job run alone. */
+typedef struct p2g_server p2g_server;   /* opaque */
+typedef struct p2g_server_options {
+    uint64_t hbm_budget;                /* bytes of source + recovery resident jobs may hold (0: 120e9) */
+    double wave_ms;                     /* target device time of one wave (0: 20) */
+    uint32_t max_jobs;                  /* resident job slots (0: 1024) */
+    uint32_t flags;                     /* reserved, 0 */
+} p2g_server_options;
+
+#define P2G_SOURCE_HOST 0u              /* host_src: the files back to back, slice-padded, copied at admission
+                                           (pinned memory copies asynchronously); keep it until the job completes */
+#define P2G_SOURCE_SEEDED 1u            /* file_seeds: each file generated on the device as the splitmix64 counter
+                                           stream of its seed (synthetic requests for benchmarks and tests) */
+typedef struct p2g_server_job {
+    uint32_t file_count;
+    const uint64_t *file_lengths;       /* host arrays, copied at submit */
+    const uint8_t *const *names;
+    const size_t *name_lens;
+    uint64_t slice_size;
+    uint32_t recovery_count;
+    uint32_t source_kind;
+    const uint8_t *host_src;
+    const uint64_t *file_seeds;
+    uint64_t tag;                       /* caller's id, returned with the result */
+} p2g_server_job;
+
+typedef struct p2g_server_result {
+    uint64_t ticket, tag;
+    int32_t status;                     /* P2G_OK or the job's failure */
+    double submit_s, admit_s, done_s;   /* server clock (p2g_server_now) */
+    uint64_t source_bytes;
+    uint32_t input_slices, recovery_count, file_count;
+    const uint8_t *src;                 /* device pointers, valid until p2g_server_release */
+    const uint8_t *recovery;
+    uint64_t recovery_stride;
+    const p2g_slice_checksum *checksums;
+    const uint8_t *hash16k;
+    const uint8_t *packet_md5;
+    const uint8_t *set_id;
+} p2g_server_result;
+
+typedef struct p2g_server_stats {
+    uint64_t submitted, admitted, completed, released;
+    uint64_t waves, items;
+    uint32_t queued, resident;
+    uint64_t resident_bytes, peak_resident_bytes, budget_bytes;
+} p2g_server_stats;
+
+p2g_status p2g_server_create(const p2g_server_options *opts, p2g_server **out);
+/* Validates (as p2g_run_device_job) and queues one job; never blocks on the device. */
+p2g_status p2g_server_submit(p2g_server *server, const p2g_server_job *job, uint64_t *ticket);
+/* Up to cap completed jobs not yet polled; waits up to wait_ms for the first. */
+p2g_status p2g_server_poll(p2g_server *server, p2g_server_result *out, uint32_t cap, uint32_t *n_out,
+                           uint32_t wait_ms);
+/* Frees a completed job's device memory (after the caller's reads of it have finished). */
+p2g_status p2g_server_release(p2g_server *server, uint64_t ticket);
+p2g_status p2g_server_get_stats(p2g_server *server, p2g_server_stats *out);
+double p2g_server_now(p2g_server *server);
+/* Stops the scheduler, waits for the device, frees every job. */
+void p2g_server_destroy(p2g_server *server);
+/* Synchronous device-to-host copy of result bytes (for callers that do not
+ * link the CUDA runtime themselves). */
+p2g_status p2g_copy_to_host(void *dst, const void *device_src, uint64_t bytes);
+
 /* ---- host helpers of the reference's public format/packet modules ----- */
 
 /* generate_input_bases, src/reedsolomon.rs:130-149 */

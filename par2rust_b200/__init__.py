@@ -666,6 +666,131 @@ class Batch:
             pass
 
 
+# ---------------------------------------------------------------------------
+# Serving loop (no counterpart in the reference): continuous batching of
+# create requests on the device.
+# ---------------------------------------------------------------------------
+SOURCE_HOST = 0
+SOURCE_SEEDED = 1
+
+
+@dataclass
+class ServerResult:
+    ticket: int
+    tag: int
+    status: int
+    submit_s: float
+    admit_s: float
+    done_s: float
+    source_bytes: int
+    input_slices: int
+    recovery_count: int
+    file_count: int
+    slice_size: int
+    ptr: dict  # device pointers: src, recovery, checksums, hash16k, packet_md5, set_id
+    recovery_stride: int
+
+    @property
+    def latency_s(self) -> float:
+        return self.done_s - self.submit_s
+
+
+def copy_to_host(device_ptr: int, nbytes: int) -> bytes:
+    buf = C.create_string_buffer(max(nbytes, 1))
+    _check(lib().p2g_copy_to_host(buf, device_ptr, nbytes))
+    return buf.raw[:nbytes]
+
+
+class Server:
+    """Create-request server (p2g_server_*): jobs are admitted by HBM
+    footprint and run in device waves shared with the other resident jobs.
+    ``submit_*`` returns a ticket; ``poll`` returns completed jobs, whose
+    device outputs stay valid until ``release``."""
+
+    def __init__(self, hbm_budget: int = 0, wave_ms: float = 0.0, max_jobs: int = 0):
+        o = _ffi.p2g_server_options(hbm_budget=hbm_budget, wave_ms=wave_ms, max_jobs=max_jobs, flags=0)
+        h = C.c_void_p()
+        _check(lib().p2g_server_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self._slices = {}
+        self._keep = {}
+
+    def _submit(self, file_lengths, names, slice_size, recovery_count, kind, host_src=None, seeds=None, tag=0):
+        n = len(file_lengths)
+        lens = (C.c_uint64 * max(n, 1))(*file_lengths)
+        nbufs = [C.create_string_buffer(bytes(x), len(x)) for x in names]
+        nptrs = (C.c_void_p * max(n, 1))(*[C.addressof(b) for b in nbufs])
+        nlens = (C.c_size_t * max(n, 1))(*[len(x) for x in names])
+        sd = (C.c_uint64 * max(n, 1))(*(seeds or [0] * n))
+        job = _ffi.p2g_server_job(file_count=n, file_lengths=lens, names=nptrs, name_lens=nlens,
+                                  slice_size=slice_size, recovery_count=recovery_count, source_kind=kind,
+                                  host_src=host_src, file_seeds=sd, tag=tag)
+        t = C.c_uint64()
+        _check(lib().p2g_server_submit(self._h, C.byref(job), C.byref(t)))
+        self._slices[t.value] = slice_size
+        return t.value
+
+    def submit_seeded(self, file_lengths: Sequence[int], seeds: Sequence[int], names: Sequence[bytes],
+                      slice_size: int, recovery_count: int, tag: int = 0) -> int:
+        return self._submit(file_lengths, names, slice_size, recovery_count, SOURCE_SEEDED, seeds=list(seeds), tag=tag)
+
+    def submit_host(self, host_src, file_lengths: Sequence[int], names: Sequence[bytes], slice_size: int,
+                    recovery_count: int, tag: int = 0) -> int:
+        """host_src: the files back to back, slice-padded (a pinned torch tensor
+        copies asynchronously); kept referenced until the job is released."""
+        ptr = host_src.data_ptr() if hasattr(host_src, "data_ptr") else host_src.ctypes.data
+        t = self._submit(file_lengths, names, slice_size, recovery_count, SOURCE_HOST, host_src=ptr, tag=tag)
+        self._keep[t] = host_src
+        return t
+
+    def poll(self, max_results: int = 1024, wait_ms: int = 0) -> List[ServerResult]:
+        arr = (_ffi.p2g_server_result * max_results)()
+        n = C.c_uint32()
+        _check(lib().p2g_server_poll(self._h, arr, max_results, C.byref(n), wait_ms))
+        out = []
+        for r in arr[:n.value]:
+            out.append(ServerResult(r.ticket, r.tag, r.status, r.submit_s, r.admit_s, r.done_s, r.source_bytes,
+                                    r.input_slices, r.recovery_count, r.file_count, self._slices.get(r.ticket, 0),
+                                    {"src": r.src, "recovery": r.recovery, "checksums": r.checksums,
+                                     "hash16k": r.hash16k, "packet_md5": r.packet_md5, "set_id": r.set_id},
+                                    r.recovery_stride))
+        return out
+
+    def outputs(self, res: ServerResult) -> dict:
+        """Copy a completed job's outputs to host bytes."""
+        R, S, n = res.recovery_count, res.input_slices, res.file_count
+        rec = copy_to_host(res.ptr["recovery"], R * res.recovery_stride) if R else b""
+        rows = [rec[r * res.recovery_stride:r * res.recovery_stride + res.slice_size] for r in range(R)]
+        return {"recovery": rows, "checksums": copy_to_host(res.ptr["checksums"], 20 * S),
+                "hash16k": copy_to_host(res.ptr["hash16k"], 16 * n),
+                "packet_md5": copy_to_host(res.ptr["packet_md5"], 16 * R) if R else b"",
+                "set_id": copy_to_host(res.ptr["set_id"], 16)}
+
+    def release(self, ticket: int) -> None:
+        _check(lib().p2g_server_release(self._h, ticket))
+        self._keep.pop(ticket, None)
+        self._slices.pop(ticket, None)
+
+    def stats(self) -> dict:
+        st = _ffi.p2g_server_stats()
+        _check(lib().p2g_server_get_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _ffi.p2g_server_stats._fields_}
+
+    def now(self) -> float:
+        return lib().p2g_server_now(self._h)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().p2g_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def batch_plan(shapes: Sequence[Tuple[int, int, int, int]], ctas: int = 148, flags: int = 0
                ) -> Tuple[BatchInfo, List[int]]:
     """The batch planner alone (no device): shapes are (slice_size,
@@ -760,5 +885,6 @@ __all__ = [
     "encode_device", "slice_checksums", "file_hashes", "recovery_packet_md5", "input_bases", "gf_mul", "gf_pow",
     "resolve_volume_sizes", "volume_filename", "build_packet", "build_main_packet", "compute_file_id", "md5",
     "kernel_launch_count", "device_info", "DeviceJobBuffers", "run_device_job", "BATCH_NO_GRAPH",
-    "BATCH_NO_AUTOTUNE", "BATCH_DERIVE_BASIS", "BatchJobSpec", "BatchInfo", "Batch", "batch_plan",
+    "BATCH_NO_AUTOTUNE", "BATCH_DERIVE_BASIS", "SOURCE_HOST", "SOURCE_SEEDED", "ServerResult", "Server",
+    "copy_to_host", "BatchJobSpec", "BatchInfo", "Batch", "batch_plan",
 ]

@@ -178,6 +178,63 @@ class p2g_batch_shape(C.Structure):
     ]
 
 
+class p2g_server_options(C.Structure):
+    _fields_ = [("hbm_budget", C.c_uint64), ("wave_ms", C.c_double), ("max_jobs", C.c_uint32), ("flags", C.c_uint32)]
+
+
+class p2g_server_job(C.Structure):
+    _fields_ = [
+        ("file_count", C.c_uint32),
+        ("file_lengths", C.POINTER(C.c_uint64)),
+        ("names", C.POINTER(C.c_void_p)),
+        ("name_lens", C.POINTER(C.c_size_t)),
+        ("slice_size", C.c_uint64),
+        ("recovery_count", C.c_uint32),
+        ("source_kind", C.c_uint32),
+        ("host_src", C.c_void_p),
+        ("file_seeds", C.POINTER(C.c_uint64)),
+        ("tag", C.c_uint64),
+    ]
+
+
+class p2g_server_result(C.Structure):
+    _fields_ = [
+        ("ticket", C.c_uint64),
+        ("tag", C.c_uint64),
+        ("status", C.c_int32),
+        ("submit_s", C.c_double),
+        ("admit_s", C.c_double),
+        ("done_s", C.c_double),
+        ("source_bytes", C.c_uint64),
+        ("input_slices", C.c_uint32),
+        ("recovery_count", C.c_uint32),
+        ("file_count", C.c_uint32),
+        ("src", C.c_void_p),
+        ("recovery", C.c_void_p),
+        ("recovery_stride", C.c_uint64),
+        ("checksums", C.c_void_p),
+        ("hash16k", C.c_void_p),
+        ("packet_md5", C.c_void_p),
+        ("set_id", C.c_void_p),
+    ]
+
+
+class p2g_server_stats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_uint64),
+        ("admitted", C.c_uint64),
+        ("completed", C.c_uint64),
+        ("released", C.c_uint64),
+        ("waves", C.c_uint64),
+        ("items", C.c_uint64),
+        ("queued", C.c_uint32),
+        ("resident", C.c_uint32),
+        ("resident_bytes", C.c_uint64),
+        ("peak_resident_bytes", C.c_uint64),
+        ("budget_bytes", C.c_uint64),
+    ]
+
+
 # (name, restype, argtypes) for every entry point of include/par2gpu.h
 SIGNATURES = [
     ("p2g_last_error_message", C.c_char_p, []),
@@ -222,6 +279,15 @@ SIGNATURES = [
     ("p2g_batch_plan", C.c_int,
      [C.POINTER(p2g_batch_shape), C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(p2g_batch_info),
       C.POINTER(C.c_uint32)]),
+    ("p2g_server_create", C.c_int, [C.POINTER(p2g_server_options), C.POINTER(C.c_void_p)]),
+    ("p2g_server_submit", C.c_int, [C.c_void_p, C.POINTER(p2g_server_job), C.POINTER(C.c_uint64)]),
+    ("p2g_server_poll", C.c_int,
+     [C.c_void_p, C.POINTER(p2g_server_result), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
+    ("p2g_server_release", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("p2g_server_get_stats", C.c_int, [C.c_void_p, C.POINTER(p2g_server_stats)]),
+    ("p2g_server_now", C.c_double, [C.c_void_p]),
+    ("p2g_server_destroy", None, [C.c_void_p]),
+    ("p2g_copy_to_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     ("p2g_input_bases", C.c_int, [C.c_uint32, C.POINTER(C.c_uint16)]),
     ("p2g_gf_mul", C.c_uint16, [C.c_uint16, C.c_uint16]),
     ("p2g_gf_pow", C.c_uint16, [C.c_uint16, C.c_uint32]),

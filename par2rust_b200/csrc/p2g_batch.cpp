@@ -50,22 +50,9 @@ struct PlanJob {
     double finish = 0;           // finish-step estimate
 };
 
-double finish_ms(const PlanJob& j) {
-    const double files = ceil(j.n / 256.0) * (md5_ms(P2G_HASH16K_LEN) + md5_ms(24 + 256));
-    const double sort = (double)j.n * j.n / 512.0 * 4e-6;
-    const double body = md5_ms(12 + 16ull * j.n);
-    const double pkt = ceil(j.R / 256.0) * md5_ms(36 + j.slice);
-    return files + sort + body + pkt + kItemMs;
-}
-inline double encode_ms(const PlanJob& j, uint32_t syms) {
-    return (double)j.S * (round_up(syms, 8) + kBuildCost) / kEncRate + kItemMs;
-}
-inline double scan_ms(const PlanJob& j, uint32_t count) {
-    // MD5 lanes run in parallel; the CRC warps take count/8 slices each at
-    // about 6 shared loads per 4 bytes per lane, mostly hidden behind them
-    const double crc = ceil(count / 8.0) * (double)j.slice / 128.0 * 6.0 / 1.9e6;
-    return std::max(md5_ms(j.slice), crc) + kItemMs;
-}
+double finish_ms(const PlanJob& j) { return est_set_id_ms(j.n) + est_packet_item_ms(j.slice, j.R); }
+inline double encode_ms(const PlanJob& j, uint32_t syms) { return est_encode_item_ms(j.S, syms); }
+inline double scan_ms(const PlanJob& j, uint32_t count) { return est_scan_item_ms(j.slice, count); }
 
 void set_tiling(PlanJob& j, uint32_t tiles) {
     const uint32_t ts = (uint32_t)std::min<uint64_t>(round_up((j.Np + tiles - 1) / tiles, 8), kEncTileSymbols);
@@ -201,6 +188,23 @@ Plan plan_batch(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
 }
 
 }  // namespace
+
+double est_md5_ms(uint64_t bytes) { return md5_ms(bytes); }
+double est_encode_item_ms(uint32_t slices, uint32_t syms) {
+    return (double)slices * (round_up(syms, 8) + kBuildCost) / kEncRate + kItemMs;
+}
+double est_scan_item_ms(uint64_t slice, uint32_t count) {
+    // MD5 lanes run in parallel; the CRC warps take count/8 slices each at
+    // about 6 shared loads per 4 bytes per lane, mostly hidden behind them
+    const double crc = ceil(count / 8.0) * (double)slice / 128.0 * 6.0 / 1.9e6;
+    return std::max(md5_ms(slice), crc) + kItemMs;
+}
+double est_set_id_ms(uint32_t files) {
+    const double hashes = ceil(files / 256.0) * (md5_ms(P2G_HASH16K_LEN) + md5_ms(24 + 256));
+    const double sort = (double)files * files / 512.0 * 4e-6;
+    return hashes + sort + md5_ms(12 + 16ull * files) + kItemMs;
+}
+double est_packet_item_ms(uint64_t slice, uint32_t rows) { return ceil(rows / 256.0) * md5_ms(36 + slice) + kItemMs; }
 
 // ---------------------------------------------------------------------------
 // The batch object

@@ -168,6 +168,17 @@ size_t batch_smem_bytes();
 cudaError_t launch_basis_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_words, cudaStream_t st);
 // The persistent kernel: `ctas` CTAs; ctl[0] queue head, ctl[1+j] completed
 // encode items of job j (zeroed before each launch).
+// Seeded synthetic files (3 words per file in `spans`: offset, length,
+// padded length; one seed per file), blockIdx.y = file.
+cudaError_t launch_seeded_fill(uint8_t* base, const uint64_t* spans, const uint64_t* seeds, uint32_t n_files,
+                               uint64_t max_padded, cudaStream_t st);
+// Cost model shared by the batch planner and the server's wave builder
+// (milliseconds of one CTA).
+double est_md5_ms(uint64_t bytes);
+double est_encode_item_ms(uint32_t slices, uint32_t syms);
+double est_scan_item_ms(uint64_t slice, uint32_t count);
+double est_set_id_ms(uint32_t files);
+double est_packet_item_ms(uint64_t slice, uint32_t rows);
 // Sets the batch kernel's shared-memory attribute (call before stream capture).
 cudaError_t prepare_batch_kernel();
 cudaError_t launch_batch(const BatchJob* jobs, const BatchItem* items, uint32_t n_items, uint32_t* ctl, int* err,

@@ -1216,6 +1216,34 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     }
 }
 
+// Seeded synthetic source: file f of a job occupies [off, off+padded) of
+// `base`; its bytes are the splitmix64 counter stream of seed f (8-byte word
+// k = mix(seed + (k+1)*0x9E3779B97F4A7C15), little-endian) for `len` bytes,
+// then zeros.  Offsets are multiples of 4 (slice boundaries).
+__device__ __forceinline__ uint64_t splitmix_word(uint64_t seed, uint64_t k) {
+    uint64_t z = seed + (k + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__global__ void seeded_fill_kernel(uint8_t* __restrict__ base, const uint64_t* __restrict__ spans,
+                                   const uint64_t* __restrict__ seeds) {
+    const uint64_t off = spans[3 * blockIdx.y], len = spans[3 * blockIdx.y + 1], padded = spans[3 * blockIdx.y + 2];
+    const uint64_t seed = seeds[blockIdx.y];
+    uint32_t* dst = reinterpret_cast<uint32_t*>(base + off);
+    const uint64_t words = padded / 4;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t v = 0;
+        const uint64_t b = 4 * w;
+        if (b < len) {
+            const uint64_t z = splitmix_word(seed, w >> 1);
+            v = (w & 1) ? (uint32_t)(z >> 32) : (uint32_t)z;
+            if (b + 4 > len) v &= 0xFFFFFFFFu >> (8 * (b + 4 - len));
+        }
+        dst[w] = v;
+    }
+}
+
 __global__ void basis_batch_kernel(const BatchJob* __restrict__ jobs) {
     const BatchJob& J = jobs[blockIdx.y];
     if (!J.R || !J.basis) return;
@@ -1549,6 +1577,16 @@ cudaError_t launch_basis_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t m
     const uint64_t want = (max_words + 255) / 256;
     const unsigned bx = (unsigned)(want < (uint64_t)sm_count() * 4 ? want : (uint64_t)sm_count() * 4);
     basis_batch_kernel<<<dim3(bx, n_jobs), 256, 0, st>>>(jobs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_seeded_fill(uint8_t* base, const uint64_t* spans, const uint64_t* seeds, uint32_t n_files,
+                               uint64_t max_padded, cudaStream_t st) {
+    if (!n_files || !max_padded) return cudaSuccess;
+    const uint64_t want = (max_padded / 4 + 255) / 256;
+    const unsigned bx = (unsigned)(want < (uint64_t)sm_count() * 8 ? want : (uint64_t)sm_count() * 8);
+    seeded_fill_kernel<<<dim3(bx, n_files), 256, 0, st>>>(base, spans, seeds);
     count_launch();
     return cudaGetLastError();
 }

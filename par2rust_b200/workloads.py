@@ -185,3 +185,45 @@ def shard_jobs(jobs: List[Job], rank: int, world: int) -> List[int]:
         owner[i] = r
         load[r] += job_cost(jobs[i])
     return [i for i in range(len(jobs)) if owner[i] == rank]
+
+
+SERVE_SLICES = [16384, 65536, 262144, 1048576]
+
+
+def serve_requests(n: int = 10_000, seed: int = 5) -> List[Job]:
+    """Serving-loop requests: job totals log-uniform in [1 MiB, 2 GiB], split
+    into 1-32 files (random cut weights, each file >= 1 byte); slice drawn
+    from {16K, 64K, 256K, 1M} as in the batched config, raised to the
+    smallest slice of that set with at most 32,768 slices when the draw
+    exceeds it; R = max(1, ceil(f*S)), f ~ U[0.01, 0.20]."""
+    m = Meta(seed ^ 0xA5A5A5A5A5A5A5A5)
+    jobs = []
+    for jid in range(n):
+        total = m.log_uniform(1 << 20, 2 << 30)
+        nf = m.randint(1, 32)
+        w = [m.uniform() + 1e-9 for _ in range(nf)]
+        sw = sum(w)
+        lens = [max(1, int(total * x / sw)) for x in w]
+        lens[-1] = max(1, total - sum(lens[:-1]))
+        k = m.randint(0, 3)
+        f = 0.01 + 0.19 * m.uniform()
+        while True:
+            ss = SERVE_SLICES[k]
+            S = sum((x + ss - 1) // ss for x in lens)
+            if S <= 32768 or k == len(SERVE_SLICES) - 1:
+                break
+            k += 1
+        R = max(1, math.ceil(f * S))
+        jobs.append(Job(ss, R, lens, [file_seed(seed, jid, i) for i in range(nf)], "single"))
+    return jobs
+
+
+def poisson_arrivals(n: int, rate: float, seed: int) -> List[float]:
+    """Open-loop arrival times (seconds from 0) of n requests at `rate` per
+    second: exponential gaps from a splitmix64 stream."""
+    m = Meta(seed)
+    t, out = 0.0, []
+    for _ in range(n):
+        t += -math.log(1.0 - m.uniform()) / rate
+        out.append(t)
+    return out
