@@ -49,6 +49,8 @@ WORKLOADS = {
     "batch_256": dict(batch=True, n_jobs=256, seed=4),
     # serving loop: open-loop Poisson arrivals of create requests
     "serve": dict(serve=True, seed=5),
+    # dense contraction: 2,000 files log-uniform in [1 KiB, 8 MiB], R 2,000, Uniform{15}
+    "many_2000": dict(many=True, seed=3),
 }
 
 
@@ -458,6 +460,109 @@ def run_serve(args, wl):
     return 0
 
 
+def run_many(args, wl):
+    """--workload many_2000: one create job over 2,000 files with 2,000
+    recovery blocks through the plain per-job device path."""
+    import numpy as np
+    import torch
+
+    import par2rust_b200 as p2g
+    from par2rust_b200 import workloads as W
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    job = W.many_2000(seed=wl["seed"])
+    sl, R, S = job.slice_size, job.recovery, job.slices
+    names = [f"file{i:04d}.bin".encode() for i in range(len(job.file_lengths))]
+    src = torch.zeros(S * sl, dtype=torch.uint8, device=dev)
+    off = 0
+    for n, sd in zip(job.file_lengths, job.seeds):
+        src[off:off + n] = W.file_bytes_torch(sd, n, device=dev)
+        off += (n + sl - 1) // sl * sl
+    bufs = p2g.DeviceJobBuffers(S, len(names), sl, R, dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        p2g.run_device_job(src, job.file_lengths, names, sl, R, bufs, skip_hash_full=True)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = p2g.kernel_launch_count()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        p2g.run_device_job(src, job.file_lengths, names, sl, R, bufs, skip_hash_full=True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = p2g.kernel_launch_count() - l0
+    ms = a.elapsed_time(b) / args.steps
+    total = job.source_bytes
+    macs = S * R * (sl // 2)
+    # the encode alone (basis + encode kernels)
+    enc = []
+    for i in range(args.warmup + args.steps):
+        x, y = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        x.record(stream)
+        p2g.encode_device(src.data_ptr(), sl, S, sl, R, bufs.recovery.data_ptr(), bufs.rec_stride, stream.cuda_stream)
+        y.record(stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            enc.append(x.elapsed_time(y))
+    enc_ms = sum(enc) / len(enc)
+    # e2e: the public in-memory create with pinned host files
+    host = [torch.empty(n, dtype=torch.uint8, pin_memory=True) for n in job.file_lengths]
+    off = 0
+    for h, n in zip(host, job.file_lengths):
+        h.copy_(src[off:off + n])
+        off += (n + sl - 1) // sl * sl
+    opts = p2g.CreateOptions(output="many.par2", slice_size=sl, recovery_block_count=R,
+                             volume_scheme=p2g.VolumeScheme.Uniform(15))
+    e2e = None
+    if args.e2e_steps:
+        inputs = list(zip(names, host))
+        p2g.create_in_memory(opts, inputs)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            files = p2g.create_in_memory(opts, inputs)
+        es = (time.perf_counter() - t0) / args.e2e_steps
+        e2e = {"value": total / es / 1e9, "unit": "GB/s", "h2d_bytes_per_step": total,
+               "d2h_bytes_per_step": R * sl + S * 20 + 16 * R, "seconds_per_step": es,
+               "api": "p2g_create_in_memory (2,000 pinned host files)", "output_files": len(files)}
+    cb = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as orc
+
+        # a bounded prefix of the concatenated files, same slice and R
+        data = np.concatenate([h.numpy() for h in host[:200]])
+        n_sl = max(1, min(len(data) // sl, int(args.cpu_seconds * 4)))
+        sample = data[:n_sl * sl]
+        t, *_ = orc.create_timed(sample, sl, R, 0)
+        cb = {"value": len(sample) / t / 1e9, "unit": "GB/s", "cores": orc.max_threads(), "kind": "port",
+              "sample": f"{n_sl} slices ({len(sample)} B) of the first files, R={R}", "seconds": t}
+    hbm_peak, peak_kind = measured_peaks()
+    alg = S * sl + R * sl
+    line = {
+        "metric": "encode source GB/s", "value": total / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": "many_2000: 2,000 files log-uniform [1 KiB, 8 MiB], slice 262,144, R 2,000, "
+                               "Uniform{15}", "files": len(names), "source_bytes": total, "input_slices": S,
+                   "recovery_blocks": R, "parallelism": "1 GPU"},
+        "e2e": e2e,
+        "roofline": {"bound": "hbm", "achieved": alg / (enc_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": alg / (enc_ms * 1e-3) / 1e9 / hbm_peak, "traffic": None, "peak_source": peak_kind,
+                     "kernel": "basis_kernel + encode_lut_kernel", "kernel_ms": enc_ms, "algorithmic_bytes": alg},
+        "lut_roofline": {"achieved": macs / (enc_ms * 1e-3), "peak": 32 * 148 * 1965e6, "unit": "GF(2^16) MAC/s",
+                         "frac": macs / (enc_ms * 1e-3) / (32 * 148 * 1965e6), "macs_per_launch": macs},
+        "variant": "LUT (int8 bit-sliced tensor form not built: its shared-memory operand traffic per GF MAC is "
+                   "not below the packed LUT's)",
+        "cpu_baseline": cb, "clocks": clk, "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference_batch(args, wl):
     rank, world, local = dist_env()
     if rank != 0:
@@ -583,11 +688,37 @@ def main():
             return 0
         if wl.get("batch"):
             return run_reference_batch(args, wl)
+        if wl.get("many"):
+            rank, _, _ = dist_env()
+            if rank != 0:
+                return 0
+            import numpy as np
+
+            from oracle import oracle as orc
+            from par2rust_b200 import workloads as W
+
+            job = W.many_2000(seed=wl["seed"])
+            data = np.concatenate([W.file_bytes(sd, n) for n, sd in list(zip(job.file_lengths, job.seeds))[:200]])
+            n_sl = max(1, min(len(data) // job.slice_size, int(args.cpu_seconds * 4)))
+            sample = data[:n_sl * job.slice_size]
+            ts = [orc.create_timed(sample, job.slice_size, job.recovery, 0)[0] for _ in range(max(1, args.steps))]
+            v = len(sample) / (sum(ts) / len(ts)) / 1e9
+            print(json.dumps({"metric": "encode source GB/s", "value": v, "unit": "GB/s", "n_gpus": args.gpus,
+                              "steps": args.steps, "warmup": 0, "ms_per_step": sum(ts) / len(ts) * 1e3,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+                              "data": "synthetic", "impl": "reference", "config": {"workload": "many_2000"},
+                              "cpu_baseline": {"value": v, "unit": "GB/s", "cores": orc.max_threads(), "kind": "port",
+                                               "sample": f"{n_sl} slices of the first files, R={job.recovery}"},
+                              "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+                  flush=True)
+            return 0
         return run_reference(args, wl)
     if wl.get("batch"):
         return run_batch(args, wl)
     if wl.get("serve"):
         return run_serve(args, wl)
+    if wl.get("many"):
+        return run_many(args, wl)
 
     import numpy as np
     import torch
