@@ -629,7 +629,7 @@ def run_batch(args, wl):
     dev = torch.device("cuda", local)
     clocks = ClockSampler(local)
     clocks.start()
-    res = bench_batch(dev, args.steps, args.warmup, plain_steps=1, n_jobs=wl["n_jobs"],
+    res = bench_batch(dev, args.steps, args.warmup, plain_steps=1, n_jobs=args.batch_jobs or wl["n_jobs"],
                       e2e_steps=args.e2e_steps)
     clk = clocks.stop()
     t = torch.tensor([res["batched_ms"]], device=dev)
