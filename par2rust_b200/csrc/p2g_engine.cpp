@@ -345,8 +345,9 @@ static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) 
             reserve += hash_blocks(n);
             reserve_ms = std::max(reserve_ms, (double)(mx / 64) * 7.2e-4);
         }
-        plan = plan_encode(j.slice, j.S, RG, j.d_pkt != nullptr, reserve, reserve_ms);
-        if (plan.bands.size() > (size_t)Context::kBandEvents) plan = plan_encode(j.slice, j.S, RG, false, 0, 0.0);
+        plan = plan_encode(j.slice, j.S, RG, j.d_pkt != nullptr, reserve, reserve_ms, tail_fold(j.R));
+        if (plan.bands.size() > (size_t)Context::kBandEvents)
+            plan = plan_encode(j.slice, j.S, RG, false, 0, 0.0, tail_fold(j.R));
         tr.mark("basis", s_enc);
         P2G_CU(cudaEventRecord(c.ev_band[0], s_enc));  // basis (and realign) done
         P2G_CU(cudaStreamWaitEvent(s_enc2, c.ev_band[0], 0));

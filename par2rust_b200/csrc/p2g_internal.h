@@ -90,13 +90,17 @@ struct EncodeBand {
     uint32_t begin, end, ts;
 };
 struct EncodePlan {
-    uint32_t Np = 0;  // symbol positions processed per slice (slice rounded up to 16 B)
+    uint32_t Np = 0;    // symbol positions processed per slice (slice rounded up to 16 B)
+    uint32_t fold = 1;  // fold of the last row group (tail_fold)
     std::vector<EncodeBand> bands;
 };
+// Fold of the last row group for R recovery rows: 4 when it has <= 8 real
+// rows, 2 when <= 16, else 1 (its CTA then covers fold tiles).
+uint32_t tail_fold(uint32_t R);
 // banded: cut into whole-wave bands (packet-MD5 pipelining); reserve/reserve_ms:
 // SMs held by slice-MD5 blocks at the start of the job and for how long.
 EncodePlan plan_encode(uint64_t slice_size, uint32_t S, uint32_t RG, bool banded, uint32_t reserve,
-                       double reserve_ms);
+                       double reserve_ms, uint32_t fold = 1);
 cudaError_t launch_encode_band(const EncodePlan& pl, uint32_t band, const uint8_t* src, uint64_t src_stride,
                                uint32_t S, const uint16_t* basis, uint32_t RG, uint32_t R, uint8_t* rec,
                                uint64_t rec_stride, int* err, cudaStream_t st, uint32_t first_exp = 0);
@@ -105,7 +109,7 @@ uint32_t hash_blocks(uint32_t streams);
 
 // Encode tiling: tile size (symbols, multiple of 8) and tile count for Np
 // symbols, RG row groups and `sms` SMs.
-void choose_tiles(uint32_t Np, uint32_t RG, uint32_t sms, uint32_t* ts_out, uint32_t* tiles_out);
+void choose_tiles(uint32_t Np, uint32_t RG, uint32_t sms, uint32_t* ts_out, uint32_t* tiles_out, uint32_t fold = 1);
 
 // Heap-free variants used by the allocation-free entry point.
 cudaError_t upload_tables_noheap();

@@ -141,8 +141,11 @@ __device__ __forceinline__ uint32_t lds32(uint32_t addr) {
 // (lane = row pair + 16*hi) hit 32 distinct banks.  Rows r >= R get 0 (their
 // tables are all-zero and never stored).
 // ---------------------------------------------------------------------------
+// fold > 1: the last row group's rows repeat its first 32/fold rows (the
+// layout a folded encode CTA builds its replicated tables from; an unfolded
+// CTA only stores rows < R, which are the same either way).
 __device__ __forceinline__ void basis_fill(uint16_t* __restrict__ basis, uint32_t S, uint32_t RG, uint32_t R,
-                                           uint32_t first_exp, uint64_t start, uint64_t step) {
+                                           uint32_t first_exp, uint64_t start, uint64_t step, uint32_t fold = 1) {
     const uint64_t total = (uint64_t)S * RG * 512;
     for (uint64_t idx = start; idx < total; idx += step) {
         const uint32_t rl = (uint32_t)(idx & 31);
@@ -152,7 +155,7 @@ __device__ __forceinline__ void basis_fill(uint16_t* __restrict__ basis, uint32_
         const uint64_t sg = idx >> 9;
         const uint32_t rg = (uint32_t)(sg % RG);
         const uint32_t s = (uint32_t)(sg / RG);
-        const uint32_t r = rg * kRowsPerGroup + rl;
+        const uint32_t r = rg * kRowsPerGroup + (rg + 1 == RG ? rl & (31u >> (fold >> 1)) : rl);
         uint16_t v = 0;
         if (r < R) {
             const uint32_t e = first_exp + r;
@@ -166,9 +169,9 @@ __device__ __forceinline__ void basis_fill(uint16_t* __restrict__ basis, uint32_
 }
 
 __global__ void basis_kernel(uint16_t* __restrict__ basis, uint32_t S, uint32_t RG, uint32_t R,
-                             uint32_t first_exp) {
+                             uint32_t first_exp, uint32_t fold) {
     basis_fill(basis, S, RG, R, first_exp, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
-               (uint64_t)gridDim.x * blockDim.x);
+               (uint64_t)gridDim.x * blockDim.x, fold);
 }
 
 // ---------------------------------------------------------------------------
@@ -200,10 +203,14 @@ __host__ __device__ constexpr int ctz5(int u) {
     return (u & 1) ? 0 : (u & 2) ? 1 : (u & 4) ? 2 : (u & 8) ? 3 : 4;
 }
 
-template <int NCH>
+// FMAX: largest row-group fold the CTA may run (a stage holds FMAX tiles).
+template <int NCH, int FMAX = 1>
+__host__ __device__ constexpr size_t encode_bars_offset() {
+    return 2 * kTabBytes + (size_t)kEncStages * (FMAX * (kEncThreads / 32) * NCH * 64 * 2 + 1024);
+}
+template <int NCH, int FMAX = 1>
 __host__ __device__ constexpr size_t encode_smem_bytes() {
-    return 2 * kTabBytes + (size_t)kEncStages * ((kEncThreads / 32) * NCH * 64 * 2 + 1024) +
-           kEncStages * sizeof(uint64_t);
+    return encode_bars_offset<NCH, FMAX>() + kEncStages * sizeof(uint64_t);
 }
 
 // One (row group, symbol tile) work unit of the accumulator: 32 rows x
@@ -222,6 +229,13 @@ __host__ __device__ constexpr size_t encode_smem_bytes() {
 // accumulate it XORs its partial sums into the recovery rows (atomic XOR
 // reductions, so chunks of one tile may run concurrently on rows that start
 // zeroed).
+//
+// fold (1, 2 or 4; <= FMAX): a row group with at most 32/fold real rows
+// replicates its coefficients fold times across the 32 table rows, and lane
+// k's row quad then serves sub-tile k >> (2 - log2 fold) of fold adjacent
+// sub-tiles of sub_syms symbols.  Lookups keep the 32-row bank pattern (each
+// lane still reads quad k of a table row), so a short last row group costs
+// 1/fold of a full one instead of a full one.
 __device__ __forceinline__ uint32_t mod_field(uint32_t x) {  // x mod 65535 for x < 2^32
     x = (x & 0xFFFFu) + (x >> 16);
     x = (x & 0xFFFFu) + (x >> 16);
@@ -235,15 +249,15 @@ __device__ __forceinline__ void red_xor4(uint8_t* p, const uint4& v) {
     asm volatile("red.global.xor.b32 [%0], %1;" ::"l"(q + 3), "r"(v.w) : "memory");
 }
 
-template <int NCH, bool GEN = false>
+template <int NCH, bool GEN = false, int FMAX = 1>
 __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S,
                                             const uint16_t* __restrict__ basis, uint32_t RG, uint32_t rg,
                                             uint32_t R, uint32_t n0, uint32_t tile_syms,
                                             uint8_t* __restrict__ rec, uint64_t rec_stride, uint8_t* smem,
                                             uint32_t& phase, uint32_t first_exp = 0, uint32_t s0 = 0,
-                                            bool accumulate = false) {
+                                            bool accumulate = false, uint32_t fold = 1, uint32_t sub_syms = 0) {
     constexpr int WARPS = kEncThreads / 32;
-    constexpr int NT = WARPS * NCH * 64;  // symbol capacity of a tile (tile_syms <= NT)
+    constexpr int NT = FMAX * WARPS * NCH * 64;  // symbol capacity of a stage (tile_syms <= NT)
     static_assert(!GEN || WARPS == 16, "derived basis: one warp per basis product j");
     uint8_t* tabs = smem;
     uint8_t* src_st = smem + 2 * kTabBytes;
@@ -268,7 +282,7 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
         for (int st = 0; st < kEncStages && (uint32_t)st < S; ++st) issue(st, st);
 
     // derived basis: this thread's (j = warp, row = lane) entry and its offset in a slot
-    const uint32_t g_row = rg * kRowsPerGroup + lane;
+    const uint32_t g_row = rg * kRowsPerGroup + (lane & (31u >> (fold >> 1)));  // replicated when folded
     const uint32_t g_exp = first_exp + g_row;
     const bool g_live = g_row < R;
     const uint32_t g_off = (uint32_t)((((warp & 7) * 2 + (warp >> 3)) * 32 + lane) * 2);
@@ -319,7 +333,12 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
     const uint32_t offB = odd ? 16 * k : (64 + 16 * k);
     const uint32_t selA0 = odd ? 0x4441u : 0x4440u, selB0 = odd ? 0x4440u : 0x4441u;
     const uint32_t selA1 = odd ? 0x4443u : 0x4442u, selB1 = odd ? 0x4442u : 0x4443u;
-    const uint32_t src_u32 = smem_u32(src_st) + (uint32_t)(warp * NCH * 8 + g) * 16;
+    // folded: this lane's sub-tile, its symbol limit and its rows' quad
+    const uint32_t sub = fold == 1 ? 0u : (uint32_t)k >> (fold == 2 ? 1 : 0);
+    if (fold == 1) sub_syms = tile_syms;
+    const uint32_t lim = tile_syms > sub * sub_syms ? min(sub_syms, tile_syms - sub * sub_syms) : 0u;
+    const uint32_t kq = (uint32_t)k & (3u >> (fold >> 1));
+    const uint32_t src_u32 = smem_u32(src_st) + sub * sub_syms * 2 + (uint32_t)(warp * NCH * 8 + g) * 16;
     // 128 = bytes per table row; read at run time so the address multiply-add
     // stays an IMAD (FMA pipe) instead of integer-ALU shift+add
     const uint32_t row_bytes = *reinterpret_cast<volatile const uint32_t*>(&d_row_bytes);
@@ -356,7 +375,7 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
         const uint32_t sbase = src_u32 + st * NT * 2;
 #pragma unroll
         for (int j = 0; j < NCH; ++j) {
-            if ((uint32_t)(warp * NCH * 8 + j * 8 + g) * 8 >= tile_syms) continue;  // chunk outside the tile
+            if ((uint32_t)(warp * NCH * 8 + j * 8 + g) * 8 >= lim) continue;  // chunk outside the (sub-)tile
             const uint4 w4 = lds128(sbase + j * 128);
             const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
@@ -402,11 +421,11 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
 #pragma unroll
     for (int j = 0; j < NCH; ++j) {
         const uint32_t chunk = (uint32_t)(warp * NCH * 8 + j * 8 + g);
-        const uint32_t n = n0 + chunk * 8;
-        if (chunk * 8 < tile_syms) {
+        const uint32_t n = n0 + sub * sub_syms + chunk * 8;
+        if (chunk * 8 < lim) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const uint32_t re = rg * kRowsPerGroup + 8 * k + 2 * q;
+                const uint32_t re = rg * kRowsPerGroup + 8 * kq + 2 * q;
                 uint4 we, wo;
                 we.x = __byte_perm(acc[j][0][q], acc[j][1][q], 0x5410);
                 we.y = __byte_perm(acc[j][2][q], acc[j][3][q], 0x5410);
@@ -431,17 +450,19 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
     return true;
 }
 
+// tail_fold: fold of the last row group (1, 2, 4); its CTA for tile t covers
+// tail_fold adjacent tiles, so the grid's tail-group CTAs past the band exit.
 template <int NCH, bool GEN>
 __global__ void __launch_bounds__(kEncThreads, 1)
     encode_lut_kernel(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S,
                       const uint16_t* __restrict__ basis, uint32_t RG, uint32_t R, uint32_t sym_begin,
                       uint32_t sym_end, uint32_t TS, uint8_t* __restrict__ rec, uint64_t rec_stride,
-                      uint32_t first_exp, int* __restrict__ err) {
+                      uint32_t first_exp, uint32_t tail_fold, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smem[];
-    constexpr int NT = (kEncThreads / 32) * NCH * 64;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * kTabBytes + kEncStages * (NT * 2 + 1024));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + encode_bars_offset<NCH, 4>());
     const uint32_t tile = blockIdx.x / RG, rg = blockIdx.x % RG;
-    const uint32_t n0 = sym_begin + tile * TS;
+    const uint32_t fold = rg + 1 == RG ? tail_fold : 1u;
+    const uint32_t n0 = sym_begin + tile * TS * fold;
     if (n0 >= sym_end) return;  // uniform: empty tile at the end of a band
     if (threadIdx.x == 0) {
         for (int st = 0; st < kEncStages; ++st) mbar_init(&bars[st], 1);
@@ -449,8 +470,8 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     }
     __syncthreads();
     uint32_t phase = 0;
-    if (!encode_tile<NCH, GEN>(src, src_stride, S, basis, RG, rg, R, n0, min(TS, sym_end - n0), rec, rec_stride,
-                               smem, phase, first_exp) &&
+    if (!encode_tile<NCH, GEN, 4>(src, src_stride, S, basis, RG, rg, R, n0, min(TS * fold, sym_end - n0), rec,
+                                  rec_stride, smem, phase, first_exp, 0, false, fold, TS) &&
         threadIdx.x == 0)
         atomicOr(err, 1);
 }
@@ -1270,7 +1291,23 @@ static int sm_count() {
 // symbol of its tile on lookups plus a fixed ~384 on building its tables, so
 // pick the tile count minimising ceil(tiles*RG/sms) * (tile + 384): the
 // fewest, fullest waves.
-void choose_tiles(uint32_t Np, uint32_t RG, uint32_t sms, uint32_t* ts_out, uint32_t* tiles_out) {
+uint32_t tail_fold(uint32_t R) {
+    if (!R) return 1;
+    const uint32_t tail = R - (R - 1) / kRowsPerGroup * kRowsPerGroup;  // rows of the last group, 1..32
+    return tail <= 8 ? 4u : tail <= 16 ? 2u : 1u;
+}
+// CTAs of `tiles` tiles over RG row groups whose last one is folded
+static inline uint64_t eff_ctas(uint64_t tiles, uint32_t RG, uint32_t fold) {
+    return tiles * (RG - 1) + (tiles + fold - 1) / fold;
+}
+// tiles per band so that its CTAs fit `budget` SMs (at least 1)
+static inline uint32_t tiles_for_budget(uint32_t budget, uint32_t RG, uint32_t fold) {
+    uint32_t t = (uint32_t)((uint64_t)budget * fold / ((uint64_t)(RG - 1) * fold + 1));
+    while (t > 1 && eff_ctas(t, RG, fold) > budget) --t;
+    return t ? t : 1;
+}
+
+void choose_tiles(uint32_t Np, uint32_t RG, uint32_t sms, uint32_t* ts_out, uint32_t* tiles_out, uint32_t fold) {
     constexpr uint64_t kBuildCost = 384;
     const uint32_t tmin = (Np + kEncTileSymbols - 1) / kEncTileSymbols;
     uint64_t best_cost = ~0ull;
@@ -1279,7 +1316,7 @@ void choose_tiles(uint32_t Np, uint32_t RG, uint32_t sms, uint32_t* ts_out, uint
         const uint32_t ts = ((Np + t - 1) / t + 7) & ~7u;
         if (ts == 0 || ts > (uint32_t)kEncTileSymbols) continue;
         const uint32_t tt = (Np + ts - 1) / ts;
-        const uint64_t waves = ((uint64_t)tt * RG + sms - 1) / sms;
+        const uint64_t waves = (eff_ctas(tt, RG, fold) + sms - 1) / sms;
         const uint64_t cost = waves * (ts + kBuildCost);
         if (cost < best_cost) {
             best_cost = cost;
@@ -1297,13 +1334,13 @@ cudaError_t launch_basis(uint16_t* basis, uint32_t S, uint32_t RG, uint32_t R, u
     if (!total) return cudaSuccess;
     const uint64_t want = (total + 255) / 256;
     const unsigned blocks = (unsigned)(want < (uint64_t)sm_count() * 16 ? want : (uint64_t)sm_count() * 16);
-    basis_kernel<<<blocks, 256, 0, st>>>(basis, S, RG, R, first_exp);
+    basis_kernel<<<blocks, 256, 0, st>>>(basis, S, RG, R, first_exp, tail_fold(R));
     count_launch();
     return cudaGetLastError();
 }
 
 static cudaError_t encode_attr() {
-    constexpr size_t smem = encode_smem_bytes<kEncChunks>();
+    constexpr size_t smem = encode_smem_bytes<kEncChunks, 4>();
     static bool attr_set[256] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1333,8 +1370,8 @@ static double est_band_ms(uint32_t S, uint32_t ts, uint32_t waves) {
 
 static void split_even(EncodePlan& pl, uint32_t begin, uint32_t RG, uint32_t budget, double* ms, uint32_t S) {
     if (begin >= pl.Np) return;
-    const uint32_t tiles = RG <= budget ? budget / RG : 1;
-    const uint32_t waves = RG <= budget ? 1 : (RG + budget - 1) / budget;
+    const uint32_t tiles = tiles_for_budget(budget, RG, pl.fold);
+    const uint32_t waves = (uint32_t)((eff_ctas(tiles, RG, pl.fold) + budget - 1) / budget);
     const uint64_t rem = pl.Np - begin;
     const uint64_t per = (uint64_t)tiles * kEncTileSymbols;
     const uint32_t B = (uint32_t)((rem + per - 1) / per);
@@ -1349,17 +1386,27 @@ static void split_even(EncodePlan& pl, uint32_t begin, uint32_t RG, uint32_t bud
 }
 
 EncodePlan plan_encode(uint64_t slice_size, uint32_t S, uint32_t RG, bool banded, uint32_t reserve,
-                       double reserve_ms) {
+                       double reserve_ms, uint32_t fold) {
     EncodePlan pl;
     pl.Np = (uint32_t)(((slice_size + 15) & ~15ull) / 2);
+    pl.fold = fold;
     const uint32_t sms = (uint32_t)sm_count();
     uint32_t ts1 = 0, t1 = 0;
-    choose_tiles(pl.Np, RG, sms, &ts1, &t1);
+    choose_tiles(pl.Np, RG, sms, &ts1, &t1, fold);
     EncodePlan c = pl;  // C: one launch, packet MD5 after it
     c.bands.push_back({0, pl.Np, ts1});
     if (!banded || sms < 4) return c;
+    // Banded plans run each band as one wave, which lasts as long as its
+    // slowest CTA; a folded tail CTA (4x the source reads of one tile) runs
+    // ~15% longer than the others, which cancels its saving there, so bands
+    // keep the last row group unfolded.
+    if (fold != 1) {
+        EncodePlan unfolded = plan_encode(slice_size, S, RG, banded, reserve, reserve_ms, 1);
+        if (unfolded.bands.size() > 1) return unfolded;
+        return c;
+    }
     const double chain_ms_per_byte = 7.2e-4 / 64;  // one MD5 chain: ~0.72 us per 64-byte block
-    const uint32_t waves1 = (uint32_t)(((uint64_t)t1 * RG + sms - 1) / sms);
+    const uint32_t waves1 = (uint32_t)((eff_ctas(t1, RG, fold) + sms - 1) / sms);
     const double ms_c = est_band_ms(S, ts1, waves1) + 2.0 * pl.Np * chain_ms_per_byte + reserve_ms;
     auto tail = [&](const EncodePlan& p) {  // last band's packet-MD5 step + per-band launch/drain
         const EncodeBand& l = p.bands.back();
@@ -1375,8 +1422,8 @@ EncodePlan plan_encode(uint64_t slice_size, uint32_t S, uint32_t RG, bool banded
     double ms_b = 1e30;
     if (reserve && reserve + 2 < sms) {
         const uint32_t budget = sms - reserve - 1;
-        const uint32_t tiles = RG <= budget ? budget / RG : 1;
-        const uint32_t waves = RG <= budget ? 1 : (RG + budget - 1) / budget;
+        const uint32_t tiles = tiles_for_budget(budget, RG, fold);
+        const uint32_t waves = (uint32_t)((eff_ctas(tiles, RG, fold) + budget - 1) / budget);
         uint32_t sym = 0;
         ms_b = 0;
         while (sym < pl.Np && ms_b < reserve_ms) {
@@ -1398,7 +1445,7 @@ EncodePlan plan_encode(uint64_t slice_size, uint32_t S, uint32_t RG, bool banded
 cudaError_t launch_encode_band(const EncodePlan& pl, uint32_t band, const uint8_t* src, uint64_t src_stride,
                                uint32_t S, const uint16_t* basis, uint32_t RG, uint32_t R, uint8_t* rec,
                                uint64_t rec_stride, int* err, cudaStream_t st, uint32_t first_exp) {
-    constexpr size_t smem = encode_smem_bytes<kEncChunks>();
+    constexpr size_t smem = encode_smem_bytes<kEncChunks, 4>();
     cudaError_t e = encode_attr();
     if (e != cudaSuccess) return e;
     if (band >= pl.bands.size() || !R) return cudaSuccess;
@@ -1407,10 +1454,10 @@ cudaError_t launch_encode_band(const EncodePlan& pl, uint32_t band, const uint8_
     const uint32_t tiles = (bd.end - bd.begin + bd.ts - 1) / bd.ts;
     if (basis)
         encode_lut_kernel<kEncChunks, false><<<tiles * RG, kEncThreads, smem, st>>>(
-            src, src_stride, S, basis, RG, R, bd.begin, bd.end, bd.ts, rec, rec_stride, first_exp, err);
+            src, src_stride, S, basis, RG, R, bd.begin, bd.end, bd.ts, rec, rec_stride, first_exp, pl.fold, err);
     else  // coefficient basis derived in the kernel
         encode_lut_kernel<kEncChunks, true><<<tiles * RG, kEncThreads, smem, st>>>(
-            src, src_stride, S, nullptr, RG, R, bd.begin, bd.end, bd.ts, rec, rec_stride, first_exp, err);
+            src, src_stride, S, nullptr, RG, R, bd.begin, bd.end, bd.ts, rec, rec_stride, first_exp, pl.fold, err);
     count_launch();
     return cudaGetLastError();
 }
@@ -1418,7 +1465,7 @@ cudaError_t launch_encode_band(const EncodePlan& pl, uint32_t band, const uint8_
 cudaError_t launch_encode(const uint8_t* src, uint64_t src_stride, uint32_t S, const uint16_t* basis,
                           uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec, uint64_t rec_stride,
                           int* err, cudaStream_t st, uint32_t first_exp) {
-    const EncodePlan pl = plan_encode(slice_size, S, RG, false, 0, 0.0);
+    const EncodePlan pl = plan_encode(slice_size, S, RG, false, 0, 0.0, tail_fold(R));
     return launch_encode_band(pl, 0, src, src_stride, S, basis, RG, R, rec, rec_stride, err, st, first_exp);
 }
 
@@ -1650,7 +1697,7 @@ cudaError_t upload_tables_noheap() {
 cudaError_t launch_encode_noheap(const uint8_t* src, uint64_t src_stride, uint32_t S, const uint16_t* basis,
                                  uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec, uint64_t rec_stride,
                                  int* err, cudaStream_t st) {
-    constexpr size_t smem = encode_smem_bytes<kEncChunks>();
+    constexpr size_t smem = encode_smem_bytes<kEncChunks, 4>();
     cudaError_t e = encode_attr();
     if (e != cudaSuccess) return e;
     const uint32_t Np = (uint32_t)(((slice_size + 15) & ~15ull) / 2);
@@ -1658,7 +1705,7 @@ cudaError_t launch_encode_noheap(const uint8_t* src, uint64_t src_stride, uint32
     choose_tiles(Np, RG, (uint32_t)sm_count(), &ts, &tiles);
     if (!R || !tiles) return cudaSuccess;
     encode_lut_kernel<kEncChunks, false><<<tiles * RG, kEncThreads, smem, st>>>(src, src_stride, S, basis, RG, R, 0,
-                                                                                Np, ts, rec, rec_stride, 0, err);
+                                                                                Np, ts, rec, rec_stride, 0, 1, err);
     count_launch();
     return cudaGetLastError();
 }
