@@ -342,7 +342,7 @@ typedef struct p2g_batch p2g_batch;     /* opaque */
 
 typedef struct p2g_batch_info {
     uint32_t jobs, items;
-    uint32_t encode_items, scan_items, finish_items;
+    uint32_t encode_items, scan_items, setid_items;
     uint32_t ctas;                      /* persistent CTAs (one per SM) */
     double predicted_ms;                /* the autotuner's makespan estimate */
     uint64_t device_bytes;              /* scratch the batch holds (bases, tables, queue) */

@@ -597,14 +597,14 @@ class BatchInfo:
     items: int
     encode_items: int
     scan_items: int
-    finish_items: int
+    setid_items: int
     ctas: int
     predicted_ms: float
     device_bytes: int
 
 
 def _batch_info(ci: "_ffi.p2g_batch_info") -> BatchInfo:
-    return BatchInfo(ci.jobs, ci.items, ci.encode_items, ci.scan_items, ci.finish_items, ci.ctas,
+    return BatchInfo(ci.jobs, ci.items, ci.encode_items, ci.scan_items, ci.setid_items, ci.ctas,
                      ci.predicted_ms, ci.device_bytes)
 
 

@@ -162,7 +162,7 @@ class p2g_batch_info(C.Structure):
         ("items", C.c_uint32),
         ("encode_items", C.c_uint32),
         ("scan_items", C.c_uint32),
-        ("finish_items", C.c_uint32),
+        ("setid_items", C.c_uint32),
         ("ctas", C.c_uint32),
         ("predicted_ms", C.c_double),
         ("device_bytes", C.c_uint64),

@@ -63,76 +63,113 @@ inline uint32_t min_tiles(const PlanJob& j) { return (j.Np + kEncTileSymbols - 1
 
 struct Plan {
     std::vector<BatchItem> items;
-    std::vector<uint32_t> enc_items;  // per job
-    uint32_t n_scan = 0, n_enc = 0, n_fin = 0;
+    std::vector<std::vector<uint32_t>> band_items;  // per job: encode items of each band
+    std::vector<uint32_t> band_syms;                // per job
+    uint32_t n_scan = 0, n_enc = 0, n_setid = 0;
     double makespan = 0;
 };
 
-// Items of all jobs in queue order (stable: key descending, then job, then
-// generation order, which is tile-major so a tile's row groups run together
-// and share its source reads in L2).
+constexpr uint32_t kMaxBands = 16;  // packet-MD5 chain segments per job
+
+// Bands of job j: runs of band_tiles consecutive tiles, a multiple of the
+// tail fold so that no folded item straddles two bands.
+void job_bands(const PlanJob& j, uint32_t* band_tiles, uint32_t* n_bands) {
+    const uint32_t F = tail_fold(j.R);
+    uint32_t bt = std::max<uint32_t>(1, (j.tiles + kMaxBands - 1) / kMaxBands);
+    bt = (bt + F - 1) / F * F;
+    *band_tiles = bt;
+    *n_bands = (j.tiles + bt - 1) / bt;
+}
+// one chain segment of every 256-row block over one band's bytes
+inline double chain_ms(const PlanJob& j, uint32_t band_syms) {
+    return ceil(j.R / (double)kChainRows) * md5_ms(2ull * band_syms) + kItemMs;
+}
+
+// Items of all jobs in queue order: every job's set-id item (its chains wait
+// for it), then the scan items, longest first, then the encode items job by
+// job (largest job first), band by band, tile-major within a band so a
+// tile's row groups run together and share its source reads in L2.  A folded
+// item covers the last row group of `fold` adjacent tiles.
 Plan build_items(const std::vector<PlanJob>& jobs) {
-    struct Keyed {
-        double key;
-        uint32_t seq;
-        BatchItem it;
-    };
-    std::vector<Keyed> v;
     Plan p;
-    p.enc_items.assign(jobs.size(), 0);
-    uint32_t seq = 0;
+    p.band_items.resize(jobs.size());
+    p.band_syms.assign(jobs.size(), 0);
+    std::vector<std::pair<double, BatchItem>> pre;
+    struct JobItems {
+        double key;
+        uint32_t job;
+        std::vector<BatchItem> items;
+    };
+    std::vector<JobItems> enc;
     for (uint32_t ji = 0; ji < (uint32_t)jobs.size(); ++ji) {
         const PlanJob& j = jobs[ji];
+        pre.push_back({1e30, {ji, kItemSetId, 0, 0, 0, 0}});
+        p.n_setid++;
         for (uint32_t s = 0; s < j.S; s += kScanSlices) {
             const uint32_t cnt = std::min(kScanSlices, j.S - s);
-            v.push_back({scan_ms(j, cnt), seq++, {ji, kItemScan, s, cnt, 0, 0}});
+            pre.push_back({scan_ms(j, cnt), {ji, kItemScan, s, cnt, 0, 0}});
             p.n_scan++;
         }
-        if (j.R) {
-            for (uint32_t t = 0; t < j.tiles; ++t) {
+        if (!j.R) continue;
+        uint32_t bt = 0, nb = 0;
+        job_bands(j, &bt, &nb);
+        const uint32_t F = tail_fold(j.R);
+        p.band_syms[ji] = bt * j.ts;
+        p.band_items[ji].assign(nb, 0);
+        JobItems e{0.0, ji, {}};
+        for (uint32_t b = 0; b < nb; ++b) {
+            const uint32_t t0 = b * bt, t1 = std::min(j.tiles, t0 + bt);
+            for (uint32_t t = t0; t < t1; ++t) {
                 const uint32_t n0 = t * j.ts, syms = std::min(j.ts, j.Np - n0);
-                const double key = encode_ms(j, syms) + j.finish;
-                for (uint32_t rg = 0; rg < j.RG; ++rg)
-                    v.push_back({key, seq++, {ji, kItemEncode | (rg << 8), n0, syms, 0, 0}});
+                for (uint32_t rg = 0; rg + 1 < j.RG; ++rg) {
+                    e.items.push_back({ji, encode_kind(rg, 1, false), n0, (b << 16) | syms, 0, 0});
+                    e.key += encode_ms(j, syms);
+                    p.band_items[ji][b]++;
+                }
+                if ((t - t0) % F == 0) {
+                    const uint32_t end = std::min(std::min((t + F) * j.ts, t1 * j.ts), j.Np);
+                    e.items.push_back({ji, encode_kind(j.RG - 1, F, false), n0, (b << 16) | (end - n0), 0, 0});
+                    e.key += encode_ms(j, std::min(j.ts, end - n0));
+                    p.band_items[ji][b]++;
+                }
             }
-            p.enc_items[ji] = j.tiles * j.RG;
-            p.n_enc += j.tiles * j.RG;
-        } else {
-            v.push_back({j.finish, seq++, {ji, kItemFinish, 0, 0, 0, 0}});
-            p.n_fin++;
         }
+        e.key += nb * chain_ms(j, p.band_syms[ji]);
+        p.n_enc += (uint32_t)e.items.size();
+        enc.push_back(std::move(e));
     }
-    std::stable_sort(v.begin(), v.end(), [](const Keyed& a, const Keyed& b) {
+    std::stable_sort(pre.begin(), pre.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::stable_sort(enc.begin(), enc.end(), [](const JobItems& a, const JobItems& b) {
         if (a.key != b.key) return a.key > b.key;
-        if (a.it.job != b.it.job) return a.it.job < b.it.job;
-        return a.seq < b.seq;
+        return a.job < b.job;
     });
-    p.items.reserve(v.size());
-    for (const Keyed& k : v) p.items.push_back(k.it);
+    for (auto& x : pre) p.items.push_back(x.second);
+    for (auto& e : enc) p.items.insert(p.items.end(), e.items.begin(), e.items.end());
     return p;
 }
 
 double item_ms(const PlanJob& j, const BatchItem& it) {
     switch (it.kind_rg & kItemKindMask) {
     case kItemScan: return scan_ms(j, it.b);
-    case kItemEncode: return encode_ms(j, it.b);
-    default: return j.finish;
+    case kItemEncode: return encode_ms(j, std::min(j.ts, it.b & 0xFFFFu));
+    default: return est_set_id_ms(j.n);
     }
 }
 
 // List-scheduling simulation: each item goes to the CTA that frees first;
-// the CTA that runs a job's last encode item also runs its finish step.
+// the CTA that completes a band also advances that band's packet chains.
 double simulate(const std::vector<PlanJob>& jobs, const Plan& p, uint32_t ctas) {
     std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
     for (uint32_t c = 0; c < ctas; ++c) free_at.push(0.0);
-    std::vector<uint32_t> left = p.enc_items;
+    std::vector<std::vector<uint32_t>> left = p.band_items;
     double end = 0;
     for (const BatchItem& it : p.items) {
         double t = free_at.top();
         free_at.pop();
         const PlanJob& j = jobs[it.job];
         t += item_ms(j, it);
-        if ((it.kind_rg & kItemKindMask) == kItemEncode && --left[it.job] == 0) t += j.finish;
+        if ((it.kind_rg & kItemKindMask) == kItemEncode && --left[it.job][it.b >> 16] == 0)
+            t += chain_ms(j, p.band_syms[it.job]);
         end = std::max(end, t);
         free_at.push(t);
     }
@@ -151,11 +188,9 @@ Plan plan_batch(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
     if (flags & P2G_BATCH_NO_AUTOTUNE) return best;
     // lower bound at the widest tiles: all work spread evenly over the CTAs
     double total = 0;
-    for (const PlanJob& j : jobs) {
-        total += j.finish;
-        total += ceil((double)j.S / kScanSlices) * scan_ms(j, std::min(j.S, kScanSlices));
-        if (j.R) total += (double)j.tiles * j.RG * encode_ms(j, j.ts);
-    }
+    for (const BatchItem& it : best.items) total += item_ms(jobs[it.job], it);
+    for (uint32_t ji = 0; ji < (uint32_t)jobs.size(); ++ji)
+        total += best.band_items[ji].size() * chain_ms(jobs[ji], best.band_syms[ji]);
     const double bound = total / ctas;
     if (best.makespan <= 1.02 * bound) return best;
     // try finer tilings for the jobs with the longest encode items
@@ -221,7 +256,8 @@ struct p2g_batch {
     size_t arena_bytes = 0;
     p2g::BatchJob* d_jobs = nullptr;
     p2g::BatchItem* d_items = nullptr;
-    uint32_t* d_ctl = nullptr;  // queue head, per-job counters, then the error word
+    uint32_t* d_ctl = nullptr;  // queue head, per-job chain state, then the error word
+    uint64_t err_word = 0;      // index of the error word in d_ctl
     size_t ctl_bytes = 0;
     uint64_t max_basis_words = 0;
     struct Realign {
@@ -241,7 +277,7 @@ namespace p2g {
 namespace {
 
 p2g_status enqueue_run(p2g_batch* b, cudaStream_t st) {
-    int* err = reinterpret_cast<int*>(b->d_ctl + 1 + b->n_jobs);
+    int* err = reinterpret_cast<int*>(b->d_ctl + b->err_word);
     P2G_CU(cudaMemsetAsync(b->d_ctl, 0, b->ctl_bytes, st));
     if (b->max_basis_words) P2G_CU(launch_basis_batch(b->d_jobs, b->n_jobs, b->max_basis_words, st));
     for (const auto& r : b->realigns) P2G_CU(launch_realign(r.src, r.slice, r.dst, r.estride, r.S, r.slice, st));
@@ -264,7 +300,7 @@ void fill_info(const p2g_batch* b, p2g_batch_info* out) {
     out->items = b->n_items;
     out->encode_items = b->plan.n_enc;
     out->scan_items = b->plan.n_scan;
-    out->finish_items = b->plan.n_fin;
+    out->setid_items = b->plan.n_setid;
     out->ctas = b->ctas;
     out->predicted_ms = b->plan.makespan;
     out->device_bytes = b->arena_bytes;
@@ -359,8 +395,24 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
     };
     const size_t o_jobs = take(sizeof(BatchJob) * n);
     const size_t o_items = take(sizeof(BatchItem) * b->n_items);
-    b->ctl_bytes = sizeof(uint32_t) * (1 + n) + sizeof(int);
+    // control block, zeroed before each run: queue head, each job's chain
+    // state (band counts, next band and token per 256-row block, set-id flag),
+    // then the error word
+    std::vector<uint64_t> bstate_off(n);
+    uint64_t ctl_words = 1;
+    for (uint32_t i = 0; i < n; ++i) {
+        bstate_off[i] = ctl_words;
+        const uint32_t Q = (shape[i].R + kChainRows - 1) / kChainRows;
+        ctl_words += b->plan.band_items[i].size() + 2 * Q + 1;
+    }
+    b->err_word = ctl_words;
+    b->ctl_bytes = sizeof(uint32_t) * (ctl_words + 1);
     const size_t o_ctl = take(b->ctl_bytes);
+    std::vector<size_t> o_bands(n), o_chain(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        o_bands[i] = take(4 * std::max<size_t>(1, b->plan.band_items[i].size()));
+        o_chain[i] = take(16ull * std::max(1u, shape[i].R));
+    }
     const size_t o_files = take(16 * total_files);
     const size_t o_noff = take(8 * total_files);
     const size_t o_names = take(names_bytes);
@@ -413,7 +465,12 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         d.name_off = reinterpret_cast<const uint32_t*>(A + o_noff) + 2 * fcur;
         d.names = A + o_names;
         d.scratch = A + o_scratch[i];
-        d.enc_items = b->plan.enc_items[i];
+        d.n_bands = (uint32_t)b->plan.band_items[i].size();
+        d.band_syms = b->plan.band_syms[i];
+        d.ts = shape[i].ts;
+        d.bstate = b->d_ctl + bstate_off[i];
+        d.band_items = reinterpret_cast<const uint32_t*>(A + o_bands[i]);
+        d.chain = reinterpret_cast<uint32_t*>(A + o_chain[i]);
         d.first_exp = 0;
         d.vec = jb.slice_size % 16 == 0 ? 1u : 0u;
         d.basis = load_basis && d.R ? reinterpret_cast<uint16_t*>(A + o_basis[i]) : nullptr;
@@ -440,7 +497,11 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
     auto up = [&](size_t o, const void* src, size_t bytes) {
         return bytes ? cudaMemcpy(A + o, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
     };
-    if ((e = up(o_jobs, hj.data(), sizeof(BatchJob) * n)) != cudaSuccess ||
+    for (uint32_t i = 0; i < n && e == cudaSuccess; ++i)
+        if (!b->plan.band_items[i].empty())
+            e = cudaMemcpy(A + o_bands[i], b->plan.band_items[i].data(), 4 * b->plan.band_items[i].size(),
+                           cudaMemcpyHostToDevice);
+    if (e != cudaSuccess || (e = up(o_jobs, hj.data(), sizeof(BatchJob) * n)) != cudaSuccess ||
         (e = up(o_items, b->plan.items.data(), sizeof(BatchItem) * b->n_items)) != cudaSuccess ||
         (e = up(o_files, hfiles.data(), 8 * hfiles.size())) != cudaSuccess ||
         (e = up(o_noff, hnoff.data(), 4 * hnoff.size())) != cudaSuccess ||
@@ -496,7 +557,7 @@ extern "C" p2g_status p2g_batch_check(p2g_batch* b) {
     if (!b) return set_error(P2G_ERR_INVALID_ARGUMENT, "batch is NULL");
     P2G_CU(cudaSetDevice(b->device));
     int h = 0;
-    P2G_CU(cudaMemcpy(&h, b->d_ctl + 1 + b->n_jobs, sizeof(int), cudaMemcpyDeviceToHost));
+    P2G_CU(cudaMemcpy(&h, b->d_ctl + b->err_word, sizeof(int), cudaMemcpyDeviceToHost));
     if (h) return set_error(P2G_ERR_TIMEOUT, "a bounded device wait gave up in the batch kernel (TMA stage never completed)");
     return P2G_OK;
 }

@@ -127,18 +127,25 @@ inline size_t basis_bytes(uint32_t S, uint32_t RG) { return (size_t)S * RG * 512
 enum BatchItemKind : uint32_t {
     kItemScan = 0,    // slice MD5 + CRC32 of up to kScanSlices slices
     kItemEncode = 1,  // one (row group, symbol tile) of the accumulator
-    kItemFinish = 2,  // hash16k, set id and packet MD5s of a job without encode items
-    kItemSetId = 3,   // hash16k, file ids and set id only
+    kItemSetId = 3,   // hash16k, file ids and set id
     kItemPacket = 4,  // packet MD5s of recovery rows [a, a+b) (set id already written)
 };
 constexpr uint32_t kItemKindMask = 0x7Fu;
 constexpr uint32_t kItemAccumulate = 0x80u;  // encode: XOR partial sums into zeroed rows
 constexpr uint32_t kScanSlices = 256;        // one slice per MD5 lane
+constexpr uint32_t kChainRows = 256;         // recovery rows per packet-MD5 chain token
+
+// Encode item fields: kind_rg = kItemEncode | acc | rg << 8 | log2(fold) << 24;
+// b = band << 16 | symbols.
+inline uint32_t encode_kind(uint32_t rg, uint32_t fold, bool acc) {
+    return kItemEncode | (acc ? kItemAccumulate : 0u) | (rg << 8) | ((fold == 4 ? 2u : fold == 2 ? 1u : 0u) << 24);
+}
 
 struct BatchItem {
     uint32_t job;
-    uint32_t kind_rg;  // kind in bits 0-6 (+ kItemAccumulate), row group in bits 8-31
-    uint32_t a, b;     // scan: first slice, count; encode: first symbol, symbol count;
+    uint32_t kind_rg;  // kind in bits 0-6 (+ kItemAccumulate); encode: row group in bits 8-23,
+                       // log2 fold in bits 24-25
+    uint32_t a, b;     // scan: first slice, count; encode: first symbol, band << 16 | symbols;
                        // packet: first row, row count
     uint32_t s0, sn;   // encode: input slices [s0, s0+sn) (sn == 0: all of the job's)
 };
@@ -159,10 +166,18 @@ struct BatchJob {
     const uint8_t* names;      // display names, each starting 4-byte aligned
     const uint32_t* name_off;  // 2 per file: offset into names, length
     uint8_t* scratch;          // 16*n file ids, then the 12+16*n main-packet body
+    // Recovery-packet MD5 in chain segments: the symbol range is cut into
+    // n_bands bands of band_syms; when the last encode item of a band
+    // completes, the chains of every 256-row block advance over that band's
+    // bytes (n_bands 0: packets are separate items, as in the serving loop).
+    uint32_t* bstate;            // per run, zeroed: [n_bands] items done, [Q] next band, [Q] token, [1] set id ready
+    const uint32_t* band_items;  // [n_bands] encode items per band
+    uint32_t* chain;             // 4 words of MD5 state per recovery row
     uint64_t slice, estride, rec_stride;
     uint32_t S, R, RG, n_files;
-    uint32_t enc_items, first_exp;  // enc_items ~0u: the encode items trigger no finish step
-    uint32_t vec;  // slices and file starts of src are 16-byte aligned
+    uint32_t n_bands, band_syms;
+    uint32_t ts, first_exp;  // ts: tile width (sub-tile width of folded items)
+    uint32_t vec;            // slices and file starts of src are 16-byte aligned
     uint32_t pad;
 };
 

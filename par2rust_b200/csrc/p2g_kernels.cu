@@ -715,7 +715,7 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int PW, bool VEC>
+template <int PW, bool VEC, int UNITS = kRingUnits, int AHEAD = kRingAhead>
 __device__ void md5_range_ring(uint32_t st[4], const uint32_t* pre, const uint8_t* data, uint64_t len,
                                uint64_t b_from, uint64_t b_to, uint32_t ring) {
     constexpr uint32_t pre_bytes = 4 * PW;
@@ -744,7 +744,7 @@ __device__ void md5_range_ring(uint32_t st[4], const uint32_t* pre, const uint8_
         auto fetch = [&](uint64_t u) {  // one unit = one commit group (possibly empty)
             if (u < n_units) {
                 const uint8_t* g = data + 64 * u;
-                const uint32_t d = ring + (uint32_t)(u % kRingUnits) * 64;
+                const uint32_t d = ring + (uint32_t)(u % UNITS) * 64;
                 if (VEC) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) cp_async16(d + 16 * q, g + 16 * q);
@@ -759,16 +759,16 @@ __device__ void md5_range_ring(uint32_t st[4], const uint32_t* pre, const uint8_
         const uint64_t first_w = 16 * b - PW;
         const uint64_t u_lo = first_w / 16;
         const uint64_t u_hi0 = (first_w + 15) / 16;
-        for (uint64_t u = u_lo; u < u_hi0 + kRingAhead; ++u) fetch(u);
+        for (uint64_t u = u_lo; u < u_hi0 + AHEAD; ++u) fetch(u);
         for (; b < fast_end; ++b) {
             const uint64_t u_hi = (16 * b + 15 - PW) / 16;
-            fetch(u_hi + kRingAhead);
-            cp_async_wait<kRingAhead>();
+            fetch(u_hi + AHEAD);
+            cp_async_wait<AHEAD>();
             const uint64_t w0 = (16 * b - PW) & ~3ull;  // aligned quad holding the first word
             uint32_t q[NQ * 4];
 #pragma unroll
             for (int i = 0; i < NQ; ++i) {
-                const uint32_t widx = (uint32_t)((w0 + 4 * i) % (16 * kRingUnits));
+                const uint32_t widx = (uint32_t)((w0 + 4 * i) % (16 * UNITS));
                 const uint4 v = lds128(ring + widx * 4);
                 q[4 * i] = v.x;
                 q[4 * i + 1] = v.y;
@@ -1019,8 +1019,14 @@ __global__ void realign_kernel(const uint8_t* __restrict__ src, uint64_t src_str
 // ring of kRingLaneBytes for each of the kHashThreads MD5 lanes, the CRC32
 // tables and a few words of per-CTA state.
 // ---------------------------------------------------------------------------
-constexpr size_t kBatchEncBytes = encode_smem_bytes<kEncChunks>();
-constexpr size_t kBatchRingBytes = (size_t)kHashThreads * kRingLaneBytes;
+constexpr size_t kBatchEncBytes = encode_smem_bytes<kEncChunks, 4>();
+// The persistent kernel stages MD5 streams through a 4-unit ring (2 units
+// ahead: 1.4 us of chain work, more than an L2 miss) to leave shared memory
+// for an encode stage that holds a folded tail item (4 tiles).
+constexpr int kBatchRingUnits = 4;
+constexpr int kBatchRingAhead = 2;
+constexpr int kBatchRingLane = kBatchRingUnits * 64 + 16;
+constexpr size_t kBatchRingBytes = (size_t)kHashThreads * kBatchRingLane;
 constexpr size_t kBatchSmem = kBatchEncBytes + kBatchRingBytes + 4 * 256 * 4 + 64;
 static_assert(kBatchEncBytes % 16 == 0, "MD5 rings must start 16-byte aligned");
 size_t batch_smem_bytes() { return kBatchSmem; }
@@ -1059,8 +1065,8 @@ __device__ __forceinline__ void batch_scan(const BatchJob& J, uint32_t first, ui
             const uint32_t s = first + tid;
             uint32_t st[4];
             md5_init(st);
-            md5_range_ring<0, VEC>(st, nullptr, J.src + (size_t)s * J.slice, J.slice, 0, ~0ull,
-                                   ring + tid * kRingLaneBytes);
+            md5_range_ring<0, VEC, kBatchRingUnits, kBatchRingAhead>(st, nullptr, J.src + (size_t)s * J.slice,
+                                                                     J.slice, 0, ~0ull, ring + tid * kBatchRingLane);
             store_digest(J.checks[s].md5, st);
         }
     } else {
@@ -1091,8 +1097,9 @@ __device__ void batch_set_id(const BatchJob& J, uint32_t ring, uint32_t* sid) {
             const uint64_t off = J.files[2 * f], len = J.files[2 * f + 1];
             uint32_t h[4];
             md5_init(h);
-            md5_range_ring<0, VEC>(h, nullptr, J.src + off, len < P2G_HASH16K_LEN ? len : P2G_HASH16K_LEN, 0,
-                                   ~0ull, ring + tid * kRingLaneBytes);
+            md5_range_ring<0, VEC, kBatchRingUnits, kBatchRingAhead>(
+                h, nullptr, J.src + off, len < P2G_HASH16K_LEN ? len : P2G_HASH16K_LEN, 0, ~0ull,
+                ring + tid * kBatchRingLane);
             store_digest(J.h16k + 16 * (size_t)f, h);
             const uint32_t pre[6] = {h[0], h[1], h[2], h[3], (uint32_t)len, (uint32_t)(len >> 32)};
             uint32_t id[4];
@@ -1152,21 +1159,119 @@ __device__ void batch_packets(const BatchJob& J, uint32_t ring, const uint32_t* 
                                      0x63696C53u, J.first_exp + r};
             uint32_t st[4];
             md5_init(st);
-            md5_range_ring<9, true>(st, pre, J.rec + (size_t)r * J.rec_stride, J.slice, 0, ~0ull,
-                                    ring + tid * kRingLaneBytes);
+            md5_range_ring<9, true, kBatchRingUnits, kBatchRingAhead>(
+                st, pre, J.rec + (size_t)r * J.rec_stride, J.slice, 0, ~0ull, ring + tid * kBatchRingLane);
             store_digest(J.pkt + 16 * (size_t)r, st);
         }
     }
     __syncthreads();
 }
 
+// Chain segment: rows of block q advance over the message blocks that band b
+// completed (set id ‖ type ‖ exponent ‖ row bytes; the last band also pads
+// and writes the digests).  State between bands lives in J.chain.
+__device__ void advance_rows(const BatchJob& J, uint32_t q, uint32_t b, uint32_t ring, const uint32_t* sid) {
+    const int tid = threadIdx.x;
+    const uint64_t total = 36 + J.slice;
+    const uint64_t nblocks = (total + 8) / 64 + 1;
+    const uint32_t Np = (uint32_t)((J.slice + 15) / 16 * 8);
+    auto done_bytes = [&](uint32_t band) {  // row bytes final once bands 0..band are encoded
+        const uint64_t end = min((uint64_t)Np, (uint64_t)(band + 1) * J.band_syms);
+        return min(J.slice, 2 * end);
+    };
+    const bool final = b + 1 == J.n_bands;
+    const uint64_t from = b == 0 ? 0 : (36 + done_bytes(b - 1)) / 64;
+    const uint64_t to = final ? nblocks : (36 + done_bytes(b)) / 64;
+    const uint32_t r = q * kChainRows + tid;
+    if (tid < (int)kChainRows && r < J.R) {
+        const uint32_t pre[9] = {sid[0], sid[1], sid[2], sid[3], 0x20524150u, 0x00302E32u, 0x76636552u,
+                                 0x63696C53u, J.first_exp + r};
+        uint32_t st[4];
+        if (from == 0) {
+            md5_init(st);
+        } else {
+            const uint4 v = __ldcg(reinterpret_cast<const uint4*>(J.chain) + r);
+            st[0] = v.x;
+            st[1] = v.y;
+            st[2] = v.z;
+            st[3] = v.w;
+        }
+        md5_range_ring<9, true, kBatchRingUnits, kBatchRingAhead>(st, pre, J.rec + (size_t)r * J.rec_stride,
+                                                                  J.slice, from, to, ring + tid * kBatchRingLane);
+        if (final)
+            store_digest(J.pkt + 16 * (size_t)r, st);
+        else
+            __stcg(reinterpret_cast<uint4*>(J.chain) + r, make_uint4(st[0], st[1], st[2], st[3]));
+        __threadfence();  // the next token holder, on another SM, reads this state
+    }
+    __syncthreads();
+}
+
+// Take block q's chain token if it is free and advance its rows over every
+// band that is ready, in order; after releasing the token, look once more
+// (a band that became ready while the token was held was left to us).  Each
+// pass either advances at least one band or returns, so this ends.  No CTA
+// waits for another: a busy token means its holder will see the new band.
+__device__ void try_advance(const BatchJob& J, uint32_t q, uint32_t ring, uint32_t* misc) {
+    const int tid = threadIdx.x;
+    const uint32_t nb = J.n_bands, Q = (J.R + kChainRows - 1) / kChainRows;
+    uint32_t* done = J.bstate;
+    uint32_t* next = done + nb;
+    uint32_t* busy = next + Q;
+    uint32_t* sid_ready = busy + Q;
+    auto ready = [&](uint32_t b) {
+        return b < nb && atomicAdd(sid_ready, 0u) != 0 && atomicAdd(&done[b], 0u) == J.band_items[b];
+    };
+    for (;;) {
+        if (tid == 0) misc[2] = atomicCAS(&busy[q], 0u, 1u) == 0u ? 1u : 0u;
+        __syncthreads();
+        const bool got = misc[2] != 0;
+        __syncthreads();
+        if (!got) return;
+        for (;;) {
+            if (tid == 0) {
+                const uint32_t b = atomicAdd(&next[q], 0u);
+                misc[3] = b;
+                misc[2] = ready(b) ? 1u : 0u;
+            }
+            __syncthreads();
+            const bool ok = misc[2] != 0;
+            const uint32_t b = misc[3];
+            if (ok && tid < 4) misc[4 + tid] = __ldcg(reinterpret_cast<const uint32_t*>(J.set_id) + tid);
+            __syncthreads();
+            if (!ok) break;
+            __threadfence();  // acquire: the band's rows and the set id
+            advance_rows(J, q, b, ring, misc + 4);
+            if (tid == 0) {
+                __threadfence();
+                atomicExch(&next[q], b + 1);
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            __threadfence();
+            atomicExch(&busy[q], 0u);
+            __threadfence();
+            misc[2] = ready(atomicAdd(&next[q], 0u)) ? 1u : 0u;
+        }
+        __syncthreads();
+        const bool again = misc[2] != 0;
+        __syncthreads();
+        if (!again) return;
+    }
+}
+
+__device__ void advance_all(const BatchJob& J, uint32_t ring, uint32_t* misc) {
+    const uint32_t Q = (J.R + kChainRows - 1) / kChainRows;
+    for (uint32_t q = 0; q < Q; ++q) try_advance(J, q, ring, misc);
+}
+
 __global__ void __launch_bounds__(kEncThreads, 1)
     batch_kernel(const BatchJob* __restrict__ jobs, const BatchItem* __restrict__ items, uint32_t n_items,
                  uint32_t* __restrict__ ctl, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smem[];
-    constexpr int NT = (kEncThreads / 32) * kEncChunks * 64;
     uint8_t* enc = smem;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(enc + 2 * kTabBytes + kEncStages * (NT * 2 + 1024));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(enc + encode_bars_offset<kEncChunks, 4>());
     uint8_t* ring_p = smem + kBatchEncBytes;
     uint32_t(*T)[256] = reinterpret_cast<uint32_t(*)[256]>(ring_p + kBatchRingBytes);
     uint32_t* misc = reinterpret_cast<uint32_t*>(ring_p + kBatchRingBytes + 4 * 256 * 4);  // [0] item [1] last [4..7] set id
@@ -1199,6 +1304,14 @@ __global__ void __launch_bounds__(kEncThreads, 1)
                 batch_set_id<true>(J, ring, misc + 4);
             else
                 batch_set_id<false>(J, ring, misc + 4);
+            if (J.n_bands && J.R) {  // chain segments may start
+                if (tid == 0) {
+                    __threadfence();
+                    atomicExch(J.bstate + J.n_bands + 2 * ((J.R + kChainRows - 1) / kChainRows), 1u);
+                }
+                __syncthreads();
+                advance_all(J, ring, misc);
+            }
             continue;
         }
         if (kind == kItemPacket) {
@@ -1209,31 +1322,29 @@ __global__ void __launch_bounds__(kEncThreads, 1)
         }
         if (kind == kItemEncode) {
             // the job's precomputed basis when it has one, else derived per slice
-            const uint32_t rg = it.kind_rg >> 8, sn = it.sn ? it.sn : J.S;
+            const uint32_t rg = (it.kind_rg >> 8) & 0xFFFFu, sn = it.sn ? it.sn : J.S;
+            const uint32_t fold = 1u << ((it.kind_rg >> 24) & 3u);
+            const uint32_t syms = it.b & 0xFFFFu, band = it.b >> 16;
             const bool acc = (it.kind_rg & kItemAccumulate) != 0;
-            const bool ok = J.basis ? encode_tile<kEncChunks, false>(J.esrc, J.estride, sn, J.basis, J.RG, rg, J.R,
-                                                                      it.a, it.b, J.rec, J.rec_stride, enc, phase,
-                                                                      J.first_exp, it.s0, acc)
-                                    : encode_tile<kEncChunks, true>(J.esrc, J.estride, sn, nullptr, J.RG, rg, J.R,
-                                                                     it.a, it.b, J.rec, J.rec_stride, enc, phase,
-                                                                     J.first_exp, it.s0, acc);
+            const bool ok = J.basis ? encode_tile<kEncChunks, false, 4>(J.esrc, J.estride, sn, J.basis, J.RG, rg, J.R,
+                                                                         it.a, syms, J.rec, J.rec_stride, enc, phase,
+                                                                         J.first_exp, it.s0, acc, fold, J.ts)
+                                    : encode_tile<kEncChunks, true, 4>(J.esrc, J.estride, sn, nullptr, J.RG, rg, J.R,
+                                                                        it.a, syms, J.rec, J.rec_stride, enc, phase,
+                                                                        J.first_exp, it.s0, acc, fold, J.ts);
             if (!ok) {
                 if (tid == 0) atomicOr(err, 1);
                 break;
             }
+            if (!J.n_bands) continue;
             __threadfence();  // release this tile's rows before counting it
             __syncthreads();
-            if (tid == 0) misc[1] = (atomicAdd(&ctl[1 + it.job], 1u) + 1 == J.enc_items) ? 1u : 0u;
+            if (tid == 0) misc[1] = (atomicAdd(&J.bstate[band], 1u) + 1 == J.band_items[band]) ? 1u : 0u;
             __syncthreads();
             if (!misc[1]) continue;
-            __threadfence();  // acquire: every tile of the job is visible from here on
+            __threadfence();  // acquire: the whole band is visible from here on
+            advance_all(J, ring, misc);
         }
-        // finish: set id, then every row's packet MD5
-        if (J.vec)
-            batch_set_id<true>(J, ring, misc + 4);
-        else
-            batch_set_id<false>(J, ring, misc + 4);
-        batch_packets(J, ring, misc + 4, 0, J.R);
     }
 }
 

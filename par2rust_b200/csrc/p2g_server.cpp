@@ -162,7 +162,7 @@ void plan_job(p2g_server* s, SJob& j) {
             for (uint32_t c = 0; c < chunks; ++c) {
                 const uint32_t s0 = c * chunk, sn = std::min(chunk, j.S - s0);
                 for (uint32_t rg = 0; rg < j.RG; ++rg) {
-                    j.todo.push_back({j.slot, kItemEncode | acc | (rg << 8), n0, syms, s0, sn});
+                    j.todo.push_back({j.slot, encode_kind(rg, 1, acc != 0), n0, syms, s0, sn});
                     j.todo_ms.push_back(est_encode_item_ms(sn, syms));
                     j.enc_total++;
                 }
@@ -224,7 +224,8 @@ p2g_status admit(p2g_server* s) {
         d.RG = j.RG;
         d.n_files = j.n;
         d.rec_stride = rec_stride;
-        d.enc_items = ~0u;  // packet MD5s run as their own items
+        d.n_bands = 0;  // packet MD5s run as their own items
+        d.ts = std::min<uint32_t>(j.Np, kEncTileSymbols) / 8 * 8;
         d.first_exp = 0;
         d.vec = j.slice % 16 == 0 ? 1u : 0u;
         d.basis = nullptr;  // derived per slice: no basis memory per resident job

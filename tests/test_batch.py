@@ -14,10 +14,25 @@ import pytest
 from par2rust_b200.workloads import file_bytes
 
 
+def _tail_fold(R):
+    tail = R - (R - 1) // 32 * 32
+    return 4 if tail <= 8 else 2 if tail <= 16 else 1
+
+
 def _shape_items(slice_, S, R):
+    """(scan, encode, set-id) item counts at the widest tiles: the last row
+    group is folded over `fold` tiles inside each band of up to 16 bands."""
     Np = (slice_ + 15) // 16 * 16 // 2
     tiles = math.ceil(Np / 2048)
-    return math.ceil(S / 256), (tiles * math.ceil(R / 32) if R else 0), (0 if R else 1)
+    enc = 0
+    if R:
+        F = _tail_fold(R)
+        bt = max(1, math.ceil(tiles / 16))
+        bt = math.ceil(bt / F) * F
+        for t0 in range(0, tiles, bt):
+            n = min(tiles, t0 + bt) - t0
+            enc += n * (math.ceil(R / 32) - 1) + math.ceil(n / F)
+    return math.ceil(S / 256), enc, 1
 
 
 # ---- planner (CPU) -----------------------------------------------------------
@@ -25,9 +40,9 @@ def test_plan_counts_items(p2g):
     shapes = [(4096, 74, 48, 1), (1024, 600, 300, 3), (65536, 4, 0, 1), (1048576, 300, 20, 5), (4100, 10, 7, 2)]
     info, tiles = p2g.batch_plan(shapes, ctas=148, flags=p2g.BATCH_NO_AUTOTUNE)
     scan = sum(_shape_items(sl, S, R)[0] for sl, S, R, _ in shapes)
-    fin = sum(_shape_items(sl, S, R)[2] for sl, S, R, _ in shapes)
-    assert info.scan_items == scan and info.finish_items == fin
-    assert info.items == info.scan_items + info.encode_items + info.finish_items
+    enc = sum(_shape_items(sl, S, R)[1] for sl, S, R, _ in shapes)
+    assert info.scan_items == scan and info.encode_items == enc and info.setid_items == len(shapes)
+    assert info.items == info.scan_items + info.encode_items + info.setid_items
     for (sl, S, R, _), ts in zip(shapes, tiles):
         Np = (sl + 15) // 16 * 16 // 2
         if R == 0:
@@ -152,7 +167,7 @@ def test_batch_matches_oracle(p2g, oracle, gpu, batch_jobs):
     torch.cuda.synchronize()
     b.check()
     info = b.info()
-    assert info.jobs == len(JOB_SET) and info.finish_items == 1
+    assert info.jobs == len(JOB_SET) and info.setid_items == len(JOB_SET)
     for k, (spec, files, host) in enumerate(batch_jobs):
         got = _outputs(spec)
         cks, h16s, sid, rec, pkt = _expected(oracle, files, host, spec.slice_size, spec.recovery_count)
