@@ -48,6 +48,9 @@ struct PlanJob {
     uint32_t S = 0, R = 0, n = 0, RG = 0, Np = 0;
     uint32_t ts = 0, tiles = 0;  // chosen tiling
     double finish = 0;           // finish-step estimate
+    // work the job needs (all by default): slice checksums, the set-id item,
+    // packet-MD5 chains
+    bool scans = true, set_id = true, chains = true;
 };
 
 double finish_ms(const PlanJob& j) { return est_set_id_ms(j.n) + est_packet_item_ms(j.slice, j.R); }
@@ -65,7 +68,7 @@ struct Plan {
     std::vector<BatchItem> items;
     std::vector<std::vector<uint32_t>> band_items;  // per job: encode items of each band
     std::vector<uint32_t> band_syms;                // per job
-    uint32_t n_scan = 0, n_enc = 0, n_setid = 0;
+    uint32_t n_scan = 0, n_crc = 0, n_enc = 0, n_setid = 0;
     double makespan = 0;
 };
 
@@ -86,15 +89,16 @@ inline double chain_ms(const PlanJob& j, uint32_t band_syms) {
 }
 
 // Items of all jobs in queue order: every job's set-id item (its chains wait
-// for it), then the scan items, longest first, then the encode items job by
-// job (largest job first), band by band, tile-major within a band so a
-// tile's row groups run together and share its source reads in L2.  A folded
-// item covers the last row group of `fold` adjacent tiles.
+// for it), then the MD5 scan items, longest first, then the encode items job
+// by job (largest job first), band by band, tile-major within a band so a
+// tile's row groups run together and share its source reads in L2, and last
+// the short CRC items, which fill the ragged final round of the encode.  A
+// folded item covers the last row group of `fold` adjacent tiles.
 Plan build_items(const std::vector<PlanJob>& jobs) {
     Plan p;
     p.band_items.resize(jobs.size());
     p.band_syms.assign(jobs.size(), 0);
-    std::vector<std::pair<double, BatchItem>> pre;
+    std::vector<std::pair<double, BatchItem>> pre, post;
     struct JobItems {
         double key;
         uint32_t job;
@@ -103,12 +107,20 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
     std::vector<JobItems> enc;
     for (uint32_t ji = 0; ji < (uint32_t)jobs.size(); ++ji) {
         const PlanJob& j = jobs[ji];
-        pre.push_back({1e30, {ji, kItemSetId, 0, 0, 0, 0}});
-        p.n_setid++;
-        for (uint32_t s = 0; s < j.S; s += kScanSlices) {
+        if (j.set_id) {
+            pre.push_back({1e30, {ji, kItemSetId, 0, 0, 0, 0}});
+            p.n_setid++;
+        }
+        for (uint32_t s = 0; j.scans && s < j.S; s += kScanSlices) {
             const uint32_t cnt = std::min(kScanSlices, j.S - s);
             pre.push_back({scan_ms(j, cnt), {ji, kItemScan, s, cnt, 0, 0}});
             p.n_scan++;
+        }
+        const uint32_t cper = crc_item_slices(j.slice);
+        for (uint32_t s = 0; j.scans && s < j.S; s += cper) {
+            const uint32_t cnt = std::min(cper, j.S - s);
+            post.push_back({est_crc_item_ms(j.slice, cnt), {ji, kItemCrc, s, cnt, 0, 0}});
+            p.n_crc++;
         }
         if (!j.R) continue;
         uint32_t bt = 0, nb = 0;
@@ -116,6 +128,7 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
         const uint32_t F = tail_fold(j.R);
         p.band_syms[ji] = bt * j.ts;
         p.band_items[ji].assign(nb, 0);
+        std::vector<uint32_t>& counts = p.band_items[ji];
         JobItems e{0.0, ji, {}};
         for (uint32_t b = 0; b < nb; ++b) {
             const uint32_t t0 = b * bt, t1 = std::min(j.tiles, t0 + bt);
@@ -124,17 +137,22 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
                 for (uint32_t rg = 0; rg + 1 < j.RG; ++rg) {
                     e.items.push_back({ji, encode_kind(rg, 1, false), n0, (b << 16) | syms, 0, 0});
                     e.key += encode_ms(j, syms);
-                    p.band_items[ji][b]++;
+                    counts[b]++;
                 }
                 if ((t - t0) % F == 0) {
                     const uint32_t end = std::min(std::min((t + F) * j.ts, t1 * j.ts), j.Np);
                     e.items.push_back({ji, encode_kind(j.RG - 1, F, false), n0, (b << 16) | (end - n0), 0, 0});
                     e.key += encode_ms(j, std::min(j.ts, end - n0));
-                    p.band_items[ji][b]++;
+                    counts[b]++;
                 }
             }
         }
-        e.key += nb * chain_ms(j, p.band_syms[ji]);
+        if (j.chains) {
+            e.key += nb * chain_ms(j, p.band_syms[ji]);
+        } else {  // no chain segments: the encode items count nothing
+            counts.clear();
+            p.band_syms[ji] = 0;
+        }
         p.n_enc += (uint32_t)e.items.size();
         enc.push_back(std::move(e));
     }
@@ -143,14 +161,17 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
         if (a.key != b.key) return a.key > b.key;
         return a.job < b.job;
     });
+    std::stable_sort(post.begin(), post.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
     for (auto& x : pre) p.items.push_back(x.second);
     for (auto& e : enc) p.items.insert(p.items.end(), e.items.begin(), e.items.end());
+    for (auto& x : post) p.items.push_back(x.second);
     return p;
 }
 
 double item_ms(const PlanJob& j, const BatchItem& it) {
     switch (it.kind_rg & kItemKindMask) {
     case kItemScan: return scan_ms(j, it.b);
+    case kItemCrc: return est_crc_item_ms(j.slice, it.b);
     case kItemEncode: return encode_ms(j, std::min(j.ts, it.b & 0xFFFFu));
     default: return est_set_id_ms(j.n);
     }
@@ -168,7 +189,8 @@ double simulate(const std::vector<PlanJob>& jobs, const Plan& p, uint32_t ctas) 
         free_at.pop();
         const PlanJob& j = jobs[it.job];
         t += item_ms(j, it);
-        if ((it.kind_rg & kItemKindMask) == kItemEncode && --left[it.job][it.b >> 16] == 0)
+        if ((it.kind_rg & kItemKindMask) == kItemEncode && !left[it.job].empty() &&
+            --left[it.job][it.b >> 16] == 0)
             t += chain_ms(j, p.band_syms[it.job]);
         end = std::max(end, t);
         free_at.push(t);
@@ -182,6 +204,17 @@ Plan plan_batch(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
         j.Np = (uint32_t)(round_up(j.slice, 16) / 2);
         j.finish = finish_ms(j);
         set_tiling(j, min_tiles(j));
+        if (jobs.size() == 1 && j.R && !(flags & P2G_BATCH_NO_AUTOTUNE)) {
+            // alone on the GPU, equal items run in rounds of the CTAs that
+            // the (long) MD5 scan items leave free: take the tile count with
+            // the fewest, fullest rounds (choose_tiles)
+            const uint32_t scans = j.scans ? (j.S + kScanSlices - 1) / kScanSlices : 0;
+            const uint32_t free_ctas = ctas > scans + 16 ? ctas - scans : ctas;
+            uint32_t ts = 0, tiles = 0;
+            choose_tiles(j.Np, j.RG, free_ctas, &ts, &tiles, tail_fold(j.R));
+            j.ts = ts;
+            j.tiles = tiles;
+        }
     }
     Plan best = build_items(jobs);
     best.makespan = simulate(jobs, best, ctas);
@@ -229,17 +262,37 @@ double est_encode_item_ms(uint32_t slices, uint32_t syms) {
     return (double)slices * (round_up(syms, 8) + kBuildCost) / kEncRate + kItemMs;
 }
 double est_scan_item_ms(uint64_t slice, uint32_t count) {
-    // MD5 lanes run in parallel; the CRC warps take count/8 slices each at
-    // about 6 shared loads per 4 bytes per lane, mostly hidden behind them
-    const double crc = ceil(count / 8.0) * (double)slice / 128.0 * 6.0 / 1.9e6;
-    return std::max(md5_ms(slice), crc) + kItemMs;
+    (void)count;  // the lanes run their chains side by side
+    return md5_ms(slice) + kItemMs;
 }
+// CRC32 streams from DRAM at ~8 GB/s per SM (16 warps)
+double est_crc_item_ms(uint64_t slice, uint32_t count) { return (double)slice * count / 8e6 + kItemMs; }
 double est_set_id_ms(uint32_t files) {
     const double hashes = ceil(files / 256.0) * (md5_ms(P2G_HASH16K_LEN) + md5_ms(24 + 256));
     const double sort = (double)files * files / 512.0 * 4e-6;
     return hashes + sort + md5_ms(12 + 16ull * files) + kItemMs;
 }
 double est_packet_item_ms(uint64_t slice, uint32_t rows) { return ceil(rows / 256.0) * md5_ms(36 + slice) + kItemMs; }
+
+SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans, bool set_id,
+                              bool chains, uint32_t ctas) {
+    std::vector<PlanJob> jobs(1);
+    jobs[0].slice = slice;
+    jobs[0].S = S;
+    jobs[0].R = R;
+    jobs[0].n = std::max(1u, n_files);
+    jobs[0].scans = scans;
+    jobs[0].set_id = set_id;
+    jobs[0].chains = chains && R;
+    Plan p = plan_batch(jobs, ctas, 0);
+    SingleJobPlan out;
+    out.items = std::move(p.items);
+    out.band_items = p.band_items[0];
+    out.band_syms = p.band_syms[0];
+    out.ts = jobs[0].ts;
+    out.predicted_ms = p.makespan;
+    return out;
+}
 
 // ---------------------------------------------------------------------------
 // The batch object
@@ -299,7 +352,7 @@ void fill_info(const p2g_batch* b, p2g_batch_info* out) {
     out->jobs = b->n_jobs;
     out->items = b->n_items;
     out->encode_items = b->plan.n_enc;
-    out->scan_items = b->plan.n_scan;
+    out->scan_items = b->plan.n_scan + b->plan.n_crc;
     out->setid_items = b->plan.n_setid;
     out->ctas = b->ctas;
     out->predicted_ms = b->plan.makespan;

@@ -87,7 +87,8 @@ struct Context {
     cudaStream_t st[kStreams] = {};
     cudaEvent_t ev_fork = nullptr, ev_h16k = nullptr, ev_join[kStreams] = {}, ev_band[kBandEvents] = {};
     DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out, md5_state;
-    PinBuf h_spans, h_h16k, h_err, h_stage;
+    DevBuf persist;    // single-job persistent run: descriptor, items, chain state, tables
+    PinBuf h_spans, h_h16k, h_err, h_stage, h_persist;
 };
 static Context& ctx() {
     static Context* c = new Context();  // never destroyed: the CUDA runtime may be gone at exit
@@ -277,7 +278,135 @@ struct DeviceJob {
     bool have_set_id = false;
 };
 
+// The device job through the persistent kernel (p2g_kernels.cu, batch_kernel)
+// with this one job: slice MD5/CRC32 scan items and the set-id item first,
+// then encode items band by band (folded tail, tiles sized to whole rounds of
+// the SMs); each band's completion advances the recovery-packet MD5 chains.
+// Items are dynamic and SM-exclusive, so the banded path's one-wave bands
+// and its hash kernels sharing SMs with encode CTAs do not arise.
+static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream_t st) {
+    const uint32_t n = (uint32_t)j.files.size();
+    const uint32_t RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
+    const bool chains = j.R && j.S && j.d_pkt;
+    const bool sid_item = !j.have_set_id;
+    const SingleJobPlan pl = plan_single_job(j.slice, j.S, j.R && j.S ? j.R : 0, n, j.d_checks != nullptr, sid_item,
+                                             chains, (uint32_t)device_sm_count());
+    const uint32_t nb = (uint32_t)pl.band_items.size();
+    const uint32_t Q = (j.R + kChainRows - 1) / kChainRows;
+    const uint64_t ctl_words = 1 + (chains ? nb + 2 * Q + 1 : 0) + 1;  // head, chain state, error word
+    uint64_t names_bytes = 0;
+    for (const auto& f : j.files) names_bytes += round_up(f.name_len, 4);
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        const size_t o = off;
+        off = round_up(off + std::max<size_t>(b, 1), 256);
+        return o;
+    };
+    const size_t o_desc = take(sizeof(BatchJob)), o_items = take(sizeof(BatchItem) * pl.items.size());
+    const size_t o_ctl = take(4 * ctl_words), o_bands = take(4 * nb), o_chain = take(16ull * j.R);
+    const size_t o_files = take(16ull * n), o_noff = take(8ull * n), o_names = take(names_bytes);
+    const size_t o_scratch = take(32ull * n + 12), o_sid = take(16);
+    const size_t host_bytes = o_ctl;  // descriptor and items staged together
+    P2G_CU(c.persist.ensure(off));
+    P2G_CU(cudaStreamSynchronize(st));  // the staging buffer may still feed the previous call's copies
+    P2G_CU(c.h_persist.ensure(off));
+    uint8_t* D = c.persist.as<uint8_t>();
+    uint8_t* H = c.h_persist.as<uint8_t>();
+    // basis (precomputed unless P2G_ENCODE_BASIS=derive) and 16-byte aligned slices
+    const bool gen = generate_basis();
+    if (j.R && j.S && !gen) P2G_CU(c.basis.ensure(basis_bytes(j.S, RG)));
+    const uint8_t* esrc = j.d_src;
+    uint64_t estride = j.slice;
+    if (j.R && j.S && j.slice % 16) {
+        estride = round_up(j.slice, 16);
+        P2G_CU(c.src_al.ensure((size_t)estride * j.S));
+        esrc = c.src_al.as<uint8_t>();
+    }
+    BatchJob& d = *reinterpret_cast<BatchJob*>(H + o_desc);
+    memset(&d, 0, sizeof d);
+    d.src = j.d_src;
+    d.esrc = esrc;
+    d.basis = j.R && j.S && !gen ? c.basis.as<uint16_t>() : nullptr;
+    d.rec = j.d_rec;
+    d.checks = j.d_checks;
+    d.h16k = j.d_h16k;
+    d.pkt = j.d_pkt;
+    d.set_id = D + o_sid;
+    d.files = reinterpret_cast<const uint64_t*>(D + o_files);
+    d.names = D + o_names;
+    d.name_off = reinterpret_cast<const uint32_t*>(D + o_noff);
+    d.scratch = D + o_scratch;
+    d.bstate = chains ? reinterpret_cast<uint32_t*>(D + o_ctl) + 1 : nullptr;
+    d.band_items = reinterpret_cast<const uint32_t*>(D + o_bands);
+    d.chain = reinterpret_cast<uint32_t*>(D + o_chain);
+    d.slice = j.slice;
+    d.estride = estride;
+    d.rec_stride = j.rec_stride;
+    d.S = j.S;
+    d.R = j.S ? j.R : 0;
+    d.RG = RG;
+    d.n_files = n;
+    d.n_bands = chains ? nb : 0;
+    d.band_syms = pl.band_syms;
+    d.ts = pl.ts;
+    d.first_exp = j.first_exp;
+    d.vec = j.slice % 16 == 0 ? 1u : 0u;
+    memcpy(H + o_items, pl.items.data(), sizeof(BatchItem) * pl.items.size());
+    uint8_t* hb = H + o_ctl;  // band counts, file tables and names after the descriptor and items
+    memcpy(hb + (o_bands - o_ctl), pl.band_items.data(), 4 * nb);
+    uint64_t* hf = reinterpret_cast<uint64_t*>(hb + (o_files - o_ctl));
+    uint32_t* hn = reinterpret_cast<uint32_t*>(hb + (o_noff - o_ctl));
+    uint8_t* hs = hb + (o_names - o_ctl);
+    uint64_t noff = 0;
+    for (uint32_t f = 0; f < n; ++f) {
+        hf[2 * f] = j.files[f].first_slice * j.slice;
+        hf[2 * f + 1] = j.files[f].length;
+        hn[2 * f] = (uint32_t)noff;
+        hn[2 * f + 1] = (uint32_t)j.files[f].name_len;
+        memcpy(hs + noff, j.files[f].name, j.files[f].name_len);
+        noff += round_up(j.files[f].name_len, 4);
+    }
+    if (j.have_set_id) memcpy(H + o_sid, j.set_id.data(), 16);
+    int* err = reinterpret_cast<int*>(D + o_ctl) + (ctl_words - 1);
+    P2G_CU(cudaMemcpyAsync(D, H, host_bytes, cudaMemcpyHostToDevice, st));  // descriptor + items
+    P2G_CU(cudaMemsetAsync(D + o_ctl, 0, 4 * ctl_words, st));
+    P2G_CU(cudaMemcpyAsync(D + o_bands, H + o_bands, o_sid - o_bands, cudaMemcpyHostToDevice, st));
+    if (j.have_set_id) {
+        P2G_CU(cudaMemcpyAsync(D + o_sid, H + o_sid, 16, cudaMemcpyHostToDevice, st));
+        if (chains) {  // the set id is given: chain segments may start at once
+            static const uint32_t one = 1;
+            P2G_CU(cudaMemcpyAsync(reinterpret_cast<uint32_t*>(D + o_ctl) + 1 + nb + 2 * Q, &one, 4,
+                                   cudaMemcpyHostToDevice, st));
+        }
+    }
+    if (d.basis) P2G_CU(launch_basis(c.basis.as<uint16_t>(), j.S, RG, j.R, j.first_exp, st));
+    if (esrc != j.d_src) P2G_CU(launch_realign(j.d_src, j.slice, c.src_al.as<uint8_t>(), estride, j.S, j.slice, st));
+    P2G_CU(launch_batch(reinterpret_cast<const BatchJob*>(D + o_desc), reinterpret_cast<const BatchItem*>(D + o_items),
+                        (uint32_t)pl.items.size(), reinterpret_cast<uint32_t*>(D + o_ctl), err,
+                        (uint32_t)device_sm_count(), st));
+    P2G_CU(cudaMemcpyAsync(c.h_err.p, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (!j.have_set_id) {
+        // set id = MD5(main packet body) over the sorted file ids
+        // (src/source.rs:303-309, src/packet/main_packet.rs:25-42); the
+        // device derived the same value for the packet MD5s
+        P2G_CU(c.h_h16k.ensure(16 * (size_t)n));
+        P2G_CU(cudaMemcpyAsync(c.h_h16k.p, j.d_h16k, 16 * n, cudaMemcpyDeviceToHost, st));
+        P2G_CU(cudaStreamSynchronize(st));
+        j.h16k.resize(n);
+        j.file_ids.resize(n);
+        for (uint32_t f = 0; f < n; ++f) {
+            memcpy(j.h16k[f].data(), c.h_h16k.as<uint8_t>() + 16 * f, 16);
+            j.file_ids[f] = file_id_of(j.h16k[f].data(), j.files[f].length, j.files[f].name, j.files[f].name_len);
+        }
+        std::vector<uint8_t> mp;
+        j.set_id = build_main_packet(j.slice, j.file_ids, mp);
+    }
+    return P2G_OK;
+}
+
 static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) {
+    // whole-file MD5 on the device stays with the multi-stream pipeline below
+    if (!j.d_hfull && !getenv("P2G_BANDED")) return run_device_job_persistent(c, j, caller);
     const uint32_t n = (uint32_t)j.files.size();
     const uint32_t RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
     P2G_TRY(fork_from(c, caller));

@@ -125,11 +125,13 @@ inline size_t basis_bytes(uint32_t S, uint32_t RG) { return (size_t)S * RG * 512
 // persistent launch, one CTA per SM popping items off a device queue.
 // ---------------------------------------------------------------------------
 enum BatchItemKind : uint32_t {
-    kItemScan = 0,    // slice MD5 + CRC32 of up to kScanSlices slices
+    kItemScan = 0,    // slice MD5 of up to kScanSlices slices
     kItemEncode = 1,  // one (row group, symbol tile) of the accumulator
     kItemSetId = 3,   // hash16k, file ids and set id
     kItemPacket = 4,  // packet MD5s of recovery rows [a, a+b) (set id already written)
+    kItemCrc = 5,     // slice CRC32 of slices [a, a+b)
 };
+constexpr uint64_t kCrcItemBytes = 4u << 20;  // source bytes per CRC item
 constexpr uint32_t kItemKindMask = 0x7Fu;
 constexpr uint32_t kItemAccumulate = 0x80u;  // encode: XOR partial sums into zeroed rows
 constexpr uint32_t kScanSlices = 256;        // one slice per MD5 lane
@@ -181,6 +183,16 @@ struct BatchJob {
     uint32_t pad;
 };
 
+// Items of one job run alone through the persistent kernel (the plain
+// device-job path): scans / set-id item / packet-MD5 chains as requested.
+struct SingleJobPlan {
+    std::vector<BatchItem> items;    // job index 0
+    std::vector<uint32_t> band_items;  // empty: no chains
+    uint32_t band_syms = 0, ts = 0;
+    double predicted_ms = 0;
+};
+SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans, bool set_id,
+                              bool chains, uint32_t ctas);
 // Shared memory of one batch CTA.
 size_t batch_smem_bytes();
 // Fills every job's basis (one launch; blockIdx.y = job).
@@ -196,6 +208,12 @@ cudaError_t launch_seeded_fill(uint8_t* base, const uint64_t* spans, const uint6
 double est_md5_ms(uint64_t bytes);
 double est_encode_item_ms(uint32_t slices, uint32_t syms);
 double est_scan_item_ms(uint64_t slice, uint32_t count);
+double est_crc_item_ms(uint64_t slice, uint32_t count);
+// slices per CRC item: ~kCrcItemBytes, at least 1, at most kScanSlices
+inline uint32_t crc_item_slices(uint64_t slice) {
+    const uint64_t n = kCrcItemBytes / slice;
+    return (uint32_t)(n < 1 ? 1 : n > kScanSlices ? kScanSlices : n);
+}
 double est_set_id_ms(uint32_t files);
 double est_packet_item_ms(uint64_t slice, uint32_t rows);
 // Sets the batch kernel's shared-memory attribute (call before stream capture).

@@ -1020,11 +1020,11 @@ __global__ void realign_kernel(const uint8_t* __restrict__ src, uint64_t src_str
 // tables and a few words of per-CTA state.
 // ---------------------------------------------------------------------------
 constexpr size_t kBatchEncBytes = encode_smem_bytes<kEncChunks, 4>();
-// The persistent kernel stages MD5 streams through a 4-unit ring (2 units
-// ahead: 1.4 us of chain work, more than an L2 miss) to leave shared memory
-// for an encode stage that holds a folded tail item (4 tiles).
-constexpr int kBatchRingUnits = 4;
-constexpr int kBatchRingAhead = 2;
+// The persistent kernel stages MD5 streams through a 5-unit ring (3 units
+// ahead: ~2 us of chain work, more than a DRAM miss under load), the most
+// that fits beside an encode stage holding a folded tail item (4 tiles).
+constexpr int kBatchRingUnits = 5;
+constexpr int kBatchRingAhead = 3;
 constexpr int kBatchRingLane = kBatchRingUnits * 64 + 16;
 constexpr size_t kBatchRingBytes = (size_t)kHashThreads * kBatchRingLane;
 constexpr size_t kBatchSmem = kBatchEncBytes + kBatchRingBytes + 4 * 256 * 4 + 64;
@@ -1053,31 +1053,34 @@ __device__ __forceinline__ bool id_eq(const uint4& a, const uint4& b) {
     return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w;
 }
 
-// Slices [first, first+count) of job J: MD5 on the kHashThreads lanes (one
-// slice each, staged through the lane's ring), CRC32 on the remaining warps
-// (one slice per warp at a time).
+// Slice MD5 of slices [first, first+count) of job J on the kHashThreads
+// lanes (one slice each, staged through the lane's ring).  The other warps
+// idle: the lanes are bound by their chains, and the SM is the item's alone.
 template <bool VEC>
-__device__ __forceinline__ void batch_scan(const BatchJob& J, uint32_t first, uint32_t count, uint32_t ring,
-                                           const uint32_t (*T)[256]) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid < kHashThreads) {
-        if ((uint32_t)tid < count) {
-            const uint32_t s = first + tid;
-            uint32_t st[4];
-            md5_init(st);
-            md5_range_ring<0, VEC, kBatchRingUnits, kBatchRingAhead>(st, nullptr, J.src + (size_t)s * J.slice,
-                                                                     J.slice, 0, ~0ull, ring + tid * kBatchRingLane);
-            store_digest(J.checks[s].md5, st);
-        }
-    } else {
-        constexpr uint32_t kCrcWarps = (kEncThreads - kHashThreads) / 32;
-        const CrcLane cl = crc_lane<VEC>(J.slice, lane);
-        for (uint32_t i = (uint32_t)warp - kHashThreads / 32; i < count; i += kCrcWarps) {
-            const uint32_t s = first + i;
-            const uint32_t c =
-                crc_slice_warp<VEC>(reinterpret_cast<const uint32_t*>(J.src + (size_t)s * J.slice), cl, lane, T);
-            if (lane == 0) J.checks[s].crc32 = c;
-        }
+__device__ __forceinline__ void batch_scan(const BatchJob& J, uint32_t first, uint32_t count, uint32_t ring) {
+    const int tid = threadIdx.x;
+    if (tid < kHashThreads && (uint32_t)tid < count) {
+        const uint32_t s = first + tid;
+        uint32_t st[4];
+        md5_init(st);
+        md5_range_ring<0, VEC, kBatchRingUnits, kBatchRingAhead>(st, nullptr, J.src + (size_t)s * J.slice, J.slice,
+                                                                 0, ~0ull, ring + tid * kBatchRingLane);
+        store_digest(J.checks[s].md5, st);
+    }
+}
+
+// Slice CRC32 of slices [first, first+count): one slice per warp at a time
+// over all 16 warps (CRC streams from DRAM; its items are a few MB each so
+// the work spreads over many SMs).
+template <bool VEC>
+__device__ __forceinline__ void batch_crc(const BatchJob& J, uint32_t first, uint32_t count,
+                                          const uint32_t (*T)[256]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const CrcLane cl = crc_lane<VEC>(J.slice, lane);
+    for (uint32_t i = (uint32_t)warp; i < count; i += kEncThreads / 32) {
+        const uint32_t s = first + i;
+        const uint32_t c = crc_slice_warp<VEC>(reinterpret_cast<const uint32_t*>(J.src + (size_t)s * J.slice), cl, lane, T);
+        if (lane == 0) J.checks[s].crc32 = c;
     }
 }
 
@@ -1293,9 +1296,17 @@ __global__ void __launch_bounds__(kEncThreads, 1)
         const uint32_t kind = it.kind_rg & kItemKindMask;
         if (kind == kItemScan) {
             if (J.vec)
-                batch_scan<true>(J, it.a, it.b, ring, T);
+                batch_scan<true>(J, it.a, it.b, ring);
             else
-                batch_scan<false>(J, it.a, it.b, ring, T);
+                batch_scan<false>(J, it.a, it.b, ring);
+            __syncthreads();
+            continue;
+        }
+        if (kind == kItemCrc) {
+            if (J.vec)
+                batch_crc<true>(J, it.a, it.b, T);
+            else
+                batch_crc<false>(J, it.a, it.b, T);
             __syncthreads();
             continue;
         }
@@ -1379,8 +1390,11 @@ __global__ void seeded_fill_kernel(uint8_t* __restrict__ base, const uint64_t* _
 __global__ void basis_batch_kernel(const BatchJob* __restrict__ jobs) {
     const BatchJob& J = jobs[blockIdx.y];
     if (!J.R || !J.basis) return;
+    // the last row group replicated as the folded encode items build it (tail_fold)
+    const uint32_t tail = J.R - (J.R - 1) / kRowsPerGroup * kRowsPerGroup;
+    const uint32_t fold = tail <= 8 ? 4u : tail <= 16 ? 2u : 1u;
     basis_fill(J.basis, J.S, J.RG, J.R, J.first_exp, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
-               (uint64_t)gridDim.x * blockDim.x);
+               (uint64_t)gridDim.x * blockDim.x, fold);
 }
 
 // ---------------------------------------------------------------------------

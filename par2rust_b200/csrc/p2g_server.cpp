@@ -153,6 +153,13 @@ void plan_job(p2g_server* s, SJob& j) {
         j.todo_ms.push_back(est_scan_item_ms(j.slice, cnt));
         j.scan_total++;
     }
+    const uint32_t cper = crc_item_slices(j.slice);
+    for (uint32_t a = 0; a < j.S; a += cper) {
+        const uint32_t cnt = std::min(cper, j.S - a);
+        j.todo.push_back({j.slot, kItemCrc, a, cnt, 0, 0});
+        j.todo_ms.push_back(est_crc_item_ms(j.slice, cnt));
+        j.scan_total++;
+    }
     j.todo.push_back({j.slot, kItemSetId, 0, 0, 0, 0});
     j.todo_ms.push_back(est_set_id_ms(j.n));
     if (j.R) {
@@ -297,7 +304,8 @@ p2g_status retire(p2g_server* s, bool block) {
                 continue;
             }
             switch (it.kind_rg & kItemKindMask) {
-            case kItemScan: j->scan_done++; break;
+            case kItemScan:
+            case kItemCrc: j->scan_done++; break;
             case kItemSetId: j->setid_done = true; break;
             case kItemEncode: j->enc_done++; break;
             case kItemPacket: j->pkt_done += it.b; break;
@@ -376,6 +384,7 @@ p2g_status launch_wave(p2g_server* s, bool* launched) {
         const uint32_t k = it.kind_rg & kItemKindMask;
         const double ms = k == kItemEncode ? est_encode_item_ms(it.sn, it.b)
                           : k == kItemScan ? est_scan_item_ms(j->slice, it.b)
+                          : k == kItemCrc ? est_crc_item_ms(j->slice, it.b)
                           : k == kItemSetId ? est_set_id_ms(j->n)
                                             : est_packet_item_ms(j->slice, it.b);
         order.push_back({ms, it});

@@ -20,8 +20,8 @@ def _tail_fold(R):
 
 
 def _shape_items(slice_, S, R):
-    """(scan, encode, set-id) item counts at the widest tiles: the last row
-    group is folded over `fold` tiles inside each band of up to 16 bands."""
+    """(scan + CRC, encode, set-id) item counts at the widest tiles: the last
+    row group is folded over `fold` tiles inside each band of up to 16 bands."""
     Np = (slice_ + 15) // 16 * 16 // 2
     tiles = math.ceil(Np / 2048)
     enc = 0
@@ -32,7 +32,8 @@ def _shape_items(slice_, S, R):
         for t0 in range(0, tiles, bt):
             n = min(tiles, t0 + bt) - t0
             enc += n * (math.ceil(R / 32) - 1) + math.ceil(n / F)
-    return math.ceil(S / 256), enc, 1
+    crc_per_item = min(256, max(1, (4 << 20) // slice_))  # CRC items of ~4 MiB
+    return math.ceil(S / 256) + math.ceil(S / crc_per_item), enc, 1
 
 
 # ---- planner (CPU) -----------------------------------------------------------
@@ -69,7 +70,7 @@ def test_plan_large_batch_is_near_its_bound(p2g):
     jobs = W.batch_256()
     shapes = [(j.slice_size, j.slices, j.recovery, len(j.file_lengths)) for j in jobs]
     info, tiles = p2g.batch_plan(shapes, ctas=148)
-    assert info.jobs == 256 and info.scan_items == sum(math.ceil(j.slices / 256) for j in jobs)
+    assert info.jobs == 256 and info.scan_items == sum(_shape_items(j.slice_size, j.slices, j.recovery)[0] for j in jobs)
     # the mixed batch has ~43 SM-seconds of encode work: ~290 ms on 148 SMs
     assert 250 < info.predicted_ms < 400
 
