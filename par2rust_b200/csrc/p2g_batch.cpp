@@ -72,7 +72,7 @@ struct Plan {
     double makespan = 0;
 };
 
-constexpr uint32_t kMaxBands = 16;  // packet-MD5 chain segments per job
+constexpr uint32_t kMaxBands = 64;  // packet-MD5 chain segments per job (64: 10.27 ms vs 10.59 at 16 for 538 MB / R 200)
 
 // Bands of job j: runs of band_tiles consecutive tiles, a multiple of the
 // tail fold so that no folded item straddles two bands.

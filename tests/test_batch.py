@@ -21,13 +21,13 @@ def _tail_fold(R):
 
 def _shape_items(slice_, S, R):
     """(scan + CRC, encode, set-id) item counts at the widest tiles: the last
-    row group is folded over `fold` tiles inside each band of up to 16 bands."""
+    row group is folded over `fold` tiles inside each band of up to 64 bands."""
     Np = (slice_ + 15) // 16 * 16 // 2
     tiles = math.ceil(Np / 2048)
     enc = 0
     if R:
         F = _tail_fold(R)
-        bt = max(1, math.ceil(tiles / 16))
+        bt = max(1, math.ceil(tiles / 64))
         bt = math.ceil(bt / F) * F
         for t0 in range(0, tiles, bt):
             n = min(tiles, t0 + bt) - t0
