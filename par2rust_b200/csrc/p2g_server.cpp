@@ -163,13 +163,20 @@ void plan_job(p2g_server* s, SJob& j) {
     j.todo.push_back({j.slot, kItemSetId, 0, 0, 0, 0});
     j.todo_ms.push_back(est_set_id_ms(j.n));
     if (j.R) {
-        const uint32_t acc = chunks > 1 ? kItemAccumulate : 0u;
+        const bool acc = chunks > 1;
+        const uint32_t F = tail_fold(j.R);  // the last row group covers F tiles per item
         for (uint32_t t = 0; t < tiles; ++t) {
             const uint32_t n0 = t * ts, syms = std::min(ts, j.Np - n0);
             for (uint32_t c = 0; c < chunks; ++c) {
                 const uint32_t s0 = c * chunk, sn = std::min(chunk, j.S - s0);
                 for (uint32_t rg = 0; rg < j.RG; ++rg) {
-                    j.todo.push_back({j.slot, encode_kind(rg, 1, acc != 0), n0, syms, s0, sn});
+                    uint32_t fold = 1, n = syms;
+                    if (rg + 1 == j.RG && F > 1) {
+                        if (t % F) continue;  // covered by the folded item of tile t - t % F
+                        fold = F;
+                        n = std::min((t + F) * ts, j.Np) - n0;
+                    }
+                    j.todo.push_back({j.slot, encode_kind(rg, fold, acc), n0, n, s0, sn});
                     j.todo_ms.push_back(est_encode_item_ms(sn, syms));
                     j.enc_total++;
                 }
@@ -382,7 +389,7 @@ p2g_status launch_wave(p2g_server* s, bool* launched) {
     order.reserve(w.items.size());
     for (auto& [j, it] : w.items) {
         const uint32_t k = it.kind_rg & kItemKindMask;
-        const double ms = k == kItemEncode ? est_encode_item_ms(it.sn, it.b)
+        const double ms = k == kItemEncode ? est_encode_item_ms(it.sn, std::min(it.b & 0xFFFFu, j->desc.ts))
                           : k == kItemScan ? est_scan_item_ms(j->slice, it.b)
                           : k == kItemCrc ? est_crc_item_ms(j->slice, it.b)
                           : k == kItemSetId ? est_set_id_ms(j->n)

@@ -287,3 +287,39 @@ def test_write_index_file(p2g, gpu, tmp_path):
     src = p2g.SourceFile.scan(tmp_path / "a.bin", b"a.bin", 4)
     out = p2g.write_index_file(p2g.CreateOptions(output=tmp_path / "recovery.par2", slice_size=4), [src])
     assert out == tmp_path / "recovery.par2" and out.exists()
+
+
+# ---- the two device-job pipelines ---------------------------------------------
+# Jobs run as one persistent launch by default; the multi-stream banded
+# pipeline (P2G_BANDED, and jobs whose whole-file MD5 is on the device) must
+# give the same bytes: folded and unfolded tail groups, realigned slices,
+# several files, > 256 recovery rows.
+@pytest.mark.parametrize("lens,slice_,R", [
+    ([300_001], 4096, 48), ([5000, 70000, 1], 1024, 300), ([9000, 4100 * 3], 4100, 7),
+    ([2_000_000, 17], 16384, 70), ([1_100_000], 65536, 33),
+])
+def test_device_job_persistent_equals_banded(p2g, gpu, monkeypatch, lens, slice_, R):
+    import torch
+
+    S = sum((n + slice_ - 1) // slice_ for n in lens)
+    host = np.zeros(S * slice_, np.uint8)
+    off = 0
+    for i, n in enumerate(lens):
+        host[off:off + n] = rnd(i + 3 * R, n)
+        off += (n + slice_ - 1) // slice_ * slice_
+    src = torch.from_numpy(host).cuda()
+    names = [f"f{i}.bin".encode() for i in range(len(lens))]
+
+    def run():
+        b = p2g.run_device_job(src, lens, names, slice_, R, skip_hash_full=True)
+        torch.cuda.synchronize()
+        rows = b.recovery.view(-1, b.rec_stride)[:R, :slice_].cpu().numpy().copy()
+        return (rows, b.checksums[:20 * S].cpu().numpy().copy(), b.hash16k[:16 * len(lens)].cpu().numpy().copy(),
+                b.packet_md5[:16 * R].cpu().numpy().copy(), b.set_id)
+
+    persistent = run()
+    monkeypatch.setenv("P2G_BANDED", "1")
+    banded = run()
+    for k, (x, y) in enumerate(zip(persistent, banded)):
+        assert (np.asarray(x) == np.asarray(y)).all() if not isinstance(x, bytes) else x == y, k
+
