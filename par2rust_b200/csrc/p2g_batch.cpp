@@ -51,6 +51,7 @@ struct PlanJob {
     // work the job needs (all by default): slice checksums, the set-id item,
     // packet-MD5 chains
     bool scans = true, set_id = true, chains = true;
+    uint64_t file_bytes = 0;  // largest file, when whole-file MD5 items run (0: none)
 };
 
 double finish_ms(const PlanJob& j) { return est_set_id_ms(j.n) + est_packet_item_ms(j.slice, j.R); }
@@ -111,6 +112,8 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
             pre.push_back({1e30, {ji, kItemSetId, 0, 0, 0, 0}});
             p.n_setid++;
         }
+        for (uint32_t f = 0; j.file_bytes && f < j.n; f += kScanSlices)  // longest chains: right after set ids
+            pre.push_back({1e29, {ji, kItemFileHash, f, std::min(kScanSlices, j.n - f), 0, 0}});
         for (uint32_t s = 0; j.scans && s < j.S; s += kScanSlices) {
             const uint32_t cnt = std::min(kScanSlices, j.S - s);
             pre.push_back({scan_ms(j, cnt), {ji, kItemScan, s, cnt, 0, 0}});
@@ -172,6 +175,7 @@ double item_ms(const PlanJob& j, const BatchItem& it) {
     switch (it.kind_rg & kItemKindMask) {
     case kItemScan: return scan_ms(j, it.b);
     case kItemCrc: return est_crc_item_ms(j.slice, it.b);
+    case kItemFileHash: return md5_ms(j.file_bytes) + kItemMs;
     case kItemEncode: return encode_ms(j, std::min(j.ts, it.b & 0xFFFFu));
     default: return est_set_id_ms(j.n);
     }
@@ -275,7 +279,7 @@ double est_set_id_ms(uint32_t files) {
 double est_packet_item_ms(uint64_t slice, uint32_t rows) { return ceil(rows / 256.0) * md5_ms(36 + slice) + kItemMs; }
 
 SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans, bool set_id,
-                              bool chains, uint32_t ctas) {
+                              bool chains, uint32_t ctas, uint64_t file_bytes) {
     std::vector<PlanJob> jobs(1);
     jobs[0].slice = slice;
     jobs[0].S = S;
@@ -284,6 +288,7 @@ SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n
     jobs[0].scans = scans;
     jobs[0].set_id = set_id;
     jobs[0].chains = chains && R;
+    jobs[0].file_bytes = file_bytes;
     Plan p = plan_batch(jobs, ctas, 0);
     SingleJobPlan out;
     out.items = std::move(p.items);

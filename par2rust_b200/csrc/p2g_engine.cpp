@@ -289,8 +289,10 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     const uint32_t RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
     const bool chains = j.R && j.S && j.d_pkt;
     const bool sid_item = !j.have_set_id;
+    uint64_t max_len = 0;
+    for (const auto& f : j.files) max_len = std::max(max_len, f.length);
     const SingleJobPlan pl = plan_single_job(j.slice, j.S, j.R && j.S ? j.R : 0, n, j.d_checks != nullptr, sid_item,
-                                             chains, (uint32_t)device_sm_count());
+                                             chains, (uint32_t)device_sm_count(), j.d_hfull ? max_len : 0);
     const uint32_t nb = (uint32_t)pl.band_items.size();
     const uint32_t Q = (j.R + kChainRows - 1) / kChainRows;
     const uint64_t ctl_words = 1 + (chains ? nb + 2 * Q + 1 : 0) + 1;  // head, chain state, error word
@@ -332,6 +334,7 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     d.h16k = j.d_h16k;
     d.pkt = j.d_pkt;
     d.set_id = D + o_sid;
+    d.hfull = j.d_hfull;
     d.files = reinterpret_cast<const uint64_t*>(D + o_files);
     d.names = D + o_names;
     d.name_off = reinterpret_cast<const uint32_t*>(D + o_noff);
@@ -404,9 +407,9 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     return P2G_OK;
 }
 
+// P2G_BANDED=1 selects the multi-stream banded pipeline below instead.
 static p2g_status run_device_job(Context& c, DeviceJob& j, cudaStream_t caller) {
-    // whole-file MD5 on the device stays with the multi-stream pipeline below
-    if (!j.d_hfull && !getenv("P2G_BANDED")) return run_device_job_persistent(c, j, caller);
+    if (!getenv("P2G_BANDED")) return run_device_job_persistent(c, j, caller);
     const uint32_t n = (uint32_t)j.files.size();
     const uint32_t RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
     P2G_TRY(fork_from(c, caller));

@@ -130,6 +130,7 @@ enum BatchItemKind : uint32_t {
     kItemSetId = 3,   // hash16k, file ids and set id
     kItemPacket = 4,  // packet MD5s of recovery rows [a, a+b) (set id already written)
     kItemCrc = 5,     // slice CRC32 of slices [a, a+b)
+    kItemFileHash = 6,  // whole-file MD5 (hash_full) of files [a, a+b), one lane each
 };
 constexpr uint64_t kCrcItemBytes = 4u << 20;  // source bytes per CRC item
 constexpr uint32_t kItemKindMask = 0x7Fu;
@@ -164,6 +165,7 @@ struct BatchJob {
     uint8_t* h16k;             // 16 bytes per file
     uint8_t* pkt;              // 16 bytes per recovery row
     uint8_t* set_id;           // 16 bytes
+    uint8_t* hfull;            // 16 bytes per file (whole-file MD5), when file-hash items run
     const uint64_t* files;     // 2 per file: byte offset in src, length
     const uint8_t* names;      // display names, each starting 4-byte aligned
     const uint32_t* name_off;  // 2 per file: offset into names, length
@@ -191,8 +193,9 @@ struct SingleJobPlan {
     uint32_t band_syms = 0, ts = 0;
     double predicted_ms = 0;
 };
+// file_bytes: largest file (non-zero: whole-file MD5 items, 256 files each)
 SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans, bool set_id,
-                              bool chains, uint32_t ctas);
+                              bool chains, uint32_t ctas, uint64_t file_bytes = 0);
 // Shared memory of one batch CTA.
 size_t batch_smem_bytes();
 // Fills every job's basis (one launch; blockIdx.y = job).

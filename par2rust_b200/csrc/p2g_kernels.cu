@@ -1069,6 +1069,22 @@ __device__ __forceinline__ void batch_scan(const BatchJob& J, uint32_t first, ui
     }
 }
 
+// Whole-file MD5 (hash_full, src/source.rs:222-228) of files [first,
+// first+count) of job J, one file per MD5 lane: a serial chain each.
+template <bool VEC>
+__device__ __forceinline__ void batch_file_hash(const BatchJob& J, uint32_t first, uint32_t count, uint32_t ring) {
+    const int tid = threadIdx.x;
+    if (tid < kHashThreads && (uint32_t)tid < count) {
+        const uint32_t f = first + tid;
+        uint32_t st[4];
+        md5_init(st);
+        md5_range_ring<0, VEC, kBatchRingUnits, kBatchRingAhead>(st, nullptr, J.src + J.files[2 * f],
+                                                                 J.files[2 * f + 1], 0, ~0ull,
+                                                                 ring + tid * kBatchRingLane);
+        store_digest(J.hfull + 16 * (size_t)f, st);
+    }
+}
+
 // Slice CRC32 of slices [first, first+count): one slice per warp at a time
 // over all 16 warps (CRC streams from DRAM; its items are a few MB each so
 // the work spreads over many SMs).
@@ -1299,6 +1315,14 @@ __global__ void __launch_bounds__(kEncThreads, 1)
                 batch_scan<true>(J, it.a, it.b, ring);
             else
                 batch_scan<false>(J, it.a, it.b, ring);
+            __syncthreads();
+            continue;
+        }
+        if (kind == kItemFileHash) {
+            if (J.vec)
+                batch_file_hash<true>(J, it.a, it.b, ring);
+            else
+                batch_file_hash<false>(J, it.a, it.b, ring);
             __syncthreads();
             continue;
         }

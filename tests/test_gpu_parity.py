@@ -311,15 +311,20 @@ def test_device_job_persistent_equals_banded(p2g, gpu, monkeypatch, lens, slice_
     names = [f"f{i}.bin".encode() for i in range(len(lens))]
 
     def run():
-        b = p2g.run_device_job(src, lens, names, slice_, R, skip_hash_full=True)
+        # whole-file MD5 on the device too (file-hash items / the banded pipeline's file kernel)
+        b = p2g.run_device_job(src, lens, names, slice_, R, skip_hash_full=False)
         torch.cuda.synchronize()
         rows = b.recovery.view(-1, b.rec_stride)[:R, :slice_].cpu().numpy().copy()
         return (rows, b.checksums[:20 * S].cpu().numpy().copy(), b.hash16k[:16 * len(lens)].cpu().numpy().copy(),
-                b.packet_md5[:16 * R].cpu().numpy().copy(), b.set_id)
+                b.packet_md5[:16 * R].cpu().numpy().copy(), b.set_id, b.hash_full[:16 * len(lens)].cpu().numpy().copy())
 
     persistent = run()
     monkeypatch.setenv("P2G_BANDED", "1")
     banded = run()
     for k, (x, y) in enumerate(zip(persistent, banded)):
         assert (np.asarray(x) == np.asarray(y)).all() if not isinstance(x, bytes) else x == y, k
+    off = 0
+    for i, n in enumerate(lens):  # hash_full against hashlib
+        assert persistent[5][16 * i:16 * i + 16].tobytes() == hashlib.md5(host[off:off + n].tobytes()).digest(), i
+        off += (n + slice_ - 1) // slice_ * slice_
 
