@@ -278,6 +278,8 @@ struct DeviceJob {
     bool have_set_id = false;
 };
 
+static p2g_status check_device_error(Context& c);
+
 // The device job through the persistent kernel (p2g_kernels.cu, batch_kernel)
 // with this one job: slice MD5/CRC32 scan items and the set-id item first,
 // then encode items band by band (folded tail, tiles sized to whole rounds of
@@ -395,6 +397,7 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
         P2G_CU(c.h_h16k.ensure(16 * (size_t)n));
         P2G_CU(cudaMemcpyAsync(c.h_h16k.p, j.d_h16k, 16 * n, cudaMemcpyDeviceToHost, st));
         P2G_CU(cudaStreamSynchronize(st));
+        P2G_TRY(check_device_error(c));  // the error word arrived with the hash16k values
         j.h16k.resize(n);
         j.file_ids.resize(n);
         for (uint32_t f = 0; f < n; ++f) {

@@ -75,6 +75,7 @@ struct SJob {
     double enc_ms = 0, pkt_ms_per_item = 0;
     // state
     int state = 0;  // 0 queued, 1 resident, 2 complete, 3 released
+    bool counted = false;  // footprint added to the resident bytes (admitted)
     int32_t status = P2G_OK;
     double t_submit = 0, t_admit = 0, t_done = 0;
 };
@@ -201,10 +202,22 @@ p2g_status admit(p2g_server* s) {
         const uint64_t realign_b = j.slice % 16 ? round_up((uint64_t)j.S * rec_stride, 256) : 0;
         const uint64_t total = src_b + rec_b + chk_b + small_b + realign_b;
         cudaError_t e = cudaMallocAsync(&j.mem, total, s->copy);
-        if (e == cudaErrorMemoryAllocation) {  // the pool cannot place it now: retry after a release
+        if (e == cudaErrorMemoryAllocation) {
             cudaGetLastError();
             j.mem = nullptr;
-            break;
+            bool any_resident = false;
+            for (auto& up : s->live) any_resident |= up->mem != nullptr;
+            if (any_resident) break;  // the pool cannot place it now: retry after a release
+            // nothing else holds device memory: the job can never be placed
+            j.status = P2G_ERR_OOM;
+            j.state = 2;
+            j.t_admit = j.t_done = s->now();
+            s->completed.push_back(&j);
+            s->st.completed++;
+            s->live.push_back(std::move(s->queue.front()));
+            s->queue.pop_front();
+            s->cv_done.notify_all();
+            continue;
         }
         if (e != cudaSuccess) return fail_cuda(s, e, "cudaMallocAsync");
         uint8_t* m = static_cast<uint8_t*>(j.mem);
@@ -275,6 +288,7 @@ p2g_status admit(p2g_server* s) {
         j.state = 1;
         j.t_admit = s->now();
         s->resident_bytes += j.footprint;
+        j.counted = true;
         s->peak_bytes = std::max(s->peak_bytes, s->resident_bytes);
         s->st.admitted++;
         s->live.push_back(std::move(s->queue.front()));
@@ -447,7 +461,8 @@ void free_job_memory(p2g_server* s, SJob& j) {
     j.ready = nullptr;
     if (j.slot != ~0u) s->free_slots.push_back(j.slot);
     j.slot = ~0u;
-    s->resident_bytes -= j.footprint;
+    if (j.counted) s->resident_bytes -= j.footprint;
+    j.counted = false;
 }
 
 }  // namespace
