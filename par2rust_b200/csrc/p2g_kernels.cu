@@ -203,14 +203,15 @@ __host__ __device__ constexpr int ctz5(int u) {
     return (u & 1) ? 0 : (u & 2) ? 1 : (u & 4) ? 2 : (u & 8) ? 3 : 4;
 }
 
-// FMAX: largest row-group fold the CTA may run (a stage holds FMAX tiles).
-template <int NCH, int FMAX = 1>
+// FMAX: largest row-group fold the CTA may run (a stage holds FMAX tiles);
+// STAGES: depth of the TMA ring.
+template <int NCH, int FMAX = 1, int STAGES = kEncStages>
 __host__ __device__ constexpr size_t encode_bars_offset() {
-    return 2 * kTabBytes + (size_t)kEncStages * (FMAX * (kEncThreads / 32) * NCH * 64 * 2 + 1024);
+    return 2 * kTabBytes + (size_t)STAGES * (FMAX * (kEncThreads / 32) * NCH * 64 * 2 + 1024);
 }
-template <int NCH, int FMAX = 1>
+template <int NCH, int FMAX = 1, int STAGES = kEncStages>
 __host__ __device__ constexpr size_t encode_smem_bytes() {
-    return encode_bars_offset<NCH, FMAX>() + kEncStages * sizeof(uint64_t);
+    return encode_bars_offset<NCH, FMAX, STAGES>() + STAGES * sizeof(uint64_t);
 }
 
 // One (row group, symbol tile) work unit of the accumulator: 32 rows x
@@ -249,7 +250,7 @@ __device__ __forceinline__ void red_xor4(uint8_t* p, const uint4& v) {
     asm volatile("red.global.xor.b32 [%0], %1;" ::"l"(q + 3), "r"(v.w) : "memory");
 }
 
-template <int NCH, bool GEN = false, int FMAX = 1>
+template <int NCH, bool GEN = false, int FMAX = 1, int STAGES = kEncStages>
 __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S,
                                             const uint16_t* __restrict__ basis, uint32_t RG, uint32_t rg,
                                             uint32_t R, uint32_t n0, uint32_t tile_syms,
@@ -261,8 +262,8 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
     static_assert(!GEN || WARPS == 16, "derived basis: one warp per basis product j");
     uint8_t* tabs = smem;
     uint8_t* src_st = smem + 2 * kTabBytes;
-    uint8_t* bas_st = src_st + kEncStages * NT * 2;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(bas_st + kEncStages * 1024);
+    uint8_t* bas_st = src_st + STAGES * NT * 2;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(bas_st + STAGES * 1024);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile_bytes = tile_syms * 2;
@@ -270,7 +271,7 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
     src += (size_t)s0 * src_stride;
     if (!GEN) basis += (size_t)s0 * RG * 512;
     const uint16_t* lbase = d_logbase + s0;
-    auto parity = [&](uint32_t s) { return ((ph >> (s % kEncStages)) ^ (s / kEncStages)) & 1u; };
+    auto parity = [&](uint32_t s) { return ((ph >> (s % STAGES)) ^ (s / STAGES)) & 1u; };
 
     auto issue = [&](uint32_t s, int st) {
         mbar_arrive_expect_tx(&bars[st], GEN ? tile_bytes : tile_bytes + 1024);
@@ -279,7 +280,7 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
         if (!GEN) tma_load_1d(bas_st + st * 1024, basis + ((size_t)s * RG + rg) * 512, 1024, &bars[st]);
     };
     if (tid == 0)
-        for (int st = 0; st < kEncStages && (uint32_t)st < S; ++st) issue(st, st);
+        for (int st = 0; st < STAGES && (uint32_t)st < S; ++st) issue(st, st);
 
     // derived basis: this thread's (j = warp, row = lane) entry and its offset in a slot
     const uint32_t g_row = rg * kRowsPerGroup + (lane & (31u >> (fold >> 1)));  // replicated when folded
@@ -358,15 +359,15 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
     }
     if (__syncthreads_or(bad)) {
         if (tid == 0)
-            for (uint32_t s2 = 1; s2 < S && s2 < (uint32_t)kEncStages; ++s2) mbar_wait_bounded(&bars[s2], parity(s2));
+            for (uint32_t s2 = 1; s2 < S && s2 < (uint32_t)STAGES; ++s2) mbar_wait_bounded(&bars[s2], parity(s2));
         return false;
     }
 
     for (uint32_t s = 0; s < S; ++s) {
-        const int st = (int)(s % kEncStages);
+        const int st = (int)(s % STAGES);
         const int t = (int)(s & 1);
         if (s + 1 < S) {
-            const int st1 = (int)((s + 1) % kEncStages);
+            const int st1 = (int)((s + 1) % STAGES);
             if (!mbar_wait_bounded(&bars[st1], parity(s + 1))) bad = 1;
             build(t ^ 1, GEN ? (int)((s + 1) & 1) : st1);  // GEN: the slice's slot
         }
@@ -403,17 +404,17 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
         }
         if (__syncthreads_or(bad)) {
             if (tid == 0)  // drain copies still in flight before the CTA's shared memory goes away
-                for (uint32_t s2 = s + 1; s2 < S && s2 < s + kEncStages; ++s2)
-                    mbar_wait_bounded(&bars[s2 % kEncStages], parity(s2));
+                for (uint32_t s2 = s + 1; s2 < S && s2 < s + STAGES; ++s2)
+                    mbar_wait_bounded(&bars[s2 % STAGES], parity(s2));
             return false;
         }
-        if (tid == 0 && s + kEncStages < S) issue(s + kEncStages, st);
+        if (tid == 0 && s + STAGES < S) issue(s + STAGES, st);
     }
-    // stage st was used ceil((S - st) / kEncStages) times: flip its parity if odd
+    // stage st was used ceil((S - st) / STAGES) times: flip its parity if odd
     uint32_t flip = 0;
 #pragma unroll
-    for (int st = 0; st < kEncStages; ++st)
-        if ((uint32_t)st < S && (((S - 1 - st) / kEncStages) & 1u) == 0) flip |= 1u << st;
+    for (int st = 0; st < STAGES; ++st)
+        if ((uint32_t)st < S && (((S - 1 - st) / STAGES) & 1u) == 0) flip |= 1u << st;
     phase = ph ^ flip;
 
     // Epilogue: transpose (symbol-major, row pairs packed) into row-major
@@ -1016,15 +1017,17 @@ __global__ void realign_kernel(const uint8_t* __restrict__ src, uint64_t src_str
 // runs that job's finish step itself, so the launch has no inter-CTA waits.
 //
 // Shared memory: the encode region (tables, TMA ring, mbarriers), a cp.async
-// ring of kRingLaneBytes for each of the kHashThreads MD5 lanes, the CRC32
-// tables and a few words of per-CTA state.
+// ring of kBatchRingLane bytes for each of the kHashThreads MD5 lanes, the
+// CRC32 tables and a few words of per-CTA state.
 // ---------------------------------------------------------------------------
-constexpr size_t kBatchEncBytes = encode_smem_bytes<kEncChunks, 4>();
-// The persistent kernel stages MD5 streams through a 5-unit ring (3 units
-// ahead: ~2 us of chain work, more than a DRAM miss under load), the most
-// that fits beside an encode stage holding a folded tail item (4 tiles).
-constexpr int kBatchRingUnits = 5;
-constexpr int kBatchRingAhead = 3;
+// The persistent kernel runs its encode items on a 3-deep TMA ring (3 slices
+// of lead, ~4.5 us, hide any load) so that its MD5 streams get a 6-unit ring
+// (4 units ahead, like the dedicated hash kernels) beside an encode stage
+// that holds a folded tail item (4 tiles).
+constexpr int kBatchEncStages = 3;
+constexpr size_t kBatchEncBytes = (encode_smem_bytes<kEncChunks, 4, kBatchEncStages>() + 15) / 16 * 16;
+constexpr int kBatchRingUnits = 6;
+constexpr int kBatchRingAhead = 4;
 constexpr int kBatchRingLane = kBatchRingUnits * 64 + 16;
 constexpr size_t kBatchRingBytes = (size_t)kHashThreads * kBatchRingLane;
 constexpr size_t kBatchSmem = kBatchEncBytes + kBatchRingBytes + 4 * 256 * 4 + 64;
@@ -1290,14 +1293,14 @@ __global__ void __launch_bounds__(kEncThreads, 1)
                  uint32_t* __restrict__ ctl, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* enc = smem;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(enc + encode_bars_offset<kEncChunks, 4>());
+    uint64_t* bars = reinterpret_cast<uint64_t*>(enc + encode_bars_offset<kEncChunks, 4, kBatchEncStages>());
     uint8_t* ring_p = smem + kBatchEncBytes;
     uint32_t(*T)[256] = reinterpret_cast<uint32_t(*)[256]>(ring_p + kBatchRingBytes);
     uint32_t* misc = reinterpret_cast<uint32_t*>(ring_p + kBatchRingBytes + 4 * 256 * 4);  // [0] item [1] last [4..7] set id
     const uint32_t ring = smem_u32(ring_p);
     const int tid = threadIdx.x;
     if (tid == 0) {
-        for (int st = 0; st < kEncStages; ++st) mbar_init(&bars[st], 1);
+        for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
         fence_mbar_init();
     }
     crc_tables_build(T);  // ends with __syncthreads
@@ -1361,10 +1364,10 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             const uint32_t fold = 1u << ((it.kind_rg >> 24) & 3u);
             const uint32_t syms = it.b & 0xFFFFu, band = it.b >> 16;
             const bool acc = (it.kind_rg & kItemAccumulate) != 0;
-            const bool ok = J.basis ? encode_tile<kEncChunks, false, 4>(J.esrc, J.estride, sn, J.basis, J.RG, rg, J.R,
+            const bool ok = J.basis ? encode_tile<kEncChunks, false, 4, kBatchEncStages>(J.esrc, J.estride, sn, J.basis, J.RG, rg, J.R,
                                                                          it.a, syms, J.rec, J.rec_stride, enc, phase,
                                                                          J.first_exp, it.s0, acc, fold, J.ts)
-                                    : encode_tile<kEncChunks, true, 4>(J.esrc, J.estride, sn, nullptr, J.RG, rg, J.R,
+                                    : encode_tile<kEncChunks, true, 4, kBatchEncStages>(J.esrc, J.estride, sn, nullptr, J.RG, rg, J.R,
                                                                         it.a, syms, J.rec, J.rec_stride, enc, phase,
                                                                         J.first_exp, it.s0, acc, fold, J.ts);
             if (!ok) {
