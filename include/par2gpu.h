@@ -312,9 +312,10 @@ p2g_status p2g_run_device_job(p2g_device_job *job);
  * encode items and (job, 256-slice) scan items off a device queue; the CTA
  * that completes a job's last encode item derives that job's hash16k, file
  * ids, set id (on the device) and recovery-packet MD5s.  Per job the device
- * outputs are byte-identical to p2g_run_device_job with
- * P2G_JOB_SKIP_HASH_FULL (hash_full stays with the caller, who usually hashes
- * it on the host while reading the files).  An autotuner picks each job's
+ * outputs are byte-identical to p2g_run_device_job; hash_full is computed
+ * only when its output is given (one chain per file, which bounds the batch by
+ * its largest file), else it stays with the caller, who usually hashes files
+ * on the host while reading them.  An autotuner picks each job's
  * tile width and the queue order by simulating the launch with a cost model.
  * Coefficient bases are precomputed into batch scratch (S x ceil(R/32) x
  * 1 KiB per job) while the batch's total stays within 16 GiB
@@ -336,6 +337,8 @@ typedef struct p2g_batch_job {
     uint8_t *hash16k;                   /* device, 16 per file */
     uint8_t *packet_md5;                /* device, 16 per recovery row */
     uint8_t *set_id;                    /* device, 16 bytes, 4-byte aligned */
+    uint8_t *hash_full;                 /* device, 16 per file, 4-byte aligned; NULL: the caller hashes
+                                           whole files itself (one serial MD5 chain per file) */
 } p2g_batch_job;
 
 typedef struct p2g_batch p2g_batch;     /* opaque */

@@ -585,6 +585,7 @@ class BatchJobSpec:
     slice_size: int
     recovery_count: int
     bufs: DeviceJobBuffers
+    hash_full: bool = False  # whole-file MD5s on the device too (into bufs.hash_full)
 
     @property
     def input_slices(self) -> int:
@@ -630,7 +631,8 @@ class Batch:
                                         name_lens=nlens, slice_size=j.slice_size, recovery_count=j.recovery_count,
                                         recovery=b.recovery.data_ptr(), recovery_stride=b.rec_stride,
                                         checksums=b.checksums.data_ptr(), hash16k=b.hash16k.data_ptr(),
-                                        packet_md5=b.packet_md5.data_ptr(), set_id=b.set_id_device.data_ptr())
+                                        packet_md5=b.packet_md5.data_ptr(), set_id=b.set_id_device.data_ptr(),
+                                        hash_full=b.hash_full.data_ptr() if j.hash_full else None)
         self.jobs = list(jobs)
         h = C.c_void_p()
         _check(lib().p2g_batch_create(arr, len(jobs), flags, C.byref(h)))

@@ -153,6 +153,7 @@ class p2g_batch_job(C.Structure):
         ("hash16k", C.c_void_p),
         ("packet_md5", C.c_void_p),
         ("set_id", C.c_void_p),
+        ("hash_full", C.c_void_p),
     ]
 
 

@@ -433,6 +433,12 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         shape[i].S = (uint32_t)S;
         shape[i].R = jb.recovery_count;
         shape[i].n = jb.file_count;
+        if (jb.hash_full) {
+            if ((uintptr_t)jb.hash_full % 4)
+                return set_error(P2G_ERR_INVALID_ARGUMENT, "batch job %u: hash_full must be 4-byte aligned", i);
+            for (uint32_t f = 0; f < jb.file_count; ++f)
+                shape[i].file_bytes = std::max<uint64_t>(shape[i].file_bytes, jb.file_lengths[f]);
+        }
     }
     P2G_TRY(ensure_device_ready());
     p2g_batch* b = new p2g_batch();
@@ -519,6 +525,7 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         d.h16k = jb.hash16k;
         d.pkt = jb.packet_md5;
         d.set_id = jb.set_id;
+        d.hfull = jb.hash_full;
         d.files = reinterpret_cast<const uint64_t*>(A + o_files) + 2 * fcur;
         d.name_off = reinterpret_cast<const uint32_t*>(A + o_noff) + 2 * fcur;
         d.names = A + o_names;

@@ -122,7 +122,8 @@ def _make_job(p2g, k, spec, slice_, R):
         off += (len(d) + slice_ - 1) // slice_ * slice_
     src = torch.from_numpy(host).cuda()
     bufs = p2g.DeviceJobBuffers(S, len(files), slice_, R, src.device)
-    spec_ = p2g.BatchJobSpec(src, [len(d) for _, d in files], [n for n, _ in files], slice_, R, bufs)
+    # whole-file MD5s on the device as well (file-hash items)
+    spec_ = p2g.BatchJobSpec(src, [len(d) for _, d in files], [n for n, _ in files], slice_, R, bufs, hash_full=True)
     return spec_, files, host
 
 
@@ -136,22 +137,24 @@ def _outputs(spec):
         "h16k": b.hash16k[:16 * n].cpu().numpy().copy(),
         "pkt": b.packet_md5[:16 * R].cpu().numpy().copy() if R else None,
         "set_id": b.set_id_device.cpu().numpy().tobytes(),
+        "hfull": b.hash_full[:16 * n].cpu().numpy().copy(),
     }
 
 
 def _expected(oracle, files, host, slice_, R):
     S = len(host) // slice_
-    cks, h16s, fids = [], [], []
+    cks, h16s, fids, hfs = [], [], [], []
     for name, d in files:
-        st, c, _hf, h16, fid = oracle.scan(d, slice_, name)
+        st, c, hf, h16, fid = oracle.scan(d, slice_, name)
         assert st == 0
         cks += c
         h16s.append(h16)
         fids.append(fid)
+        hfs.append(hf)
     sid = oracle.set_id(slice_, fids)
     rec = np.asarray(oracle.encode(host, S, slice_, R)).reshape(R, slice_) if R else None
     pkt = [oracle.recovery_packet_md5(sid, r, rec[r].tobytes()) for r in range(R)] if R else []
-    return cks, h16s, sid, rec, pkt
+    return cks, h16s, sid, rec, pkt, hfs
 
 
 @pytest.fixture(scope="module")
@@ -171,7 +174,8 @@ def test_batch_matches_oracle(p2g, oracle, gpu, batch_jobs):
     assert info.jobs == len(JOB_SET) and info.setid_items == len(JOB_SET)
     for k, (spec, files, host) in enumerate(batch_jobs):
         got = _outputs(spec)
-        cks, h16s, sid, rec, pkt = _expected(oracle, files, host, spec.slice_size, spec.recovery_count)
+        cks, h16s, sid, rec, pkt, hfs = _expected(oracle, files, host, spec.slice_size, spec.recovery_count)
+        assert got["hfull"].tobytes() == b"".join(hfs), f"job {k} hash_full"
         ch = got["checks"].reshape(-1, 20)
         assert [(bytes(r[:16]), int.from_bytes(bytes(r[16:]), "little")) for r in ch] == cks, f"job {k} checksums"
         assert got["h16k"].tobytes() == b"".join(h16s), f"job {k} hash16k"
@@ -217,14 +221,14 @@ def test_batch_job_alone_equals_in_mix(p2g, gpu, batch_jobs):
     in_mix = [_outputs(j) for j, _, _ in batch_jobs]
     for k, (spec, _, _) in enumerate(batch_jobs):
         for t in (spec.bufs.recovery, spec.bufs.checksums, spec.bufs.hash16k, spec.bufs.packet_md5,
-                  spec.bufs.set_id_device):
+                  spec.bufs.set_id_device, spec.bufs.hash_full):
             t.fill_(0xA5)
         alone = p2g.Batch([spec])
         alone.launch()
         torch.cuda.synchronize()
         alone.check()
         got = _outputs(spec)
-        for key in ("checks", "h16k", "set_id"):
+        for key in ("checks", "h16k", "set_id", "hfull"):
             assert np.array_equal(np.frombuffer(bytes(got[key]), np.uint8),
                                   np.frombuffer(bytes(in_mix[k][key]), np.uint8)), (k, key)
         if spec.recovery_count:
