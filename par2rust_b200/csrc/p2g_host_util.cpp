@@ -57,15 +57,22 @@ namespace p2g {
 static inline uint32_t rol(uint32_t x, int s) { return (x << s) | (x >> (32 - s)); }
 
 
-// Fully unrolled compression: the round functions use the shortest
-// dependent forms (z ^ (x & (y ^ z)) etc.) so one core runs the serial
-// chain of a whole-file hash as fast as plain C allows.
+// Fully unrolled compression, written for the shortest dependent chain
+// through b (the value the previous step produced), since one core runs the
+// serial chain of a whole-file hash: the message word and constant are added
+// to a before the round function; H groups y ^ z, which does not wait for b;
+// and G = (x & z) | (y & ~z) is added as two disjoint terms, (y & ~z) early
+// and (x & z) last, so its chain is AND, ADD instead of XOR, AND, XOR, ADD.
 #define HM_F(x, y, z) ((z) ^ ((x) & ((y) ^ (z))))
-#define HM_G(x, y, z) ((y) ^ ((z) & ((x) ^ (y))))
-#define HM_H(x, y, z) ((x) ^ (y) ^ (z))
+#define HM_H(x, y, z) ((x) ^ ((y) ^ (z)))
 #define HM_I(x, y, z) ((y) ^ ((x) | ~(z)))
 #define HM_STEP(f, a, b, c, d, x, t, s) \
-    (a) += f((b), (c), (d)) + (x) + (t); \
+    (a) += (x) + (t);                   \
+    (a) += f((b), (c), (d));            \
+    (a) = rol((a), (s)) + (b);
+#define HM_STEP_G(a, b, c, d, x, t, s) \
+    (a) += (x) + (t) + ((c) & ~(d));   \
+    (a) += (b) & (d);                  \
     (a) = rol((a), (s)) + (b);
 
 static void md5_block(uint32_t st[4], const uint8_t* p) {
@@ -80,14 +87,14 @@ static void md5_block(uint32_t st[4], const uint8_t* p) {
     HM_STEP(HM_F, c, d, a, b, m[10], 0xffff5bb1, 17) HM_STEP(HM_F, b, c, d, a, m[11], 0x895cd7be, 22)
     HM_STEP(HM_F, a, b, c, d, m[12], 0x6b901122, 7) HM_STEP(HM_F, d, a, b, c, m[13], 0xfd987193, 12)
     HM_STEP(HM_F, c, d, a, b, m[14], 0xa679438e, 17) HM_STEP(HM_F, b, c, d, a, m[15], 0x49b40821, 22)
-    HM_STEP(HM_G, a, b, c, d, m[1], 0xf61e2562, 5) HM_STEP(HM_G, d, a, b, c, m[6], 0xc040b340, 9)
-    HM_STEP(HM_G, c, d, a, b, m[11], 0x265e5a51, 14) HM_STEP(HM_G, b, c, d, a, m[0], 0xe9b6c7aa, 20)
-    HM_STEP(HM_G, a, b, c, d, m[5], 0xd62f105d, 5) HM_STEP(HM_G, d, a, b, c, m[10], 0x02441453, 9)
-    HM_STEP(HM_G, c, d, a, b, m[15], 0xd8a1e681, 14) HM_STEP(HM_G, b, c, d, a, m[4], 0xe7d3fbc8, 20)
-    HM_STEP(HM_G, a, b, c, d, m[9], 0x21e1cde6, 5) HM_STEP(HM_G, d, a, b, c, m[14], 0xc33707d6, 9)
-    HM_STEP(HM_G, c, d, a, b, m[3], 0xf4d50d87, 14) HM_STEP(HM_G, b, c, d, a, m[8], 0x455a14ed, 20)
-    HM_STEP(HM_G, a, b, c, d, m[13], 0xa9e3e905, 5) HM_STEP(HM_G, d, a, b, c, m[2], 0xfcefa3f8, 9)
-    HM_STEP(HM_G, c, d, a, b, m[7], 0x676f02d9, 14) HM_STEP(HM_G, b, c, d, a, m[12], 0x8d2a4c8a, 20)
+    HM_STEP_G(a, b, c, d, m[1], 0xf61e2562, 5) HM_STEP_G(d, a, b, c, m[6], 0xc040b340, 9)
+    HM_STEP_G(c, d, a, b, m[11], 0x265e5a51, 14) HM_STEP_G(b, c, d, a, m[0], 0xe9b6c7aa, 20)
+    HM_STEP_G(a, b, c, d, m[5], 0xd62f105d, 5) HM_STEP_G(d, a, b, c, m[10], 0x02441453, 9)
+    HM_STEP_G(c, d, a, b, m[15], 0xd8a1e681, 14) HM_STEP_G(b, c, d, a, m[4], 0xe7d3fbc8, 20)
+    HM_STEP_G(a, b, c, d, m[9], 0x21e1cde6, 5) HM_STEP_G(d, a, b, c, m[14], 0xc33707d6, 9)
+    HM_STEP_G(c, d, a, b, m[3], 0xf4d50d87, 14) HM_STEP_G(b, c, d, a, m[8], 0x455a14ed, 20)
+    HM_STEP_G(a, b, c, d, m[13], 0xa9e3e905, 5) HM_STEP_G(d, a, b, c, m[2], 0xfcefa3f8, 9)
+    HM_STEP_G(c, d, a, b, m[7], 0x676f02d9, 14) HM_STEP_G(b, c, d, a, m[12], 0x8d2a4c8a, 20)
     HM_STEP(HM_H, a, b, c, d, m[5], 0xfffa3942, 4) HM_STEP(HM_H, d, a, b, c, m[8], 0x8771f681, 11)
     HM_STEP(HM_H, c, d, a, b, m[11], 0x6d9d6122, 16) HM_STEP(HM_H, b, c, d, a, m[14], 0xfde5380c, 23)
     HM_STEP(HM_H, a, b, c, d, m[1], 0xa4beea44, 4) HM_STEP(HM_H, d, a, b, c, m[4], 0x4bdecfa9, 11)
