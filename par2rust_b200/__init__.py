@@ -385,14 +385,26 @@ def write_index_file(opts: CreateOptions, sources: Sequence[SourceFile]) -> Path
     return Path(os.fsdecode(p))
 
 
+class _OutputSetOwner:
+    """Frees a library-owned p2g_output_set once no view of it is left."""
+
+    def __init__(self, os_):
+        self.os_ = os_
+
+    def __del__(self):
+        lib().p2g_output_set_free(C.byref(self.os_))
+
+
 def create_in_memory(opts: CreateOptions, inputs: Sequence[Tuple[bytes, object]],
-                     return_sources: bool = False):
+                     return_sources: bool = False, copy: bool = True):
     """run_create_fused without a filesystem.
 
     ``inputs`` are (display_name, data) pairs; data is any buffer (bytes,
     numpy array, pinned torch tensor, ...).  Returns a list of
     (file_name, bytes) for the index and each volume, plus the scanned
-    SourceFile records when ``return_sources``.
+    SourceFile records when ``return_sources``.  With ``copy=False`` the
+    file contents are read-only memoryviews of the library's buffers (no
+    copy into Python bytes); the buffers are freed when the last view goes.
     """
     keep: list = []
     o = opts._to_c(keep)
@@ -409,10 +421,18 @@ def create_in_memory(opts: CreateOptions, inputs: Sequence[Tuple[bytes, object]]
     os_ = _ffi.p2g_output_set()
     _check(lib().p2g_create_in_memory(C.byref(o), arr, len(inputs), srcs, C.byref(os_)))
     files = []
-    for i in range(os_.count):
-        f = os_.files[i]
-        files.append((os.fsdecode(f.name), C.string_at(f.data, f.length)))
-    lib().p2g_output_set_free(C.byref(os_))
+    if copy:
+        for i in range(os_.count):
+            f = os_.files[i]
+            files.append((os.fsdecode(f.name), C.string_at(f.data, f.length)))
+        lib().p2g_output_set_free(C.byref(os_))
+    else:
+        owner = _OutputSetOwner(os_)
+        for i in range(os_.count):
+            f = os_.files[i]
+            buf = (C.c_uint8 * f.length).from_address(C.cast(f.data, C.c_void_p).value)
+            buf._owner = owner  # the view keeps buf, buf keeps the output set
+            files.append((os.fsdecode(f.name), memoryview(buf).cast("B").toreadonly()))
     if not return_sources:
         return files
     out_src = []

@@ -10,6 +10,7 @@
 //            rec_stride = slice_size rounded up to 16 bytes.
 //   basis    [s][row group][16][32] u16 coefficient-basis scratch.
 //   checks   one 20-byte IFSC record (md5 ‖ crc32) per input slice.
+#include <functional>
 #include <cuda_runtime.h>
 #include <errno.h>
 #include <fcntl.h>
@@ -89,6 +90,7 @@ struct Context {
     DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out, md5_state;
     DevBuf persist;    // single-job persistent run: descriptor, items, chain state, tables
     PinBuf h_spans, h_h16k, h_err, h_stage, h_persist;
+    PinBuf h_rec;  // host copy of the recovery rows (create calls)
 };
 static Context& ctx() {
     static Context* c = new Context();  // never destroyed: the CUDA runtime may be gone at exit
@@ -644,29 +646,40 @@ static Md5 critical_packets(uint64_t slice, const p2g_source_file* src, uint32_t
     return set_id;
 }
 
+// Pinned host copy of a create call's recovery rows.  The context keeps the
+// buffer for the next call (pinning ~100 MB takes tens of milliseconds)
+// unless it grew past kRetainPinnedRec.
+constexpr size_t kRetainPinnedRec = size_t(1) << 30;
 struct PinnedRec {
+    PinBuf& buf;
     uint8_t* p = nullptr;
-    size_t cap = 0;
+    explicit PinnedRec(Context& c) : buf(c.h_rec) {}
     cudaError_t ensure(size_t n) {
-        if (n <= cap && p) return cudaSuccess;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
-        cudaError_t e = cudaHostAlloc((void**)&p, std::max<size_t>(n, 1), cudaHostAllocDefault);
-        if (e == cudaSuccess) cap = n;
+        const cudaError_t e = buf.ensure(n);
+        p = buf.as<uint8_t>();
         return e;
     }
     ~PinnedRec() {
-        if (p) cudaFreeHost(p);
+        if (buf.cap > kRetainPinnedRec) {
+            cudaFreeHost(buf.p);
+            buf.p = nullptr;
+            buf.cap = 0;
+        }
     }
 };
+
+// Work a create call can do while the host is still hashing whole files:
+// called with the device results (set id, packet MD5s, recovery rows) and
+// the byte length the critical packet block will have.
+using WhileHashing = std::function<void(const CreateOutput&, size_t critical_len)>;
 
 // Scan (+ encode when R > 0) n in-memory inputs on the device.
 // `src_known` (optional): already-scanned SourceFile records; then only the
 // encode and the packet MD5s run and the critical packets use them.
 static p2g_status device_create(Context& c, const CreateInput* in, uint32_t n, uint64_t slice, uint32_t R,
                                 const p2g_source_file* src_known, const char* const* comments, uint32_t n_comments,
-                                CreateOutput& out, PinnedRec& rec_host) {
+                                CreateOutput& out, PinnedRec& rec_host,
+                                const WhileHashing* while_hashing = nullptr) {
     std::vector<JobFile> files(n);
     uint64_t S = 0;
     for (uint32_t f = 0; f < n; ++f) {
@@ -754,7 +767,8 @@ static p2g_status device_create(Context& c, const CreateInput* in, uint32_t n, u
     P2G_CU(cudaStreamSynchronize(main));
     P2G_TRY(check_device_error(c));
     if (R) memcpy(out.pkt_md5.data(), c.h_stage.p, 16 * (size_t)R);
-    hh.join();
+    out.set_id = j.set_id;
+    out.rec_host = rec_host.p;
 
     if (!src_known) {
         scanned.resize(n);
@@ -769,14 +783,27 @@ static p2g_status device_create(Context& c, const CreateInput* in, uint32_t n, u
             sf.length = in[f].length;
             memcpy(sf.hash16k, j.h16k[f].data(), 16);
             memcpy(sf.file_id, j.file_ids[f].data(), 16);
-            if (fmode == FileHashMode::Device)
-                memcpy(sf.hash_full, hfull_dev.data() + 16 * f, 16);
-            else
-                memcpy(sf.hash_full, host_full[f].data(), 16);
+            if (fmode == FileHashMode::Device) memcpy(sf.hash_full, hfull_dev.data() + 16 * f, 16);
             sf.slice_count = files[f].slices;
             sf.slice_checksums = (p2g_slice_checksum*)malloc(sizeof(p2g_slice_checksum) * std::max<uint64_t>(1, sf.slice_count));
             memcpy(sf.slice_checksums, checks.data() + files[f].first_slice, sizeof(p2g_slice_checksum) * sf.slice_count);
         }
+    }
+    if (while_hashing) {
+        // the critical block's length does not depend on the whole-file hashes
+        size_t crit_len = crit.size();
+        if (!src_known) {
+            std::vector<uint8_t> probe;
+            critical_packets(slice, scanned.data(), n, comments, n_comments, probe);
+            crit_len = probe.size();
+        }
+        (*while_hashing)(out, crit_len);
+    }
+    hh.join();
+
+    if (!src_known) {
+        if (fmode == FileHashMode::Host)
+            for (uint32_t f = 0; f < n; ++f) memcpy(scanned[f].hash_full, host_full[f].data(), 16);
         const Md5 sid = critical_packets(slice, scanned.data(), n, comments, n_comments, crit);
         if (sid != j.set_id) {
             for (auto& sf : scanned) free_source(sf);
@@ -784,25 +811,31 @@ static p2g_status device_create(Context& c, const CreateInput* in, uint32_t n, u
         }
     }
     out.critical = std::move(crit);
-    out.set_id = j.set_id;
-    out.rec_host = rec_host.p;
     out.sources = std::move(scanned);
     return P2G_OK;
 }
 
 // Byte pieces of one volume file: critical ‖ recovery packets ‖ critical
 // (build_volume_packet, src/creator.rs:1025-1042).
-static void volume_pieces(const CreateOutput& o, uint64_t slice, uint32_t first, uint32_t count,
-                          std::vector<uint8_t>& headers, std::vector<std::pair<const uint8_t*, size_t>>& pieces) {
+static void volume_pieces_recovery(const CreateOutput& o, uint64_t slice, uint32_t first, uint32_t count,
+                                   std::vector<uint8_t>& headers,
+                                   std::vector<std::pair<const uint8_t*, size_t>>& pieces) {
     headers.assign(68 * (size_t)count, 0);
     pieces.clear();
-    pieces.push_back({o.critical.data(), o.critical.size()});
     for (uint32_t k = 0; k < count; ++k) {
         const uint32_t e = first + k;
         recovery_packet_header(headers.data() + 68 * (size_t)k, o.set_id, o.pkt_md5.data() + 16 * (size_t)e, slice, e);
         pieces.push_back({headers.data() + 68 * (size_t)k, 68});
         pieces.push_back({o.rec_host + (size_t)e * slice, (size_t)slice});
     }
+}
+static void volume_pieces(const CreateOutput& o, uint64_t slice, uint32_t first, uint32_t count,
+                          std::vector<uint8_t>& headers, std::vector<std::pair<const uint8_t*, size_t>>& pieces) {
+    std::vector<std::pair<const uint8_t*, size_t>> mid;
+    volume_pieces_recovery(o, slice, first, count, headers, mid);
+    pieces.clear();
+    pieces.push_back({o.critical.data(), o.critical.size()});
+    pieces.insert(pieces.end(), mid.begin(), mid.end());
     pieces.push_back({o.critical.data(), o.critical.size()});
 }
 
@@ -1126,7 +1159,7 @@ static p2g_status scan_impl(const char* path, const uint8_t* name, size_t name_l
     if (hf.length == 0) return set_error(P2G_ERR_EMPTY_FILE, "input file \"%s\" is empty; PAR2 requires non-empty files", path);
     CreateInput in = {hf.data, hf.length, name, name_len, path};
     CreateOutput o;
-    PinnedRec rec;
+    PinnedRec rec(c);
     P2G_TRY(device_create(c, &in, 1, slice, 0, nullptr, nullptr, 0, o, rec));
     const uint64_t done = o.sources[0].slice_count;
     ev = mk(P2G_EV_SCAN_PROGRESS);
@@ -1237,7 +1270,7 @@ static p2g_status run_create_impl(const p2g_create_options* opts, const p2g_sour
             ins[f] = {hfs[f]->data, hfs[f]->length, sources[f].name, sources[f].name_len, sources[f].path};
         }
         CreateOutput enc;
-        PinnedRec rec;
+        PinnedRec rec(c);
         P2G_TRY(device_create(c, ins.data(), n, slice, R, sources, opts->comments, opts->comment_count, enc, rec));
         emit_encode_events(cb, user, S, R, true);
         co.rec_host = enc.rec_host;
@@ -1322,7 +1355,7 @@ extern "C" p2g_status p2g_run_create_fused(const p2g_create_options* opts, const
         ins[f] = {hfs[f]->data, hfs[f]->length, inputs[f].display_name, inputs[f].name_len, inputs[f].path};
     }
     CreateOutput co;
-    PinnedRec rec;
+    PinnedRec rec(c);
     P2G_TRY(device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co, rec));
     for (uint32_t f = 0; f < n; ++f) {
         p2g_progress_event ev = mk(P2G_EV_SCAN_PROGRESS);
@@ -1376,33 +1409,68 @@ extern "C" p2g_status p2g_create_in_memory(const p2g_create_options* opts, const
     if (R) P2G_TRY(resolve_volume_sizes(opts->volume_scheme, R, vs));
     P2G_TRY(ensure_ready(c));
     CreateOutput co;
-    PinnedRec rec;
-    P2G_TRY(device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co, rec));
+    PinnedRec rec(c);
     co.vol_sizes = vs;
     const std::string index = opts->output ? opts->output : "recovery.par2";
-    out->count = 1 + (uint32_t)co.vol_sizes.size();
+    // Volumes = critical | recovery packets | critical.  The recovery packets
+    // only need the device results, so they are laid into the volume buffers
+    // while the host still hashes whole files; the critical block (it holds
+    // those hashes) fills both ends afterwards.
+    std::vector<p2g_output_file> vols(vs.size());
+    size_t crit_len = 0;
+    bool vols_ok = true;
+    auto free_vols = [&]() {
+        for (auto& of : vols) {
+            free(of.name);
+            free(of.data);
+            of = p2g_output_file{};
+        }
+    };
+    const WhileHashing lay_out = [&](const CreateOutput& o, size_t clen) {
+        crit_len = clen;
+        uint32_t first = 0;
+        std::vector<uint8_t> headers;
+        std::vector<std::pair<const uint8_t*, size_t>> pieces;
+        for (size_t v = 0; v < vs.size() && vols_ok; ++v) {
+            volume_pieces_recovery(o, slice, first, vs[v], headers, pieces);
+            size_t tot = 2 * clen;
+            for (auto& p : pieces) tot += p.second;
+            p2g_output_file& of = vols[v];
+            of.name = dupstr(volume_filename(index, (uint16_t)first, vs[v]));
+            of.length = tot;
+            of.data = (uint8_t*)malloc(std::max<size_t>(tot, 1));
+            if (!of.name || !of.data) {
+                vols_ok = false;
+                break;
+            }
+            size_t at = clen;
+            for (auto& p : pieces) {
+                memcpy(of.data + at, p.first, p.second);
+                at += p.second;
+            }
+            first += vs[v];
+        }
+    };
+    const p2g_status st = device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co,
+                                        rec, &lay_out);
+    if (st != P2G_OK || !vols_ok || co.critical.size() != crit_len) {
+        free_vols();
+        if (st != P2G_OK) return st;
+        for (auto& sf : co.sources) free_source(sf);
+        if (!vols_ok) return set_error(P2G_ERR_OOM, "out of host memory for the volume buffers");
+        return set_error(P2G_ERR_CUDA, "internal: critical packet length changed after hashing");
+    }
+    out->count = 1 + (uint32_t)vs.size();
     out->files = (p2g_output_file*)calloc(out->count, sizeof(p2g_output_file));
     out->files[0].name = dupstr(index);
     out->files[0].length = co.critical.size();
     out->files[0].data = (uint8_t*)malloc(std::max<size_t>(co.critical.size(), 1));
     memcpy(out->files[0].data, co.critical.data(), co.critical.size());
-    uint32_t first = 0;
-    std::vector<uint8_t> headers;
-    std::vector<std::pair<const uint8_t*, size_t>> pieces;
-    for (size_t v = 0; v < co.vol_sizes.size(); ++v) {
-        volume_pieces(co, slice, first, co.vol_sizes[v], headers, pieces);
-        size_t tot = 0;
-        for (auto& p : pieces) tot += p.second;
-        p2g_output_file& of = out->files[1 + v];
-        of.name = dupstr(volume_filename(index, (uint16_t)first, co.vol_sizes[v]));
-        of.length = tot;
-        of.data = (uint8_t*)malloc(std::max<size_t>(tot, 1));
-        size_t at = 0;
-        for (auto& p : pieces) {
-            memcpy(of.data + at, p.first, p.second);
-            at += p.second;
-        }
-        first += co.vol_sizes[v];
+    for (size_t v = 0; v < vs.size(); ++v) {
+        p2g_output_file& of = vols[v];
+        memcpy(of.data, co.critical.data(), crit_len);
+        memcpy(of.data + of.length - crit_len, co.critical.data(), crit_len);
+        out->files[1 + v] = of;
     }
     if (sources_out)
         for (uint32_t f = 0; f < n; ++f) sources_out[f] = co.sources[f];

@@ -161,6 +161,25 @@ def test_create_in_memory_bit_exact(p2g, oracle, gpu, case):
         assert [(c.md5, c.crc32) for c in sf.slice_checksums] == cks
 
 
+@pytest.mark.parametrize("case", CREATE_CASES[:3], ids=[c[0] for c in CREATE_CASES[:3]])
+def test_create_in_memory_views_equal_copies(p2g, oracle, gpu, case):
+    """copy=False hands out views of the library's buffers; they must hold
+    the same bytes as the copies and stay valid after the call returns."""
+    _, inputs, slice_, R, scheme, count, sizes, comments = case
+    vs, _ = _scheme(p2g, oracle, scheme, count, sizes)
+    opts = p2g.CreateOptions(output="recovery.par2", slice_size=slice_, recovery_block_count=R, volume_scheme=vs,
+                             comments=comments)
+    copies = p2g.create_in_memory(opts, [(n, d) for n, d in inputs])
+    views = p2g.create_in_memory(opts, [(n, d) for n, d in inputs], copy=False)
+    p2g.create_in_memory(opts, [(n, d) for n, d in inputs], copy=False)  # a later call must not disturb them
+    assert [n for n, _ in views] == [n for n, _ in copies]
+    for (n, v), (_, b) in zip(views, copies):
+        assert isinstance(v, memoryview) and v.readonly
+        assert v.tobytes() == b, n
+    del copies
+    assert views[-1][1].tobytes()[:8] == b"PAR2\0PKT"
+
+
 @pytest.mark.parametrize("n_slices,R", [(3, 40), (2, 200), (5, 7)])
 def test_banded_encode_and_packet_md5(p2g, oracle, gpu, n_slices, R):
     """Large slices split the encode into symbol bands and chain the packet
