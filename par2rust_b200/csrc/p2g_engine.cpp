@@ -10,18 +10,19 @@
 //            rec_stride = slice_size rounded up to 16 bytes.
 //   basis    [s][row group][16][32] u16 coefficient-basis scratch.
 //   checks   one 20-byte IFSC record (md5 ‖ crc32) per input slice.
-#include <functional>
 #include <cuda_runtime.h>
 #include <errno.h>
 #include <fcntl.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -217,7 +218,7 @@ static FileHashMode choose_file_hash_mode(const std::vector<uint64_t>& lens) {
     }
     // chain rates in bytes/s: one device thread, one host core
     const double dev_rate = env_double("P2G_DEVICE_MD5_RATE", 1.2e8);
-    const double host_rate = env_double("P2G_HOST_MD5_RATE", 6.0e8);
+    const double host_rate = env_double("P2G_HOST_MD5_RATE", 8.0e8);
     uint64_t mx = 0, total = 0;
     for (uint64_t l : lens) {
         mx = std::max(mx, l);
@@ -558,14 +559,20 @@ static p2g_progress_event mk(uint32_t kind) {
 }
 
 // ---------------------------------------------------------------------------
-// File reading into pinned host memory
+// Input files: mapped read-only (like scan_via_mmap, src/source.rs:145-232),
+// so the whole-file hash threads start on the page cache at once and the
+// upload copies from the mapping; no staging copy, no pinning of the input.
+// Files that cannot be mapped are read into pinned memory instead.
 // ---------------------------------------------------------------------------
 struct HostFile {
     std::string path;
     uint64_t length = 0;
-    uint8_t* data = nullptr;  // pinned
+    uint8_t* data = nullptr;  // mapping, or pinned copy when !mapped
+    size_t map_len = 0;
+    bool mapped = false;
     ~HostFile() {
-        if (data) cudaFreeHost(data);
+        if (data && mapped) munmap(data, map_len);
+        else if (data) cudaFreeHost(data);
     }
 };
 static p2g_status stat_len(const char* path, uint64_t* len) {
@@ -580,6 +587,17 @@ static p2g_status read_file(HostFile& hf, uint64_t max_bytes) {
     struct stat sb;
     fstat(fd, &sb);
     hf.length = std::min<uint64_t>((uint64_t)sb.st_size, max_bytes);
+    if (S_ISREG(sb.st_mode) && hf.length > 0 && !getenv("P2G_NO_MMAP")) {
+        void* m = mmap(nullptr, hf.length, PROT_READ, MAP_PRIVATE, fd, 0);
+        if (m != MAP_FAILED) {
+            madvise(m, hf.length, MADV_SEQUENTIAL);
+            close(fd);
+            hf.data = static_cast<uint8_t*>(m);
+            hf.map_len = hf.length;
+            hf.mapped = true;
+            return P2G_OK;
+        }
+    }
     if (cudaHostAlloc((void**)&hf.data, std::max<uint64_t>(hf.length, 1), cudaHostAllocDefault) != cudaSuccess) {
         close(fd);
         cudaGetLastError();
