@@ -19,8 +19,10 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <queue>
+#include <tuple>
 #include <vector>
 
 #include "p2g_host_util.h"
@@ -29,9 +31,14 @@
 namespace p2g {
 namespace {
 
-constexpr double kEncRate = 0.78 * 1.9e6;  // tile-symbol wavefronts per ms per CTA
-constexpr double kBuildCost = 384.0;       // table build per slice, in wavefronts
-constexpr double kChainMs = 7.2e-4;        // one MD5 chain step of 64 bytes
+// Calibrated on the persistent kernel's per-item timeline (538 MB, R 200):
+// a 1027-slice x 1920-symbol item takes 1.49 ms, a folded tail item 15 %
+// more, an accumulating item 4 % more; a scan chain steps 64 bytes in
+// 0.76 us, a packet chain in 0.81 us; CRC32 streams at ~10 GB/s per CTA.
+constexpr double kEncRate = 0.838 * 1.9e6;  // tile-symbol wavefronts per ms per CTA
+constexpr double kBuildCost = 384.0;        // table build per slice, in wavefronts
+constexpr double kChainMs = 7.6e-4;         // one MD5 chain step of 64 bytes
+constexpr double kFoldCost = 1.15, kAccCost = 1.04;
 constexpr double kItemMs = 0.003;          // pop, descriptor loads, pipeline fill
 
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
@@ -52,6 +59,11 @@ struct PlanJob {
     // packet-MD5 chains
     bool scans = true, set_id = true, chains = true;
     uint64_t file_bytes = 0;  // largest file, when whole-file MD5 items run (0: none)
+    // Tail split (single job with chains; the caller zeroes the columns of the
+    // split bands): the encode items of the last split_bands bands are cut
+    // into split_chunks slice ranges that XOR-accumulate into the rows.
+    // split_chunks 0: the caller does not zero, never split.
+    uint32_t split_bands = 0, split_chunks = 0;
 };
 
 double finish_ms(const PlanJob& j) { return est_set_id_ms(j.n) + est_packet_item_ms(j.slice, j.R); }
@@ -86,7 +98,7 @@ void job_bands(const PlanJob& j, uint32_t* band_tiles, uint32_t* n_bands) {
 }
 // one chain segment of every 256-row block over one band's bytes
 inline double chain_ms(const PlanJob& j, uint32_t band_syms) {
-    return ceil(j.R / (double)kChainRows) * md5_ms(2ull * band_syms) + kItemMs;
+    return ceil(j.R / (double)kChainRows) * md5_ms(2ull * band_syms) * 1.07 + kItemMs;
 }
 
 // Items of all jobs in queue order: every job's set-id item (its chains wait
@@ -133,20 +145,26 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
         p.band_items[ji].assign(nb, 0);
         std::vector<uint32_t>& counts = p.band_items[ji];
         JobItems e{0.0, ji, {}};
+        const uint32_t first_split = j.chains && j.split_chunks > 1 && j.split_bands
+                                         ? nb - std::min(nb, j.split_bands) : nb;
         for (uint32_t b = 0; b < nb; ++b) {
             const uint32_t t0 = b * bt, t1 = std::min(j.tiles, t0 + bt);
-            for (uint32_t t = t0; t < t1; ++t) {
-                const uint32_t n0 = t * j.ts, syms = std::min(j.ts, j.Np - n0);
-                for (uint32_t rg = 0; rg + 1 < j.RG; ++rg) {
-                    e.items.push_back({ji, encode_kind(rg, 1, false), n0, (b << 16) | syms, 0, 0});
-                    e.key += encode_ms(j, syms);
+            const uint32_t C = b >= first_split ? j.split_chunks : 1;
+            const uint32_t cs = (j.S + C - 1) / C;
+            auto push = [&](uint32_t rg, uint32_t fold, uint32_t n0, uint32_t syms) {
+                for (uint32_t s0 = 0; s0 < j.S; s0 += cs) {
+                    const uint32_t sn = C > 1 ? std::min(cs, j.S - s0) : 0;
+                    e.items.push_back({ji, encode_kind(rg, fold, C > 1), n0, (b << 16) | syms, s0, sn});
+                    e.key += est_encode_item_ms(sn ? sn : j.S, std::min(j.ts, syms));
                     counts[b]++;
                 }
+            };
+            for (uint32_t t = t0; t < t1; ++t) {
+                const uint32_t n0 = t * j.ts, syms = std::min(j.ts, j.Np - n0);
+                for (uint32_t rg = 0; rg + 1 < j.RG; ++rg) push(rg, 1, n0, syms);
                 if ((t - t0) % F == 0) {
                     const uint32_t end = std::min(std::min((t + F) * j.ts, t1 * j.ts), j.Np);
-                    e.items.push_back({ji, encode_kind(j.RG - 1, F, false), n0, (b << 16) | (end - n0), 0, 0});
-                    e.key += encode_ms(j, std::min(j.ts, end - n0));
-                    counts[b]++;
+                    push(j.RG - 1, F, n0, end - n0);
                 }
             }
         }
@@ -176,34 +194,94 @@ double item_ms(const PlanJob& j, const BatchItem& it) {
     case kItemScan: return scan_ms(j, it.b);
     case kItemCrc: return est_crc_item_ms(j.slice, it.b);
     case kItemFileHash: return md5_ms(j.file_bytes) + kItemMs;
-    case kItemEncode: return encode_ms(j, std::min(j.ts, it.b & 0xFFFFu));
+    case kItemEncode: {
+        double ms = est_encode_item_ms(it.sn ? it.sn : j.S, std::min(j.ts, it.b & 0xFFFFu));
+        if ((it.kind_rg >> 24) & 3u) ms *= kFoldCost;
+        if (it.kind_rg & kItemAccumulate) ms *= kAccCost;
+        return ms;
+    }
     default: return est_set_id_ms(j.n);
     }
 }
 
-// List-scheduling simulation: each item goes to the CTA that frees first;
-// the CTA that completes a band also advances that band's packet chains.
+// List-scheduling simulation: each item goes to the CTA that frees first.
+// A job's packet chains advance band by band in order: band b's segment
+// starts when the band's last item ends and the previous segment is done.
+// (The advancing CTA's time is charged to it when the chain was waiting for
+// that band; a band that completes while the chain is busy is picked up by
+// the chain's holder.)
 double simulate(const std::vector<PlanJob>& jobs, const Plan& p, uint32_t ctas) {
     std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
     for (uint32_t c = 0; c < ctas; ++c) free_at.push(0.0);
     std::vector<std::vector<uint32_t>> left = p.band_items;
+    std::vector<std::vector<double>> done(jobs.size());
+    for (size_t ji = 0; ji < jobs.size(); ++ji) done[ji].assign(p.band_items[ji].size(), 0.0);
     double end = 0;
     for (const BatchItem& it : p.items) {
         double t = free_at.top();
         free_at.pop();
         const PlanJob& j = jobs[it.job];
         t += item_ms(j, it);
-        if ((it.kind_rg & kItemKindMask) == kItemEncode && !left[it.job].empty() &&
-            --left[it.job][it.b >> 16] == 0)
-            t += chain_ms(j, p.band_syms[it.job]);
+        if ((it.kind_rg & kItemKindMask) == kItemEncode && !left[it.job].empty()) {
+            const uint32_t b = it.b >> 16;
+            done[it.job][b] = std::max(done[it.job][b], t);
+            --left[it.job][b];
+        }
         end = std::max(end, t);
         free_at.push(t);
+    }
+    for (size_t ji = 0; ji < jobs.size(); ++ji) {
+        double chain = 0;
+        for (double d : done[ji]) chain = std::max(chain, d) + chain_ms(jobs[ji], p.band_syms[ji]);
+        end = std::max(end, chain);
     }
     return end;
 }
 
+Plan plan_tiles(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags);
+
+// A job alone with packet chains: its items run in rounds of equal length,
+// so several bands complete together at the end of each round and the last
+// round leaves the chains a burst of bands to hash after the encode is done.
+// Cutting the items of the last bands into slice ranges spreads their
+// completions out; the simulation picks how many bands and how many pieces.
 Plan plan_batch(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
+    Plan best = plan_tiles(jobs, ctas, flags);
+    if (jobs.size() != 1 || !jobs[0].split_chunks || !jobs[0].chains || !jobs[0].R ||
+        (flags & P2G_BATCH_NO_AUTOTUNE))
+        return best;
+    PlanJob& j = jobs[0];
+    const uint32_t nb = (uint32_t)best.band_items[0].size();
+    if (nb < 2) {
+        j.split_bands = 0;
+        j.split_chunks = 1;
+        return best;
+    }
+    const uint32_t per_band = std::max(1u, best.band_items[0][0]);
+    const uint32_t wave = std::max(1u, (ctas + per_band - 1) / per_band);
+    uint32_t bb = 0, bc = 1;
+    for (uint32_t bands : {wave, 2 * wave, 3 * wave, 4 * wave, nb / 2, nb}) {
+        for (uint32_t chunks : {2u, 4u, 8u}) {
+            j.split_bands = std::min(bands, nb);
+            j.split_chunks = chunks;
+            Plan p = build_items(jobs);
+            p.makespan = simulate(jobs, p, ctas);
+            if (p.makespan < best.makespan * 0.995) {
+                best = std::move(p);
+                bb = j.split_bands;
+                bc = chunks;
+            }
+        }
+    }
+    j.split_bands = bb;
+    j.split_chunks = bc;
+    return best;
+}
+
+Plan plan_tiles(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
     for (PlanJob& j : jobs) {
+        j.split_bands = 0;  // tiles are chosen unsplit
+
         j.RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
         j.Np = (uint32_t)(round_up(j.slice, 16) / 2);
         j.finish = finish_ms(j);
@@ -269,8 +347,8 @@ double est_scan_item_ms(uint64_t slice, uint32_t count) {
     (void)count;  // the lanes run their chains side by side
     return md5_ms(slice) + kItemMs;
 }
-// CRC32 streams from DRAM at ~8 GB/s per SM (16 warps)
-double est_crc_item_ms(uint64_t slice, uint32_t count) { return (double)slice * count / 8e6 + kItemMs; }
+// CRC32 streams from DRAM at ~10 GB/s per SM (16 warps)
+double est_crc_item_ms(uint64_t slice, uint32_t count) { return (double)slice * count / 1e7 + kItemMs; }
 double est_set_id_ms(uint32_t files) {
     const double hashes = ceil(files / 256.0) * (md5_ms(P2G_HASH16K_LEN) + md5_ms(24 + 256));
     const double sort = (double)files * files / 512.0 * 4e-6;
@@ -278,8 +356,46 @@ double est_set_id_ms(uint32_t files) {
 }
 double est_packet_item_ms(uint64_t slice, uint32_t rows) { return ceil(rows / 256.0) * md5_ms(36 + slice) + kItemMs; }
 
+// Plans depend only on the job's shape, and the search (tilings, tail
+// splits, each simulated) costs milliseconds of host time, so single-job
+// plans are kept per shape: repeated jobs of one shape plan once.
+namespace {
+struct PlanKey {
+    uint64_t slice, file_bytes;
+    uint32_t S, R, n, ctas, flags;
+    bool operator<(const PlanKey& o) const {
+        return std::tie(slice, file_bytes, S, R, n, ctas, flags) <
+               std::tie(o.slice, o.file_bytes, o.S, o.R, o.n, o.ctas, o.flags);
+    }
+};
+std::mutex g_plan_mu;
+std::map<PlanKey, SingleJobPlan> g_plans;
+constexpr size_t kMaxCachedPlans = 256;
+SingleJobPlan plan_single_job_uncached(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans,
+                                       bool set_id, bool chains, uint32_t ctas, uint64_t file_bytes,
+                                       bool split_tail);
+}  // namespace
+
 SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans, bool set_id,
-                              bool chains, uint32_t ctas, uint64_t file_bytes) {
+                              bool chains, uint32_t ctas, uint64_t file_bytes, bool split_tail) {
+    const PlanKey key{slice, file_bytes, S, R, n_files, ctas,
+                      (scans ? 1u : 0u) | (set_id ? 2u : 0u) | (chains ? 4u : 0u) | (split_tail ? 8u : 0u)};
+    {
+        std::lock_guard<std::mutex> lk(g_plan_mu);
+        auto it = g_plans.find(key);
+        if (it != g_plans.end()) return it->second;
+    }
+    SingleJobPlan p = plan_single_job_uncached(slice, S, R, n_files, scans, set_id, chains, ctas, file_bytes, split_tail);
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    if (g_plans.size() >= kMaxCachedPlans) g_plans.clear();
+    g_plans.emplace(key, p);
+    return p;
+}
+
+namespace {
+SingleJobPlan plan_single_job_uncached(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans,
+                                       bool set_id, bool chains, uint32_t ctas, uint64_t file_bytes,
+                                       bool split_tail) {
     std::vector<PlanJob> jobs(1);
     jobs[0].slice = slice;
     jobs[0].S = S;
@@ -289,8 +405,14 @@ SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n
     jobs[0].set_id = set_id;
     jobs[0].chains = chains && R;
     jobs[0].file_bytes = file_bytes;
+    jobs[0].split_chunks = split_tail ? 1 : 0;  // non-zero: the split search may run
     Plan p = plan_batch(jobs, ctas, 0);
     SingleJobPlan out;
+    out.zero_from_sym = jobs[0].Np;
+    if (jobs[0].split_chunks > 1 && jobs[0].split_bands) {
+        const uint32_t nb = (uint32_t)p.band_items[0].size();
+        out.zero_from_sym = (nb - std::min(nb, jobs[0].split_bands)) * p.band_syms[0];
+    }
     out.items = std::move(p.items);
     out.band_items = p.band_items[0];
     out.band_syms = p.band_syms[0];
@@ -298,6 +420,7 @@ SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n
     out.predicted_ms = p.makespan;
     return out;
 }
+}  // namespace
 
 // ---------------------------------------------------------------------------
 // The batch object

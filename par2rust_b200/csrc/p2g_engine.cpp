@@ -296,8 +296,15 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     const bool sid_item = !j.have_set_id;
     uint64_t max_len = 0;
     for (const auto& f : j.files) max_len = std::max(max_len, f.length);
+    // the last bands' items may be cut into accumulating slice ranges (the
+    // columns they write are zeroed below); P2G_TAIL_SPLIT=0 turns that off
+    static const bool split_tail = [] {
+        const char* e = getenv("P2G_TAIL_SPLIT");
+        return !(e && !strcmp(e, "0"));
+    }();
     const SingleJobPlan pl = plan_single_job(j.slice, j.S, j.R && j.S ? j.R : 0, n, j.d_checks != nullptr, sid_item,
-                                             chains, (uint32_t)device_sm_count(), j.d_hfull ? max_len : 0);
+                                             chains, (uint32_t)device_sm_count(), j.d_hfull ? max_len : 0,
+                                             split_tail);
     const uint32_t nb = (uint32_t)pl.band_items.size();
     const uint32_t Q = (j.R + kChainRows - 1) / kChainRows;
     const uint64_t ctl_words = 1 + (chains ? nb + 2 * Q + 1 : 0) + 1;  // head, chain state, error word
@@ -387,6 +394,10 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
                                    cudaMemcpyHostToDevice, st));
         }
     }
+    const uint64_t np_bytes = round_up(j.slice, 16);
+    if (j.R && j.S && 2ull * pl.zero_from_sym < np_bytes)
+        P2G_CU(cudaMemset2DAsync(j.d_rec + 2ull * pl.zero_from_sym, j.rec_stride, 0,
+                                 np_bytes - 2ull * pl.zero_from_sym, j.R, st));
     if (d.basis) P2G_CU(launch_basis(c.basis.as<uint16_t>(), j.S, RG, j.R, j.first_exp, st));
     if (esrc != j.d_src) P2G_CU(launch_realign(j.d_src, j.slice, c.src_al.as<uint8_t>(), estride, j.S, j.slice, st));
     P2G_CU(launch_batch(reinterpret_cast<const BatchJob*>(D + o_desc), reinterpret_cast<const BatchItem*>(D + o_items),

@@ -191,11 +191,16 @@ struct SingleJobPlan {
     std::vector<BatchItem> items;    // job index 0
     std::vector<uint32_t> band_items;  // empty: no chains
     uint32_t band_syms = 0, ts = 0;
+    // recovery columns [zero_from_sym, Np) are written by XOR-accumulating
+    // items: the caller zeroes them first (Np: none)
+    uint32_t zero_from_sym = 0;
     double predicted_ms = 0;
 };
-// file_bytes: largest file (non-zero: whole-file MD5 items, 256 files each)
+// file_bytes: largest file (non-zero: whole-file MD5 items, 256 files each);
+// split_tail: the caller zeroes the columns from zero_from_sym, so the last
+// bands' encode items may be cut into accumulating slice ranges.
 SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans, bool set_id,
-                              bool chains, uint32_t ctas, uint64_t file_bytes = 0);
+                              bool chains, uint32_t ctas, uint64_t file_bytes = 0, bool split_tail = false);
 // Shared memory of one batch CTA.
 size_t batch_smem_bytes();
 // Fills every job's basis (one launch; blockIdx.y = job).
