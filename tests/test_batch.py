@@ -55,12 +55,13 @@ def test_plan_counts_items(p2g):
 
 def test_plan_autotune_splits_tiles_of_a_lone_job(p2g):
     # one job, 1 row group, 16 tiles of 2048: 16 of 148 CTAs busy; finer tiles
-    # spread it wider and the simulated makespan must drop
+    # spread it wider and the simulated makespan must drop by a quarter or
+    # more (not in proportion: every slice of a tile also pays a fixed cost)
     shapes = [(65536, 2000, 20, 1)]
     base, t0 = p2g.batch_plan(shapes, ctas=148, flags=p2g.BATCH_NO_AUTOTUNE)
     tuned, t1 = p2g.batch_plan(shapes, ctas=148)
     assert t0 == [2048] and t1[0] < 2048
-    assert tuned.predicted_ms < 0.6 * base.predicted_ms
+    assert tuned.predicted_ms < 0.75 * base.predicted_ms
     assert tuned.encode_items > base.encode_items
 
 
