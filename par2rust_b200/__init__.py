@@ -688,6 +688,88 @@ class Batch:
             pass
 
 
+class StagedBatch:
+    """Batched create for jobs whose sources sit in pinned host memory.
+
+    The jobs are cut into ``groups`` consecutive batches of about equal
+    source bytes (the first one half as large, so the device starts early).
+    All uploads are queued at once on a copy stream; group g's batch launches
+    on the compute stream when its own uploads are done.  So group g+1's
+    sources cross PCIe while group g runs.  Each group's outputs download on a
+    third stream as soon as that group ends.  Outputs equal one Batch over all
+    jobs.
+
+    ``hosts[i]`` is job i's pinned source (its first ``hosts[i].numel()``
+    bytes go to ``jobs[i].src``).  ``outputs[i]``, when given, is a tuple of
+    pinned tensors (recovery, checksums, packet_md5, hash16k, set_id) that
+    receive the job's device buffers of the same names.
+    """
+
+    def __init__(self, jobs: Sequence[BatchJobSpec], hosts: Sequence[object], outputs=None, groups: int = 4,
+                 flags: int = 0):
+        import torch
+
+        if len(hosts) != len(jobs) or (outputs is not None and len(outputs) != len(jobs)):
+            raise InvalidArgument("one pinned source (and output set) per job")
+        groups = max(1, min(int(groups), len(jobs)))
+        sizes = [int(h.numel()) for h in hosts]
+        total = max(1, sum(sizes))
+        # group k ends where the cumulative bytes pass its share (first share halved)
+        shares = [0.5] + [1.0] * (groups - 1)
+        bounds, acc, k, edge = [], 0, 0, shares[0] / sum(shares) * total
+        for i, n in enumerate(sizes):
+            acc += n
+            if acc >= edge and k < groups - 1 and i + 1 < len(jobs):
+                bounds.append(i + 1)
+                k += 1
+                edge += shares[k] / sum(shares) * total
+        bounds = [0] + bounds + [len(jobs)]
+        self.ranges = [(a, b) for a, b in zip(bounds, bounds[1:]) if b > a]
+        self.jobs, self.hosts, self.outputs = list(jobs), list(hosts), outputs
+        self.batches = [Batch(self.jobs[a:b], flags) for a, b in self.ranges]
+        self._up = torch.cuda.Stream()
+        self._down = torch.cuda.Stream()
+
+    def launch(self, stream: Optional[int] = None) -> None:
+        """Enqueue uploads, launches and downloads; the caller synchronises."""
+        import torch
+
+        comp = torch.cuda.current_stream() if stream is None else torch.cuda.ExternalStream(stream)
+        self._up.wait_stream(comp)  # the previous run's readers of the sources are done
+        uploaded = []
+        with torch.cuda.stream(self._up):
+            for a, b in self.ranges:
+                for i in range(a, b):
+                    n = self.hosts[i].numel()
+                    self.jobs[i].src.view(-1)[:n].copy_(self.hosts[i].view(-1), non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self._up)
+                uploaded.append(ev)
+        for (a, b), batch, ev in zip(self.ranges, self.batches, uploaded):
+            comp.wait_event(ev)
+            batch.launch(comp.cuda_stream)
+            if self.outputs is None:
+                continue
+            done = torch.cuda.Event()
+            done.record(comp)
+            self._down.wait_event(done)
+            with torch.cuda.stream(self._down):
+                for i in range(a, b):
+                    bf = self.jobs[i].bufs
+                    for t, d in zip(self.outputs[i], (bf.recovery, bf.checksums, bf.packet_md5, bf.hash16k,
+                                                      bf.set_id_device)):
+                        t.copy_(d, non_blocking=True)
+        comp.wait_stream(self._down)
+
+    def check(self) -> None:
+        for b in self.batches:
+            b.check()
+
+    def close(self) -> None:
+        for b in self.batches:
+            b.close()
+
+
 # ---------------------------------------------------------------------------
 # Serving loop (no counterpart in the reference): continuous batching of
 # create requests on the device.

@@ -239,6 +239,49 @@ def test_batch_job_alone_equals_in_mix(p2g, gpu, batch_jobs):
 
 
 @pytest.mark.gpu
+def test_staged_batch_from_host_equals_batch(p2g, gpu, batch_jobs):
+    """Sources uploaded group by group beside the running groups: every
+    output must equal one Batch over all jobs, on two runs in a row."""
+    import torch
+
+    specs = [j for j, _, _ in batch_jobs]
+    ref = p2g.Batch(specs)
+    ref.launch()
+    torch.cuda.synchronize()
+    ref.check()
+    want = [_outputs(j) for j in specs]
+    ref.close()
+    hosts = [torch.from_numpy(h).pin_memory() for _, _, h in batch_jobs]
+    outs = [tuple(torch.empty(t.numel(), dtype=torch.uint8).pin_memory()
+                  for t in (j.bufs.recovery, j.bufs.checksums, j.bufs.packet_md5, j.bufs.hash16k,
+                            j.bufs.set_id_device)) for j in specs]
+    staged = p2g.StagedBatch(specs, hosts, outs, groups=3)
+    assert len(staged.ranges) >= 2 and staged.ranges[0][0] == 0 and staged.ranges[-1][1] == len(specs)
+    assert all(a < b and b == c for (a, b), (c, _) in zip(staged.ranges, staged.ranges[1:]))
+    for _ in range(2):
+        for j in specs:  # the device copies must come from the host sources
+            j.src.fill_(0x5A)
+            for t in (j.bufs.recovery, j.bufs.checksums, j.bufs.packet_md5, j.bufs.hash16k, j.bufs.set_id_device):
+                t.fill_(0xA5)
+        for o in outs:
+            for t in o:
+                t.fill_(0)
+        staged.launch()
+        torch.cuda.synchronize()
+        staged.check()
+        for k, (j, w, o) in enumerate(zip(specs, want, outs)):
+            S, R, n = j.input_slices, j.recovery_count, len(j.file_lengths)
+            assert o[1][:20 * S].numpy().tobytes() == w["checks"].tobytes(), k
+            assert o[3][:16 * n].numpy().tobytes() == w["h16k"].tobytes(), k
+            assert o[4].numpy().tobytes() == w["set_id"], k
+            if R:
+                rec = o[0].view(-1, j.bufs.rec_stride)[:R, :j.slice_size].numpy()
+                assert (rec == w["rec"]).all(), k
+                assert o[2][:16 * R].numpy().tobytes() == w["pkt"].tobytes(), k
+    staged.close()
+
+
+@pytest.mark.gpu
 def test_batch_graph_replay_direct_launch_and_derived_basis_agree(p2g, gpu, batch_jobs):
     import torch
 
