@@ -8,7 +8,8 @@ Exponential volume split.
   value      device-resident step: the source already in HBM; one step is the
              device work of one create job -- coefficient basis + Reed-Solomon
              encode + per-slice MD5/CRC32 + hash16k + recovery-packet MD5
-             (the whole-file MD5 chain is reported separately).
+             (the whole-file MD5 chain is one serial stream; it is timed
+             separately as file_md5_device_chain_gbs and counted in e2e).
              Timed with CUDA events on the launching stream; max over ranks.
   e2e        the same metric through the public API (p2g_create_in_memory):
              pinned host source -> H2D -> device job -> whole-file MD5 ->
