@@ -144,34 +144,44 @@ __device__ __forceinline__ uint32_t lds32(uint32_t addr) {
 // fold > 1: the last row group's rows repeat its first 32/fold rows (the
 // layout a folded encode CTA builds its replicated tables from; an unfolded
 // CTA only stores rows < R, which are the same either way).
+//
+// One warp per (s, rg) block, lane = table row: one exponent and one antilog
+// lookup per row give c, then c*2^(j+1) = (c*2^j)*2, a shift that folds the
+// generator polynomial 0x1100B back in when bit 15 falls off.  Each store of
+// the warp writes 32 consecutive u16 (one 64-byte run).
 __device__ __forceinline__ void basis_fill(uint16_t* __restrict__ basis, uint32_t S, uint32_t RG, uint32_t R,
-                                           uint32_t first_exp, uint64_t start, uint64_t step, uint32_t fold = 1) {
-    const uint64_t total = (uint64_t)S * RG * 512;
-    for (uint64_t idx = start; idx < total; idx += step) {
-        const uint32_t rl = (uint32_t)(idx & 31);
-        const uint32_t hi = (uint32_t)((idx >> 5) & 1);
-        const uint32_t jj = (uint32_t)((idx >> 6) & 7);
-        const uint32_t j = 8 * hi + jj;
-        const uint64_t sg = idx >> 9;
+                                           uint32_t first_exp, uint64_t warp_start, uint64_t warp_step,
+                                           uint32_t fold = 1) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t blocks = (uint64_t)S * RG;
+    for (uint64_t sg = warp_start; sg < blocks; sg += warp_step) {
         const uint32_t rg = (uint32_t)(sg % RG);
         const uint32_t s = (uint32_t)(sg / RG);
-        const uint32_t r = rg * kRowsPerGroup + (rg + 1 == RG ? rl & (31u >> (fold >> 1)) : rl);
-        uint16_t v = 0;
+        const uint32_t r = rg * kRowsPerGroup + (rg + 1 == RG ? lane & (31u >> (fold >> 1)) : lane);
+        uint32_t v = 0;
         if (r < R) {
-            const uint32_t e = first_exp + r;
-            const uint32_t L = (uint32_t)(((uint64_t)d_logbase[s] * e) % kFieldLimit);
-            uint32_t k = L + j;
-            if (k >= kFieldLimit) k -= kFieldLimit;
-            v = d_antilog[k];
+            // logbase * e < 2^33; 2^32 = 1 (mod 65535), so fold the high word in
+            const uint64_t p = (uint64_t)d_logbase[s] * (first_exp + r);
+            uint32_t x = (uint32_t)p;
+            x = (x & 0xFFFFu) + (x >> 16);
+            x = (x & 0xFFFFu) + (x >> 16) + (uint32_t)(p >> 32);
+            x = (x & 0xFFFFu) + (x >> 16);
+            if (x >= kFieldLimit) x -= kFieldLimit;
+            v = d_antilog[x];
         }
-        basis[idx] = v;
+        uint16_t* out = basis + sg * 512 + lane;
+#pragma unroll
+        for (uint32_t j = 0; j < 16; ++j) {
+            out[((j & 7u) * 2u + (j >> 3)) * 32u] = (uint16_t)v;
+            v = ((v << 1) & 0xFFFFu) ^ ((v & 0x8000u) ? 0x100Bu : 0u);
+        }
     }
 }
 
 __global__ void basis_kernel(uint16_t* __restrict__ basis, uint32_t S, uint32_t RG, uint32_t R,
                              uint32_t first_exp, uint32_t fold) {
-    basis_fill(basis, S, RG, R, first_exp, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
-               (uint64_t)gridDim.x * blockDim.x, fold);
+    basis_fill(basis, S, RG, R, first_exp, ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+               ((uint64_t)gridDim.x * blockDim.x) >> 5, fold);
 }
 
 // ---------------------------------------------------------------------------
@@ -1420,8 +1430,8 @@ __global__ void basis_batch_kernel(const BatchJob* __restrict__ jobs) {
     // the last row group replicated as the folded encode items build it (tail_fold)
     const uint32_t tail = J.R - (J.R - 1) / kRowsPerGroup * kRowsPerGroup;
     const uint32_t fold = tail <= 8 ? 4u : tail <= 16 ? 2u : 1u;
-    basis_fill(J.basis, J.S, J.RG, J.R, J.first_exp, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
-               (uint64_t)gridDim.x * blockDim.x, fold);
+    basis_fill(J.basis, J.S, J.RG, J.R, J.first_exp, ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+               ((uint64_t)gridDim.x * blockDim.x) >> 5, fold);
 }
 
 // ---------------------------------------------------------------------------
@@ -1482,9 +1492,9 @@ void choose_tiles(uint32_t Np, uint32_t RG, uint32_t sms, uint32_t* ts_out, uint
 
 cudaError_t launch_basis(uint16_t* basis, uint32_t S, uint32_t RG, uint32_t R, uint32_t first_exp,
                          cudaStream_t st) {
-    const uint64_t total = (uint64_t)S * RG * 512;
+    const uint64_t total = (uint64_t)S * RG;  // 1 KiB blocks, one warp each
     if (!total) return cudaSuccess;
-    const uint64_t want = (total + 255) / 256;
+    const uint64_t want = (total + 7) / 8;
     const unsigned blocks = (unsigned)(want < (uint64_t)sm_count() * 16 ? want : (uint64_t)sm_count() * 16);
     basis_kernel<<<blocks, 256, 0, st>>>(basis, S, RG, R, first_exp, tail_fold(R));
     count_launch();
@@ -1773,7 +1783,7 @@ int device_sm_count() { return sm_count(); }
 
 cudaError_t launch_basis_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_words, cudaStream_t st) {
     if (!n_jobs || !max_words) return cudaSuccess;
-    const uint64_t want = (max_words + 255) / 256;
+    const uint64_t want = (max_words / 512 + 7) / 8;  // one warp per 1 KiB block
     const unsigned bx = (unsigned)(want < (uint64_t)sm_count() * 4 ? want : (uint64_t)sm_count() * 4);
     basis_batch_kernel<<<dim3(bx, n_jobs), 256, 0, st>>>(jobs);
     count_launch();
