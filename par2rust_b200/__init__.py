@@ -688,6 +688,26 @@ class Batch:
             pass
 
 
+def staged_groups(sizes: Sequence[int], groups: int) -> List[Tuple[int, int]]:
+    """Consecutive job ranges [a, b) for StagedBatch: about equal source bytes
+    per group, the first group half as large; a job is never split, so a
+    single large job can leave fewer groups than asked."""
+    n = len(sizes)
+    groups = max(1, min(int(groups), n))
+    total = max(1, sum(sizes))
+    shares = [0.5] + [1.0] * (groups - 1)
+    unit = total / sum(shares)
+    bounds, acc, k, edge = [], 0, 0, shares[0] * unit
+    for i, sz in enumerate(sizes):
+        acc += sz
+        if acc >= edge and k < groups - 1 and i + 1 < n:
+            bounds.append(i + 1)
+            k += 1
+            edge += shares[k] * unit
+    bounds = [0] + bounds + [n]
+    return [(a, b) for a, b in zip(bounds, bounds[1:]) if b > a]
+
+
 class StagedBatch:
     """Batched create for jobs whose sources sit in pinned host memory.
 
@@ -711,20 +731,7 @@ class StagedBatch:
 
         if len(hosts) != len(jobs) or (outputs is not None and len(outputs) != len(jobs)):
             raise InvalidArgument("one pinned source (and output set) per job")
-        groups = max(1, min(int(groups), len(jobs)))
-        sizes = [int(h.numel()) for h in hosts]
-        total = max(1, sum(sizes))
-        # group k ends where the cumulative bytes pass its share (first share halved)
-        shares = [0.5] + [1.0] * (groups - 1)
-        bounds, acc, k, edge = [], 0, 0, shares[0] / sum(shares) * total
-        for i, n in enumerate(sizes):
-            acc += n
-            if acc >= edge and k < groups - 1 and i + 1 < len(jobs):
-                bounds.append(i + 1)
-                k += 1
-                edge += shares[k] / sum(shares) * total
-        bounds = [0] + bounds + [len(jobs)]
-        self.ranges = [(a, b) for a, b in zip(bounds, bounds[1:]) if b > a]
+        self.ranges = staged_groups([int(h.numel()) for h in hosts], groups)
         self.jobs, self.hosts, self.outputs = list(jobs), list(hosts), outputs
         self.batches = [Batch(self.jobs[a:b], flags) for a, b in self.ranges]
         self._up = torch.cuda.Stream()

@@ -76,6 +76,24 @@ def test_plan_large_batch_is_near_its_bound(p2g):
     assert 250 < info.predicted_ms < 400
 
 
+def test_staged_groups_cover_jobs_in_order(p2g):
+    # equal jobs: the first group gets about half of the others' share
+    r = p2g.staged_groups([10] * 70, 4)
+    assert r == [(0, 10), (10, 30), (30, 50), (50, 70)]
+    # every split covers all jobs once, in order, without empty groups
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        sizes = list(rng.integers(1, 1000, rng.integers(1, 40)))
+        g = int(rng.integers(1, 6))
+        r = p2g.staged_groups(sizes, g)
+        assert r[0][0] == 0 and r[-1][1] == len(sizes) and 1 <= len(r) <= min(g, len(sizes))
+        assert all(a < b for a, b in r) and all(b == c for (_, b), (c, _) in zip(r, r[1:]))
+    # one job holding most bytes cannot be split
+    assert p2g.staged_groups([1, 1, 1000], 4) == [(0, 3)]
+    assert p2g.staged_groups([1000, 1, 1], 3) == [(0, 1), (1, 2), (2, 3)]
+    assert p2g.staged_groups([5], 4) == [(0, 1)]
+
+
 def test_plan_rejects_bad_shapes(p2g):
     with pytest.raises(p2g.InvalidSliceSize):
         p2g.batch_plan([(4098, 10, 5, 1)])
