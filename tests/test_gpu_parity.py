@@ -141,6 +141,11 @@ CREATE_CASES = [
     ("explicit-unicode", [(b"x", rnd(4, 20000).tobytes())], 2048, 6, "explicit", 0, [2, 3, 1], ["trés", "ok"]),
     ("limited", [(b"y", rnd(5, 9000).tobytes())], 512, 20, "limited", 3, None, []),
     ("odd-slice", [(b"z", rnd(6, 1001).tobytes()), (b"w", rnd(7, 77).tobytes())], 20, 37, "single", 0, None, []),
+    # the limits: 32,768 input slices; 65,535 recovery blocks; thousands of files
+    ("max-input-slices", [(b"maxs.bin", rnd(8, 131072).tobytes())], 4, 3, "single", 0, None, []),
+    ("max-recovery", [(b"maxr.bin", rnd(9, 40).tobytes())], 4, 65535, "exponential", 0, None, []),
+    ("many-files", [(f"f{i:04d}.dat".encode(), rnd(100 + i, 1 + (i * 37) % 200).tobytes()) for i in range(3000)],
+     64, 10, "uniform", 4, None, []),
 ]
 
 
