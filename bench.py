@@ -919,6 +919,10 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, _ = cpu_baseline(host_src.numpy(), wl, target_s=args.cpu_seconds)
+        # and on one core, on a shorter sample (the scalar chains set the pace)
+        c1, _ = cpu_baseline(host_src.numpy(), wl, target_s=max(2.0, args.cpu_seconds / 4), threads=1)
+        cb["one_thread"] = {"value": c1["value"], "unit": c1["unit"], "seconds_per_step": c1["seconds_per_step"],
+                            "sample": c1["sample"]}
 
     if world > 1:
         dist.barrier()
