@@ -78,7 +78,46 @@ def parse():
                     help="profiling aid: run only the device-job steps (no JSON line)")
     ap.add_argument("--only-encode", action="store_true",
                     help="profiling aid: run only the single-launch encode kernel loop (no JSON line)")
+    ap.add_argument("--int8-ceiling", action="store_true",
+                    help="print the library int8 / bf16 GEMM rates on this GPU and the GF(2^16) MAC ceiling "
+                         "that a bit-sliced int8 tensor-core encode could reach (int8 ops / 512)")
     return ap.parse_args()
+
+
+def int8_ceiling():
+    """A bit-sliced GF(2^16) product spends 16 x 16 binary products, i.e. 512
+    int8 tensor ops, on every GF MAC, so the best int8 GEMM rate / 512 bounds
+    any tensor-core form of the encode (before its operand expansion and
+    parity reduction).  Timed with CUDA events on cuBLAS (torch._int_mm)."""
+    import torch
+
+    dev = torch.device("cuda:0")
+    out = {"metric": "int8 tensor-core ceiling for the GF(2^16) encode", "int8": [], "unit": "GF(2^16) MAC/s"}
+
+    def timed(fn, n=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    for M, N, K in [(8192, 8192, 8192), (16384, 16384, 8192), (4096, 16384, 16384)]:
+        x = torch.randint(-128, 127, (M, K), dtype=torch.int8, device=dev)
+        y = torch.randint(-128, 127, (K, N), dtype=torch.int8, device=dev).t().contiguous().t()
+        ms = timed(lambda: torch._int_mm(x, y))
+        tops = 2 * M * N * K / (ms * 1e-3)
+        out["int8"].append({"shape": [M, N, K], "ms": ms, "tops": tops / 1e12, "gf_mac_ceiling": tops / 512})
+    x = torch.randn(8192, 8192, dtype=torch.bfloat16, device=dev)
+    ms = timed(lambda: x @ x)
+    out["bf16_tflops"] = 2 * 8192 ** 3 / (ms * 1e-3) / 1e12
+    out["value"] = max(r["gf_mac_ceiling"] for r in out["int8"])
+    print(json.dumps(out))
+    return 0
 
 
 def dist_env():
@@ -698,6 +737,8 @@ def run_batch(args, wl):
 
 def main():
     args = parse()
+    if args.int8_ceiling:
+        return int8_ceiling()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         if wl.get("serve"):
