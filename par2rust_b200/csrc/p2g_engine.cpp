@@ -1458,10 +1458,17 @@ extern "C" p2g_status p2g_create_in_memory(const p2g_create_options* opts, const
     const WhileHashing lay_out = [&](const CreateOutput& o, size_t clen) {
         crit_len = clen;
         uint32_t first = 0;
-        std::vector<uint8_t> headers;
+        std::vector<std::vector<uint8_t>> headers(vs.size());
         std::vector<std::pair<const uint8_t*, size_t>> pieces;
+        struct Copy {
+            uint8_t* dst;
+            const uint8_t* src;
+            size_t len;
+        };
+        std::vector<Copy> copies;
+        size_t bytes = 0;
         for (size_t v = 0; v < vs.size() && vols_ok; ++v) {
-            volume_pieces_recovery(o, slice, first, vs[v], headers, pieces);
+            volume_pieces_recovery(o, slice, first, vs[v], headers[v], pieces);
             size_t tot = 2 * clen;
             for (auto& p : pieces) tot += p.second;
             p2g_output_file& of = vols[v];
@@ -1474,11 +1481,30 @@ extern "C" p2g_status p2g_create_in_memory(const p2g_create_options* opts, const
             }
             size_t at = clen;
             for (auto& p : pieces) {
-                memcpy(of.data + at, p.first, p.second);
+                copies.push_back({of.data + at, p.first, p.second});
                 at += p.second;
+                bytes += p.second;
             }
             first += vs[v];
         }
+        if (!vols_ok) return;
+        // hundreds of MB for large recovery sets: copy in ~4 MB pieces on a
+        // few threads (one core may still be hashing whole files)
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const unsigned nt = (unsigned)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, bytes >> 24));
+        std::atomic<size_t> next{0};
+        constexpr size_t kPiece = 4u << 20;
+        auto worker = [&]() {
+            for (size_t i = next++; i < copies.size(); i = next++) {
+                const Copy& cp = copies[i];
+                for (size_t off = 0; off < cp.len; off += kPiece)
+                    memcpy(cp.dst + off, cp.src + off, std::min(kPiece, cp.len - off));
+            }
+        };
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < nt; ++t) th.emplace_back(worker);
+        worker();
+        for (auto& t : th) t.join();
     };
     const p2g_status st = device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co,
                                         rec, &lay_out);
