@@ -1214,6 +1214,48 @@ extern "C" p2g_status p2g_scan_with_progress(const char* path, const uint8_t* di
     return scan_impl(path, display_name, name_len, slice_size, cb, user, out);
 }
 
+// Writes the volume files of an already computed set on up to 8 threads (the
+// reference writes volumes in parallel too, src/creator.rs:296-314); events
+// follow in volume order.  On failure the volumes before the first failing
+// one are reported written and its error is returned.
+static p2g_status write_volumes(const std::string& output, const CreateOutput& co, uint64_t slice,
+                                p2g_progress_fn cb, void* user, std::vector<std::string>& written) {
+    const size_t nv = co.vol_sizes.size();
+    std::vector<std::string> paths(nv);
+    std::vector<uint32_t> firsts(nv);
+    uint32_t first = 0;
+    for (size_t v = 0; v < nv; ++v) {
+        firsts[v] = first;
+        paths[v] = volume_filename(output, (uint16_t)first, co.vol_sizes[v]);
+        first += co.vol_sizes[v];
+    }
+    std::vector<p2g_status> st(nv, P2G_OK);
+    std::vector<std::string> msg(nv);
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+        std::vector<uint8_t> headers;
+        std::vector<std::pair<const uint8_t*, size_t>> pieces;
+        for (size_t v = next++; v < nv; v = next++) {
+            volume_pieces(co, slice, firsts[v], co.vol_sizes[v], headers, pieces);
+            st[v] = write_atomic(paths[v], pieces);
+            if (st[v] != P2G_OK) msg[v] = p2g_last_error_message();
+        }
+    };
+    const unsigned nt = (unsigned)std::min<size_t>(std::min(8u, std::max(1u, std::thread::hardware_concurrency())), nv);
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(worker);
+    worker();
+    for (auto& t : th) t.join();
+    for (size_t v = 0; v < nv; ++v) {
+        if (st[v] != P2G_OK) return set_error(st[v], "%s", msg[v].c_str());
+        p2g_progress_event ev = mk(P2G_EV_VOLUME_WRITTEN);
+        ev.path = paths[v].c_str();
+        emit(cb, user, ev);
+        written.push_back(paths[v]);
+    }
+    return P2G_OK;
+}
+
 // Writes the index and (if R > 0) volume files of an already computed set.
 static p2g_status write_outputs(const p2g_create_options& o, const CreateOutput& co, uint32_t R, uint64_t slice,
                                 p2g_progress_fn cb, void* user, std::vector<std::string>& written) {
@@ -1224,19 +1266,7 @@ static p2g_status write_outputs(const p2g_create_options& o, const CreateOutput&
     emit(cb, user, ev);
     written.push_back(o.output);
     if (!R) return P2G_OK;
-    uint32_t first = 0;
-    std::vector<uint8_t> headers;
-    for (uint32_t cnt : co.vol_sizes) {
-        const std::string vp = volume_filename(o.output, (uint16_t)first, cnt);
-        volume_pieces(co, slice, first, cnt, headers, pieces);
-        P2G_TRY(write_atomic(vp, pieces));
-        ev = mk(P2G_EV_VOLUME_WRITTEN);
-        ev.path = vp.c_str();
-        emit(cb, user, ev);
-        written.push_back(vp);
-        first += cnt;
-    }
-    return P2G_OK;
+    return write_volumes(o.output, co, slice, cb, user, written);
 }
 
 static void emit_encode_events(p2g_progress_fn cb, void* user, uint64_t S, uint32_t R, bool completed) {
@@ -1304,19 +1334,7 @@ static p2g_status run_create_impl(const p2g_create_options* opts, const p2g_sour
         emit_encode_events(cb, user, S, R, true);
         co.rec_host = enc.rec_host;
         co.pkt_md5 = std::move(enc.pkt_md5);
-        uint32_t first = 0;
-        std::vector<uint8_t> headers;
-        std::vector<std::pair<const uint8_t*, size_t>> pieces;
-        for (uint32_t cnt : co.vol_sizes) {
-            const std::string vp = volume_filename(opts->output, (uint16_t)first, cnt);
-            volume_pieces(co, slice, first, cnt, headers, pieces);
-            P2G_TRY(write_atomic(vp, pieces));
-            p2g_progress_event ev = mk(P2G_EV_VOLUME_WRITTEN);
-            ev.path = vp.c_str();
-            emit(cb, user, ev);
-            written.push_back(vp);
-            first += cnt;
-        }
+        P2G_TRY(write_volumes(opts->output, co, slice, cb, user, written));
     }
     fill_path_list(out, written);
     return P2G_OK;
