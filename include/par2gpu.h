@@ -203,6 +203,15 @@ p2g_status p2g_create_in_memory(const p2g_create_options *opts, const p2g_buffer
                                 uint32_t n, p2g_source_file *sources_out, p2g_output_set *out);
 void p2g_output_set_free(p2g_output_set *os);
 
+/* ---- failure-path check (no counterpart in the reference) ------------
+ * Every device wait in this library is bounded: when a copy or a chain
+ * step it waits for never completes, the kernel gives up, records it, and
+ * the call returns P2G_ERR_TIMEOUT with the device still usable.  This runs
+ * that path on purpose: one block waits on a barrier that nothing ever
+ * completes, for at most `polls` tries (1..2^24), and the call returns
+ * P2G_ERR_TIMEOUT when the bound fired (it always should). */
+p2g_status p2g_check_bounded_wait(uint32_t polls);
+
 /* ---- hot-path seams -------------------------------------------------- */
 
 /* Pointer placement for the seams below. */

@@ -461,6 +461,14 @@ def _host_buffer(data, keep: list) -> Tuple[int, int]:
 # ---------------------------------------------------------------------------
 # Kernel-level seams
 # ---------------------------------------------------------------------------
+def check_bounded_wait(polls: int = 1 << 16) -> None:
+    """Run the library's device-wait failure path on purpose (a barrier that
+    nothing completes, waited for at most ``polls`` tries).  Raises
+    DeviceTimeout, as a job whose copy never lands would; the device stays
+    usable afterwards."""
+    _check(lib().p2g_check_bounded_wait(int(polls)))
+
+
 def gf_mul_xor(coeff: int, input: bytes, output: bytearray) -> None:
     """output ^= coeff * input over LE GF(2^16) symbols (gf_mul_xor_dispatch)."""
     import numpy as np

@@ -264,6 +264,7 @@ SIGNATURES = [
     ("p2g_gf_mul_xor", C.c_int, [C.c_uint16, C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint32, C.c_void_p]),
     ("p2g_encode", C.c_int, [C.POINTER(p2g_encode_job)]),
     ("p2g_encode_noalloc", C.c_int, [C.POINTER(p2g_encode_job)]),
+    ("p2g_check_bounded_wait", C.c_int, [C.c_uint32]),
     ("p2g_slice_checksums", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("p2g_file_hashes", C.c_int,

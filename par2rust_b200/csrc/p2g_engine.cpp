@@ -924,6 +924,23 @@ extern "C" void p2g_output_set_free(p2g_output_set* os) {
     os->count = 0;
 }
 
+extern "C" p2g_status p2g_check_bounded_wait(uint32_t polls) {
+    Context& c = ctx();
+    std::lock_guard<std::recursive_mutex> lk(c.mu);
+    clear_error();
+    if (polls == 0 || polls > (1u << 24)) return set_error(P2G_ERR_INVALID_ARGUMENT, "polls must be in [1, 2^24]");
+    P2G_TRY(ensure_ready(c));
+    cudaStream_t s = c.st[0];
+    P2G_CU(c.err.ensure(sizeof(int)));
+    P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s));
+    P2G_CU(launch_bounded_wait_probe(c.err.as<int>(), polls, s));
+    int gave_up = 0;
+    P2G_CU(cudaMemcpyAsync(&gave_up, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    P2G_CU(cudaStreamSynchronize(s));
+    if (gave_up) return set_error(P2G_ERR_TIMEOUT, "a bounded device wait gave up (diagnostic barrier never completes)");
+    return P2G_OK;
+}
+
 // ---- seams ----------------------------------------------------------------
 extern "C" p2g_status p2g_gf_mul_xor(uint16_t coeff, const uint8_t* input, uint8_t* output, size_t len,
                                      uint32_t flags, void* stream) {

@@ -64,6 +64,9 @@ cudaError_t launch_basis(uint16_t* basis, uint32_t S, uint32_t RG, uint32_t R, u
 cudaError_t launch_encode(const uint8_t* src, uint64_t src_stride, uint32_t S, const uint16_t* basis,
                           uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec,
                           uint64_t rec_stride, int* err, cudaStream_t st, uint32_t first_exp = 0);
+// One block waits (at most `polls` tries) on an mbarrier nothing arrives on;
+// *gave_up becomes 1 when the bound fired.
+cudaError_t launch_bounded_wait_probe(int* gave_up, uint32_t polls, cudaStream_t st);
 cudaError_t launch_gf_mul_xor(uint16_t coeff, const uint8_t* in, uint8_t* out, size_t len,
                               cudaStream_t st);
 cudaError_t launch_md5_slices(const uint8_t* src, uint64_t stride, uint32_t count,

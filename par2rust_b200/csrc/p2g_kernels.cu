@@ -1631,6 +1631,28 @@ cudaError_t launch_encode(const uint8_t* src, uint64_t src_stride, uint32_t S, c
     return launch_encode_band(pl, 0, src, src_stride, S, basis, RG, R, rec, rec_stride, err, st, first_exp);
 }
 
+// Diagnostic for the failure path every TMA wait in this file takes: an
+// mbarrier that nothing ever arrives on, waited for with the same bounded
+// poll loop (`polls` tries instead of the production limit).  The wait gives
+// up, the kernel records it in *gave_up and returns; nothing faults or hangs.
+__global__ void bounded_wait_probe_kernel(int* __restrict__ gave_up, uint32_t polls) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    bool ok = false;
+    for (uint32_t it = 0; it < polls && !ok; ++it) ok = mbar_try_wait(&bar, 0);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(gave_up, 1);
+}
+
+cudaError_t launch_bounded_wait_probe(int* gave_up, uint32_t polls, cudaStream_t st) {
+    bounded_wait_probe_kernel<<<1, 32, 0, st>>>(gave_up, polls);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_gf_mul_xor(uint16_t coeff, const uint8_t* in, uint8_t* out, size_t len, cudaStream_t st) {
     const uint64_t nsym = len / 2;
     if (!nsym) return cudaSuccess;

@@ -209,6 +209,27 @@ def test_single_16m_bit_exact(p2g, oracle, gpu):
     assert all(a == b for (_, a), (_, b) in zip(got, want))
 
 
+def test_bounded_wait_gives_up_and_device_stays_usable(p2g, oracle, gpu):
+    """A device wait that can never complete must end in DeviceTimeout (the
+    status a job gets when a copy never lands), not a hang, and the next
+    create on the same device must still be bit-exact."""
+    import time
+
+    for polls in (1, 1 << 12, 1 << 16):
+        t0 = time.time()
+        with pytest.raises(p2g.DeviceTimeout):
+            p2g.check_bounded_wait(polls)
+        assert time.time() - t0 < 30
+    with pytest.raises(p2g.InvalidArgument):
+        p2g.check_bounded_wait(0)
+    data = file_bytes(0xB0D, 50_000).tobytes()
+    opts = p2g.CreateOptions(output="recovery.par2", slice_size=1024, recovery_block_count=9)
+    got = p2g.create_in_memory(opts, [(b"after.bin", data)])
+    want = oracle.create([(b"after.bin", data)], 1024, 9)
+    assert [n for n, _ in got] == [n for n, _ in want]
+    assert all(a == b for (_, a), (_, b) in zip(got, want))
+
+
 # ---- filesystem entry points -------------------------------------------------
 class Capture:
     def __init__(self):
