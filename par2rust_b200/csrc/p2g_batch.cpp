@@ -375,7 +375,9 @@ struct PlanKey {
 };
 std::mutex g_plan_mu;
 std::map<PlanKey, SingleJobPlan> g_plans;
+size_t g_plan_items = 0;                    // items held by the cached plans
 constexpr size_t kMaxCachedPlans = 256;
+constexpr size_t kMaxCachedItems = 1u << 20;  // 24 MiB of items
 SingleJobPlan plan_single_job_uncached(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans,
                                        bool set_id, bool chains, uint32_t ctas, uint64_t file_bytes,
                                        bool split_tail);
@@ -392,8 +394,11 @@ SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n
     }
     SingleJobPlan p = plan_single_job_uncached(slice, S, R, n_files, scans, set_id, chains, ctas, file_bytes, split_tail);
     std::lock_guard<std::mutex> lk(g_plan_mu);
-    if (g_plans.size() >= kMaxCachedPlans) g_plans.clear();
-    g_plans.emplace(key, p);
+    if (g_plans.size() >= kMaxCachedPlans || g_plan_items + p.items.size() > kMaxCachedItems) {
+        g_plans.clear();
+        g_plan_items = 0;
+    }
+    if (g_plans.emplace(key, p).second) g_plan_items += p.items.size();
     return p;
 }
 

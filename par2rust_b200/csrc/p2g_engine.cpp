@@ -230,22 +230,55 @@ static FileHashMode choose_file_hash_mode(const std::vector<uint64_t>& lens) {
     return t_host < t_dev ? FileHashMode::Host : FileHashMode::Device;
 }
 
-// Host-side whole-file MD5 of several buffers on a small thread pool.
+// Runs fn() on up to n threads including the caller's; threads that cannot
+// be started are simply not used (fn must share its work through a counter).
+template <class F>
+static void run_on_threads(unsigned n, F&& fn) {
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < n; ++t) {
+        try {
+            th.emplace_back(fn);
+        } catch (const std::exception&) {
+            break;
+        }
+    }
+    fn();
+    for (auto& t : th) t.join();
+}
+
+// Host-side whole-file MD5 of several buffers on a small thread pool.  The
+// caller's own thread takes whatever is left when it joins, so every buffer
+// is hashed even when no thread could be started.
 struct HostHasher {
     std::vector<std::thread> th;
-    void start(const std::vector<const uint8_t*>& data, const std::vector<uint64_t>& lens, std::vector<Md5>& out) {
-        out.resize(data.size());
+    const std::vector<const uint8_t*>* data = nullptr;
+    const std::vector<uint64_t>* lens = nullptr;
+    std::vector<Md5>* out = nullptr;
+    std::shared_ptr<std::atomic<size_t>> next;
+    void work() {
+        for (size_t i = (*next)++; i < data->size(); i = (*next)++) (*out)[i] = md5_of((*data)[i], (*lens)[i]);
+    }
+    void start(const std::vector<const uint8_t*>& d, const std::vector<uint64_t>& l, std::vector<Md5>& o) {
+        o.resize(d.size());
+        data = &d;
+        lens = &l;
+        out = &o;
+        next = std::make_shared<std::atomic<size_t>>(0);
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        const unsigned nt = (unsigned)std::min<size_t>(hw, data.size());
-        auto next = std::make_shared<std::atomic<size_t>>(0);
-        for (unsigned t = 0; t < nt; ++t)
-            th.emplace_back([&data, &lens, &out, next]() {
-                for (size_t i = (*next)++; i < data.size(); i = (*next)++) out[i] = md5_of(data[i], lens[i]);
-            });
+        const unsigned nt = (unsigned)std::min<size_t>(hw, d.size());
+        for (unsigned t = 0; t < nt; ++t) {
+            try {
+                th.emplace_back([this]() { work(); });
+            } catch (const std::exception&) {
+                break;
+            }
+        }
     }
     void join() {
+        if (next) work();
         for (auto& t : th) t.join();
         th.clear();
+        next.reset();
     }
     ~HostHasher() { join(); }
 };
@@ -1258,11 +1291,8 @@ static p2g_status write_volumes(const std::string& output, const CreateOutput& c
             if (st[v] != P2G_OK) msg[v] = p2g_last_error_message();
         }
     };
-    const unsigned nt = (unsigned)std::min<size_t>(std::min(8u, std::max(1u, std::thread::hardware_concurrency())), nv);
-    std::vector<std::thread> th;
-    for (unsigned t = 1; t < nt; ++t) th.emplace_back(worker);
-    worker();
-    for (auto& t : th) t.join();
+    run_on_threads((unsigned)std::min<size_t>(std::min(8u, std::max(1u, std::thread::hardware_concurrency())), nv),
+                   worker);
     for (size_t v = 0; v < nv; ++v) {
         if (st[v] != P2G_OK) return set_error(st[v], "%s", msg[v].c_str());
         p2g_progress_event ev = mk(P2G_EV_VOLUME_WRITTEN);
@@ -1536,10 +1566,7 @@ extern "C" p2g_status p2g_create_in_memory(const p2g_create_options* opts, const
                     memcpy(cp.dst + off, cp.src + off, std::min(kPiece, cp.len - off));
             }
         };
-        std::vector<std::thread> th;
-        for (unsigned t = 1; t < nt; ++t) th.emplace_back(worker);
-        worker();
-        for (auto& t : th) t.join();
+        run_on_threads(nt, worker);
     };
     const p2g_status st = device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co,
                                         rec, &lay_out);

@@ -503,7 +503,12 @@ extern "C" p2g_status p2g_server_create(const p2g_server_options* opts, p2g_serv
     P2G_CU(prepare_batch_kernel());
     for (uint32_t i = s->max_jobs; i-- > 0;) s->free_slots.push_back(i);
     p2g_server* raw = s.release();
-    raw->th = std::thread(scheduler, raw);
+    try {
+        raw->th = std::thread(scheduler, raw);
+    } catch (const std::exception& e) {  // no thread for the scheduler: nothing was started
+        p2g_server_destroy(raw);
+        return set_error(P2G_ERR_INVALID_ARGUMENT, "cannot start the server's scheduler thread: %s", e.what());
+    }
     *out = raw;
     return P2G_OK;
 }
