@@ -972,9 +972,13 @@ __device__ __forceinline__ uint32_t crc_slice_warp(const uint32_t* __restrict__ 
                                                    const uint32_t (*T)[256]) {
     uint32_t c = lane == 0 ? 0xFFFFFFFFu : 0u;
     uint64_t w = cl.start;
-    if (VEC) {
+    if (VEC && w + 4 <= cl.end) {
+        // the next 16 bytes are loaded before the current 16 are folded in,
+        // so a lane has two loads in flight instead of one
+        uint4 nxt = __ldg(reinterpret_cast<const uint4*>(p + w));
         for (; w + 4 <= cl.end; w += 4) {
-            const uint4 v = __ldg(reinterpret_cast<const uint4*>(p + w));
+            const uint4 v = nxt;
+            if (w + 8 <= cl.end) nxt = __ldg(reinterpret_cast<const uint4*>(p + w + 4));
             const uint32_t vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
