@@ -294,7 +294,9 @@ __device__ __forceinline__ bool encode_tile(const uint8_t* __restrict__ src, uin
 
     // derived basis: this thread's (j = warp, row = lane) entry and its offset in a slot
     const uint32_t g_row = rg * kRowsPerGroup + (lane & (31u >> (fold >> 1)));  // replicated when folded
-    const uint32_t g_exp = first_exp + g_row;
+    // exponent mod 65535 (the coefficient is 2^(logbase * e mod 65535)), so
+    // the product below stays under 2^32 for first_exp + row >= 65536 too
+    const uint32_t g_exp = (first_exp + g_row) % kFieldLimit;
     const bool g_live = g_row < R;
     const uint32_t g_off = (uint32_t)((((warp & 7) * 2 + (warp >> 3)) * 32 + lane) * 2);
     auto gen_value = [&](uint32_t lb) -> uint16_t {

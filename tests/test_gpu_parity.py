@@ -57,6 +57,31 @@ def test_encode_basis_loaded_or_derived_agree(p2g, oracle, gpu, monkeypatch, S, 
     assert (want == got_gen).all() and (want == got_load).all()
 
 
+@pytest.mark.parametrize("first", [0, 5, 40000, 65496])
+def test_encode_first_exponent(p2g, oracle, gpu, monkeypatch, first):
+    """c(r,s) = base_s^(first_exponent + r) up to the largest exponent, 65535
+    (where base^65535 = 1: the field's multiplicative order); both basis
+    modes against gf_pow/gf_mul.  Exponents past 65535 are refused."""
+    S, slice_, R = 3, 64, 40
+    with pytest.raises(p2g.TooManyRecoveryBlocks):
+        p2g.encode(rnd(1, S * slice_), slice_, R, first_exponent=65536 - R + 1)
+    src = rnd(77 + first % 1000, S * slice_)
+    sym = src.view("<u2").reshape(S, slice_ // 2)
+    bases = oracle.input_bases(S)
+    want = np.zeros((R, slice_ // 2), np.uint16)
+    for r in range(R):
+        cs = [oracle.gf_pow(bases[s], first + r) for s in range(S)]
+        for k in range(slice_ // 2):
+            v = 0
+            for s in range(S):
+                v ^= oracle.gf_mul(cs[s], int(sym[s, k]))
+            want[r, k] = v
+    got_load = p2g.encode(src, slice_, R, first_exponent=first).view("<u2").reshape(R, -1)
+    monkeypatch.setenv("P2G_ENCODE_BASIS", "derive")
+    got_gen = p2g.encode(src, slice_, R, first_exponent=first).view("<u2").reshape(R, -1)
+    assert (got_load == want).all() and (got_gen == want).all()
+
+
 def test_encode_zero_source_gives_zero(p2g, gpu):
     assert not p2g.encode(np.zeros(4 * 1024, np.uint8), 1024, 70).any()
 
