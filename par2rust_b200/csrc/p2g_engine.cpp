@@ -1303,6 +1303,118 @@ static p2g_status write_volumes(const std::string& output, const CreateOutput& c
     return P2G_OK;
 }
 
+// Volume files written in two passes around the host's whole-file hashes.
+// While the files still hash, each volume's recovery packets (which need only
+// the device results) go into its temporary file after room for the critical
+// block.  Once the hashes are done, the critical block goes in at both ends,
+// then fsync and rename as in write_atomic (src/creator.rs:1070-1087).
+// Volumes are written on up to 8 threads; temp files are removed on failure.
+struct StagedVolumes {
+    std::vector<std::string> paths, tmps;
+    std::vector<int> fds;
+    std::vector<uint64_t> mid;  // recovery-packet bytes per volume
+    size_t crit_len = 0;
+    bool active = false;
+    ~StagedVolumes() { discard(); }
+    void discard() {
+        for (size_t v = 0; v < fds.size(); ++v) {
+            if (fds[v] >= 0) close(fds[v]);
+            fds[v] = -1;
+            if (!tmps[v].empty()) unlink(tmps[v].c_str());
+        }
+        active = false;
+    }
+    static p2g_status pwrite_all(int fd, const uint8_t* p, size_t n, uint64_t off, const std::string& path) {
+        while (n) {
+            const ssize_t w = pwrite(fd, p, n > (1u << 30) ? (1u << 30) : n, (off_t)off);
+            if (w < 0) {
+                if (errno == EINTR) continue;
+                return set_error(P2G_ERR_IO, "I/O error: %s: %s", path.c_str(), strerror(errno));
+            }
+            p += w;
+            n -= (size_t)w;
+            off += (uint64_t)w;
+        }
+        return P2G_OK;
+    }
+    // runs fn(v) for every volume on a few threads; the first failure (in
+    // volume order) is returned with its message
+    template <class F>
+    p2g_status each(F&& fn) {
+        const size_t nv = paths.size();
+        std::vector<p2g_status> st(nv, P2G_OK);
+        std::vector<std::string> msg(nv);
+        std::atomic<size_t> next{0};
+        run_on_threads((unsigned)std::min<size_t>(std::min(8u, std::max(1u, std::thread::hardware_concurrency())),
+                                                  std::max<size_t>(nv, 1)),
+                       [&]() {
+                           for (size_t v = next++; v < nv; v = next++) {
+                               st[v] = fn(v);
+                               if (st[v] != P2G_OK) msg[v] = p2g_last_error_message();
+                           }
+                       });
+        for (size_t v = 0; v < nv; ++v)
+            if (st[v] != P2G_OK) return set_error(st[v], "%s", msg[v].c_str());
+        return P2G_OK;
+    }
+    p2g_status write_recovery(const std::string& output, const CreateOutput& o, uint64_t slice,
+                              const std::vector<uint32_t>& vs, size_t clen) {
+        const size_t nv = vs.size();
+        paths.assign(nv, "");
+        tmps.assign(nv, "");
+        fds.assign(nv, -1);
+        mid.assign(nv, 0);
+        crit_len = clen;
+        active = true;
+        std::vector<uint32_t> firsts(nv);
+        uint32_t first = 0;
+        for (size_t v = 0; v < nv; ++v) {
+            firsts[v] = first;
+            paths[v] = volume_filename(output, (uint16_t)first, vs[v]);
+            tmps[v] = paths[v] + ".par2rust.tmp";
+            first += vs[v];
+        }
+        return each([&](size_t v) -> p2g_status {
+            const int fd = open(tmps[v].c_str(), O_WRONLY | O_CREAT | O_TRUNC | O_CLOEXEC, 0644);
+            if (fd < 0) return set_error(P2G_ERR_IO, "I/O error: %s: %s", tmps[v].c_str(), strerror(errno));
+            fds[v] = fd;
+            std::vector<uint8_t> headers;
+            std::vector<std::pair<const uint8_t*, size_t>> pieces;
+            volume_pieces_recovery(o, slice, firsts[v], vs[v], headers, pieces);
+            uint64_t at = clen;
+            for (auto& pc : pieces) {
+                P2G_TRY(pwrite_all(fd, pc.first, pc.second, at, tmps[v]));
+                at += pc.second;
+            }
+            mid[v] = at - clen;
+            return P2G_OK;
+        });
+    }
+    p2g_status finish(const std::vector<uint8_t>& critical, p2g_progress_fn cb, void* user,
+                      std::vector<std::string>& written) {
+        P2G_TRY(each([&](size_t v) -> p2g_status {
+            P2G_TRY(pwrite_all(fds[v], critical.data(), critical.size(), 0, tmps[v]));
+            P2G_TRY(pwrite_all(fds[v], critical.data(), critical.size(), crit_len + mid[v], tmps[v]));
+            if (fsync(fds[v]) != 0) return set_error(P2G_ERR_IO, "I/O error: %s: %s", tmps[v].c_str(), strerror(errno));
+            const int fd = fds[v];
+            fds[v] = -1;
+            if (close(fd) != 0) return set_error(P2G_ERR_IO, "I/O error: %s: %s", tmps[v].c_str(), strerror(errno));
+            if (rename(tmps[v].c_str(), paths[v].c_str()) != 0)
+                return set_error(P2G_ERR_IO, "I/O error: %s: %s", paths[v].c_str(), strerror(errno));
+            tmps[v].clear();  // renamed: nothing to remove any more
+            return P2G_OK;
+        }));
+        for (size_t v = 0; v < paths.size(); ++v) {
+            p2g_progress_event ev = mk(P2G_EV_VOLUME_WRITTEN);
+            ev.path = paths[v].c_str();
+            emit(cb, user, ev);
+            written.push_back(paths[v]);
+        }
+        active = false;
+        return P2G_OK;
+    }
+};
+
 // Writes the index and (if R > 0) volume files of an already computed set.
 static p2g_status write_outputs(const p2g_create_options& o, const CreateOutput& co, uint32_t R, uint64_t slice,
                                 p2g_progress_fn cb, void* user, std::vector<std::string>& written) {
@@ -1450,7 +1562,19 @@ extern "C" p2g_status p2g_run_create_fused(const p2g_create_options* opts, const
     }
     CreateOutput co;
     PinnedRec rec(c);
-    P2G_TRY(device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co, rec));
+    // with a valid volume scheme, the volumes' recovery packets are written
+    // while the whole files still hash (StagedVolumes)
+    std::vector<uint32_t> early_vs;
+    const bool stage = R && resolve_volume_sizes(opts->volume_scheme, R, early_vs) == P2G_OK;
+    clear_error();
+    StagedVolumes staged;
+    p2g_status staged_st = P2G_OK;
+    const WhileHashing write_early = [&](const CreateOutput& o, size_t clen) {
+        staged_st = staged.write_recovery(opts->output, o, slice, early_vs, clen);
+    };
+    P2G_TRY(device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co, rec,
+                          stage ? &write_early : nullptr));
+    if (staged.active && (staged_st != P2G_OK || staged.crit_len != co.critical.size())) staged.discard();
     for (uint32_t f = 0; f < n; ++f) {
         p2g_progress_event ev = mk(P2G_EV_SCAN_PROGRESS);
         ev.path = inputs[f].path;
@@ -1475,7 +1599,17 @@ extern "C" p2g_status p2g_run_create_fused(const p2g_create_options* opts, const
         co.vol_sizes = vs;
     }
     std::vector<std::string> written;
-    P2G_TRY(write_outputs(*opts, co, R, slice, cb, user, written));
+    if (staged.active) {
+        std::vector<std::pair<const uint8_t*, size_t>> pieces = {{co.critical.data(), co.critical.size()}};
+        P2G_TRY(write_atomic(opts->output, pieces));
+        p2g_progress_event ev = mk(P2G_EV_INDEX_WRITTEN);
+        ev.path = opts->output;
+        emit(cb, user, ev);
+        written.push_back(opts->output);
+        P2G_TRY(staged.finish(co.critical, cb, user, written));
+    } else {
+        P2G_TRY(write_outputs(*opts, co, R, slice, cb, user, written));
+    }
     fill_path_list(out, written);
     return P2G_OK;
 }
