@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <functional>
 #include <memory>
 #include <mutex>
@@ -91,7 +92,8 @@ struct Context {
     DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out, md5_state;
     DevBuf persist;    // single-job persistent run: descriptor, items, chain state, tables
     PinBuf h_spans, h_h16k, h_err, h_stage, h_persist;
-    PinBuf h_rec;  // host copy of the recovery rows (create calls)
+    PinBuf h_rec;   // host copy of the recovery rows (create calls)
+    PinBuf h_prog;  // encode progress: the device queue head, read while a job runs
 };
 static Context& ctx() {
     static Context* c = new Context();  // never destroyed: the CUDA runtime may be gone at exit
@@ -312,9 +314,52 @@ struct DeviceJob {
     Md5 set_id{};
     // set instead of computing from hash16k (run_create with scanned sources)
     bool have_set_id = false;
+    // optional: called from the calling thread while the encode runs, with
+    // input slices done (an estimate from the items the device has taken)
+    std::function<void(uint64_t done, uint64_t total)> progress;
 };
 
 static p2g_status check_device_error(Context& c);
+
+// Encode progress from the device's own counter: while the persistent launch
+// runs, the queue head (items taken so far) is read back on a side stream
+// every ~0.5 ms.  Items are queued set-id / file hashes / scans, then encode
+// items, then CRC32, so the encode items taken give the fraction done.
+// Reported as input slices, monotonic, below S until the launch ends (the
+// caller reports S itself).
+static p2g_status poll_progress(Context& c, DeviceJob& j, const SingleJobPlan& pl, const uint32_t* d_head,
+                                cudaStream_t st) {
+    uint64_t first_enc = 0, n_enc = 0;
+    for (size_t i = 0; i < pl.items.size(); ++i)
+        if ((pl.items[i].kind_rg & kItemKindMask) == kItemEncode) {
+            if (!n_enc) first_enc = i;
+            ++n_enc;
+        }
+    if (!n_enc) return P2G_OK;
+    P2G_CU(c.h_prog.ensure(64));
+    volatile uint32_t* head = c.h_prog.as<uint32_t>();
+    cudaStream_t side = c.st[1];
+    uint64_t last = 0;
+    for (;;) {
+        const cudaError_t q = cudaStreamQuery(st);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) P2G_CU(q);
+        P2G_CU(cudaMemcpyAsync(c.h_prog.p, d_head, sizeof(uint32_t), cudaMemcpyDeviceToHost, side));
+        P2G_CU(cudaStreamSynchronize(side));
+        const uint64_t taken = *head;
+        const uint64_t enc = taken > first_enc ? std::min<uint64_t>(taken - first_enc, n_enc) : 0;
+        const uint64_t done = std::min<uint64_t>((uint64_t)j.S * enc / n_enc, j.S ? j.S - 1 : 0);
+        if (done > last) {
+            last = done;
+            j.progress(done, j.S);
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(500));
+    }
+    // "not ready" answers are status, not errors: keep them out of the
+    // error state the launch wrappers read next
+    if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();
+    return P2G_OK;
+}
 
 // The device job through the persistent kernel (p2g_kernels.cu, batch_kernel)
 // with this one job: slice MD5/CRC32 scan items and the set-id item first,
@@ -437,6 +482,7 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
                         (uint32_t)pl.items.size(), reinterpret_cast<uint32_t*>(D + o_ctl), err,
                         (uint32_t)device_sm_count(), st));
     P2G_CU(cudaMemcpyAsync(c.h_err.p, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (j.progress && j.R && j.S) P2G_TRY(poll_progress(c, j, pl, reinterpret_cast<const uint32_t*>(D + o_ctl), st));
     if (!j.have_set_id) {
         // set id = MD5(main packet body) over the sorted file ids
         // (src/source.rs:303-309, src/packet/main_packet.rs:25-42); the
@@ -741,7 +787,8 @@ using WhileHashing = std::function<void(const CreateOutput&, size_t critical_len
 static p2g_status device_create(Context& c, const CreateInput* in, uint32_t n, uint64_t slice, uint32_t R,
                                 const p2g_source_file* src_known, const char* const* comments, uint32_t n_comments,
                                 CreateOutput& out, PinnedRec& rec_host,
-                                const WhileHashing* while_hashing = nullptr) {
+                                const WhileHashing* while_hashing = nullptr,
+                                const std::function<void(uint64_t, uint64_t)>* progress = nullptr) {
     std::vector<JobFile> files(n);
     uint64_t S = 0;
     for (uint32_t f = 0; f < n; ++f) {
@@ -805,6 +852,7 @@ static p2g_status device_create(Context& c, const CreateInput* in, uint32_t n, u
         j.have_set_id = true;
     }
     cudaStream_t main = c.st[0];
+    if (progress) j.progress = *progress;
     P2G_TRY(run_device_job(c, j, main));
 
     // Downloads
@@ -1489,7 +1537,15 @@ static p2g_status run_create_impl(const p2g_create_options* opts, const p2g_sour
         }
         CreateOutput enc;
         PinnedRec rec(c);
-        P2G_TRY(device_create(c, ins.data(), n, slice, R, sources, opts->comments, opts->comment_count, enc, rec));
+        // encode progress from the device's item counter while it runs
+        const std::function<void(uint64_t, uint64_t)> tick = [&](uint64_t done, uint64_t total) {
+            p2g_progress_event ev = mk(P2G_EV_ENCODE_PROGRESS);
+            ev.input_block_done = done;
+            ev.input_blocks = total;
+            emit(cb, user, ev);
+        };
+        P2G_TRY(device_create(c, ins.data(), n, slice, R, sources, opts->comments, opts->comment_count, enc, rec,
+                              nullptr, cb ? &tick : nullptr));
         emit_encode_events(cb, user, S, R, true);
         co.rec_host = enc.rec_host;
         co.pkt_md5 = std::move(enc.pkt_md5);

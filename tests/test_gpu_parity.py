@@ -286,6 +286,26 @@ def test_run_create_scan_fused_agree(p2g, oracle, gpu, tmp_path):
         assert not list(d1.glob("*.tmp")) and not list(d2.glob("*.tmp"))
 
 
+def test_encode_progress_from_device_counter(p2g, gpu, tmp_path):
+    """run_create_with_progress reports encode progress while the device
+    works: ENCODE_PROGRESS events between STARTED and COMPLETED with input
+    blocks done strictly rising, below the total until the last one."""
+    n, slice_, R = 96 << 20, 65536, 1000
+    (tmp_path / "big.bin").write_bytes(file_bytes(0xE7, n).tobytes())
+    src = p2g.SourceFile.scan(tmp_path / "big.bin", b"big.bin", slice_)
+    S = len(src.slice_checksums)
+    cap = Capture()
+    opts = p2g.CreateOptions(output=tmp_path / "recovery.par2", slice_size=slice_, recovery_block_count=R,
+                             volume_scheme=p2g.VolumeScheme.Uniform(4))
+    p2g.run_create_with_progress(opts, [src], cap)
+    kinds = [e.kind for e in cap.events]
+    a, b = kinds.index("EncodeStarted"), kinds.index("EncodeCompleted")
+    prog = [e.input_block_done for e in cap.events[a:b] if e.kind == "EncodeProgress"]
+    assert all(e.kind == "EncodeProgress" for e in cap.events[a + 1:b])
+    assert prog[-1] == S and all(x < y for x, y in zip(prog, prog[1:]))
+    assert len(prog) >= 3, prog  # the job runs for milliseconds: the counter is read several times
+
+
 def test_scan_matches_oracle(p2g, oracle, gpu, tmp_path):
     for n, slice_ in [(5, 4), (17, 8), (16384 + 100, 4096), (4096 * 16, 16), (1, 4)]:
         data = bytes(((i * 0x9E37) >> 5) & 0xFF for i in range(n))
