@@ -333,6 +333,23 @@ def test_scan_errors(p2g, gpu, tmp_path):
         p2g.SourceFile.scan(tmp_path / "missing", b"x", 4)
 
 
+def test_fused_create_volume_failure_leaves_no_temp_files(p2g, gpu, tmp_path):
+    """A volume whose temp file cannot be created (a directory sits at its
+    name) fails the fused create with IoError; the volumes written early
+    while the file hashed are removed, and no temp file is left behind."""
+    data = file_bytes(0xF1, 300_000).tobytes()
+    (tmp_path / "in.bin").write_bytes(data)
+    out = tmp_path / "recovery.par2"
+    first_vol = p2g.volume_filename(str(out), 0, 1)
+    (tmp_path / (os.path.basename(first_vol) + ".par2rust.tmp")).mkdir()
+    opts = p2g.CreateOptions(output=out, slice_size=4096, recovery_block_count=11,
+                             volume_scheme=p2g.VolumeScheme.Exponential())
+    with pytest.raises(p2g.IoError):
+        p2g.run_create_fused(opts, [(tmp_path / "in.bin", b"in.bin")])
+    assert [p for p in tmp_path.glob("*.par2rust.tmp") if p.is_file()] == []
+    assert not os.path.exists(first_vol)
+
+
 def test_create_errors(p2g, gpu, tmp_path):
     (tmp_path / "a.bin").write_bytes(b"x")
     src = p2g.SourceFile.scan(tmp_path / "a.bin", b"a.bin", 4)
