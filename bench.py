@@ -430,7 +430,7 @@ def bench_batch(dev, steps, warmup, plain_steps=1, n_jobs=256, e2e_steps=0):
 
         # the same through StagedBatch: uploads of later groups overlap the
         # running groups, downloads follow each group
-        staged = p2g.StagedBatch(specs, hosts, outs, groups=4)
+        staged = p2g.StagedBatch(specs, hosts, outs, groups=6)
 
         def staged_step():
             staged.launch(stream.cuda_stream)

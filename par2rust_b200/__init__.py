@@ -733,7 +733,7 @@ class StagedBatch:
     receive the job's device buffers of the same names.
     """
 
-    def __init__(self, jobs: Sequence[BatchJobSpec], hosts: Sequence[object], outputs=None, groups: int = 4,
+    def __init__(self, jobs: Sequence[BatchJobSpec], hosts: Sequence[object], outputs=None, groups: int = 6,
                  flags: int = 0):
         import torch
 
