@@ -224,6 +224,20 @@ def test_banded_encode_and_packet_md5(p2g, oracle, gpu, n_slices, R):
     assert all(a == b for (_, a), (_, b) in zip(got, want))
 
 
+@pytest.mark.parametrize("slice_,S,R", [(65540, 100, 30), (132, 3000, 200), (4100, 600, 100), (20004, 800, 40)])
+def test_split_tail_with_realigned_slices(p2g, oracle, gpu, slice_, S, R):
+    """Slice sizes that are not multiples of 16 (the encode reads a
+    realigned copy) in jobs whose planner cuts encode items into
+    XOR-accumulating slice ranges: every output byte against the oracle."""
+    data = file_bytes(slice_ + S, slice_ * S - 7).tobytes()
+    opts = p2g.CreateOptions(output="recovery.par2", slice_size=slice_, recovery_block_count=R,
+                             volume_scheme=p2g.VolumeScheme.Exponential())
+    got = p2g.create_in_memory(opts, [(b"x.bin", data)])
+    want = oracle.create([(b"x.bin", data)], slice_, R, kind=oracle.SCHEME_EXPONENTIAL)
+    assert [n for n, _ in got] == [n for n, _ in want]
+    assert all(a == b for (_, a), (_, b) in zip(got, want))
+
+
 def test_single_16m_bit_exact(p2g, oracle, gpu):
     """16,777,216 B, slice 65,536, R 32, Single: every output byte vs the oracle."""
     data = file_bytes(0x16, 16_777_216)
