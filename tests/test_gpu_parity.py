@@ -238,6 +238,30 @@ def test_split_tail_with_realigned_slices(p2g, oracle, gpu, slice_, S, R):
     assert all(a == b for (_, a), (_, b) in zip(got, want))
 
 
+@pytest.mark.parametrize("slice_,S,R", [(4100, 600, 100), (65536, 64, 40)])
+def test_device_job_writes_nothing_past_the_row(p2g, oracle, gpu, slice_, S, R):
+    """A caller's recovery stride wider than the padded row: the job (tail
+    split, zeroed columns, accumulating items) leaves the bytes past the
+    padded row untouched and the rows equal to the oracle's."""
+    import torch
+
+    L = slice_ * S - 11
+    host = np.zeros(S * slice_, np.uint8)
+    host[:L] = np.frombuffer(file_bytes(S + R, L).tobytes(), np.uint8)
+    src = torch.from_numpy(host).cuda()
+    bufs = p2g.DeviceJobBuffers(S, 1, slice_, R, src.device)
+    padded = (slice_ + 15) // 16 * 16
+    stride = padded + 64
+    bufs.recovery = torch.full((R * stride,), 0xA5, dtype=torch.uint8, device=src.device)
+    bufs.rec_stride = stride
+    p2g.run_device_job(src, [L], [b"x.bin"], slice_, R, bufs)
+    torch.cuda.synchronize()
+    rows = bufs.recovery.view(R, stride).cpu().numpy()
+    assert (rows[:, padded:] == 0xA5).all()
+    want = np.asarray(oracle.encode(host, S, slice_, R)).reshape(R, slice_)
+    assert (rows[:, :slice_] == want).all()
+
+
 def test_single_16m_bit_exact(p2g, oracle, gpu):
     """16,777,216 B, slice 65,536, R 32, Single: every output byte vs the oracle."""
     data = file_bytes(0x16, 16_777_216)
