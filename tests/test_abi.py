@@ -100,3 +100,37 @@ def test_host_volume_logic(p2g, oracle):
 def test_errors_map_to_par2error_variants(p2g):
     assert issubclass(p2g.TooManyInputBlocks, p2g.Par2Error)
     assert p2g.InvalidSliceSize.status == 2 and p2g.InvalidVolumeScheme.status == 9
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Every public struct: the ctypes mirror (which the Rust bindings in the
+    integration notes copy) has the C header's size and field offsets, as gcc
+    lays them out."""
+    import ctypes as C
+    import shutil
+    import subprocess
+
+    from par2rust_b200 import _ffi
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    structs = {n: getattr(_ffi, n) for n in dir(_ffi)
+               if n.startswith("p2g_") and isinstance(getattr(_ffi, n), type) and issubclass(getattr(_ffi, n), C.Structure)}
+    assert len(structs) >= 18
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "par2gpu.h"', "int main(void) {"]
+    for n, cls in structs.items():
+        lines.append(f'    printf("{n} %zu\\n", sizeof({n}));')
+        for f in cls._fields_:
+            lines.append(f'    printf("{n}.{f[0]} %zu\\n", offsetof({n}, {f[0]}));')
+    lines += ["    return 0;", "}"]
+    c_file = tmp_path / "layout.c"
+    c_file.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(c_file), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                       text=True).stdout.splitlines())
+    for n, cls in structs.items():
+        assert int(got[n]) == C.sizeof(cls), n
+        for f in cls._fields_:
+            assert int(got[f"{n}.{f[0]}"]) == getattr(cls, f[0]).offset, f"{n}.{f[0]}"
