@@ -69,7 +69,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-vs-plain section of the default (single-file) run")
     ap.add_argument("--batch-jobs", type=int, default=256, help="jobs in the batched comparison")
-    ap.add_argument("--requests", type=int, default=10_000, help="serving: requests per arrival rate")
+    ap.add_argument("--requests", type=int, default=2_000,
+                    help="serving: requests per arrival rate (the full mix is 10,000: ~8-13 min per rate)")
     ap.add_argument("--rates", default="", help="serving: comma-separated arrival rates (jobs/s); default "
                                                 "0.5,0.8,0.95 x the capacity measured by a closed-batch probe")
     ap.add_argument("--probe-jobs", type=int, default=200, help="serving: jobs in the capacity probe")
