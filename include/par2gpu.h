@@ -390,6 +390,20 @@ void p2g_batch_destroy(p2g_batch *batch);
 p2g_status p2g_batch_plan(const p2g_batch_shape *shapes, uint32_t n, uint32_t ctas, uint32_t flags,
                           p2g_batch_info *info, uint32_t *tiles_out);
 
+/* The plan one device job (p2g_run_device_job) runs, from the host-only
+ * planner, for inspection: up to `cap` encode items as (row group, fold,
+ * first symbol, symbols, band, first slice, slice count, accumulate), the
+ * number of encode items, and the first symbol of the columns that are
+ * zeroed for accumulating items (the padded row width when there are none).
+ * `with_chains` plans packet-MD5 chains as the job with packet MD5s does. */
+typedef struct p2g_plan_item {
+    uint32_t row_group, fold, first_symbol, symbols, band, first_slice, slices, accumulate;
+} p2g_plan_item;
+p2g_status p2g_plan_device_job(uint64_t slice_size, uint32_t input_slices, uint32_t recovery_count,
+                               uint32_t file_count, uint32_t with_chains, uint32_t ctas,
+                               p2g_plan_item *items, uint32_t cap, uint32_t *n_items,
+                               uint32_t *zero_from_symbol, uint32_t *band_count);
+
 /* ---- serving loop (no counterpart in par2rust, which runs one create at
  * a time) ------------------------------------------------------------------
  * A request loop with continuous batching.  Submitted create jobs wait in

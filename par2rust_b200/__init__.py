@@ -716,6 +716,24 @@ def staged_groups(sizes: Sequence[int], groups: int) -> List[Tuple[int, int]]:
     return [(a, b) for a, b in zip(bounds, bounds[1:]) if b > a]
 
 
+def plan_device_job(slice_size: int, input_slices: int, recovery_count: int, file_count: int = 1,
+                    with_chains: bool = True, ctas: int = 148):
+    """The encode items p2g_run_device_job would run (host-only planner):
+    returns (items, zero_from_symbol, bands); each item is a dict with
+    row_group, fold, first_symbol, symbols, band, first_slice, slices and
+    accumulate."""
+    n = C.c_uint32()
+    z = C.c_uint32()
+    nb = C.c_uint32()
+    _check(lib().p2g_plan_device_job(slice_size, input_slices, recovery_count, file_count, int(with_chains), ctas,
+                                     None, 0, C.byref(n), C.byref(z), C.byref(nb)))
+    arr = (_ffi.p2g_plan_item * max(n.value, 1))()
+    _check(lib().p2g_plan_device_job(slice_size, input_slices, recovery_count, file_count, int(with_chains), ctas,
+                                     C.cast(arr, C.c_void_p), n.value, C.byref(n), C.byref(z), C.byref(nb)))
+    items = [{f: getattr(arr[i], f) for f, _ in _ffi.p2g_plan_item._fields_} for i in range(n.value)]
+    return items, z.value, nb.value
+
+
 class StagedBatch:
     """Batched create for jobs whose sources sit in pinned host memory.
 

@@ -94,6 +94,11 @@ class p2g_buffer_input(C.Structure):
     ]
 
 
+class p2g_plan_item(C.Structure):
+    _fields_ = [("row_group", C.c_uint32), ("fold", C.c_uint32), ("first_symbol", C.c_uint32), ("symbols", C.c_uint32),
+                ("band", C.c_uint32), ("first_slice", C.c_uint32), ("slices", C.c_uint32), ("accumulate", C.c_uint32)]
+
+
 class p2g_output_file(C.Structure):
     _fields_ = [("name", C.c_char_p), ("data", C.POINTER(C.c_uint8)), ("length", C.c_uint64)]
 
@@ -265,6 +270,9 @@ SIGNATURES = [
     ("p2g_encode", C.c_int, [C.POINTER(p2g_encode_job)]),
     ("p2g_encode_noalloc", C.c_int, [C.POINTER(p2g_encode_job)]),
     ("p2g_check_bounded_wait", C.c_int, [C.c_uint32]),
+    ("p2g_plan_device_job", C.c_int,
+     [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
+      C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     ("p2g_slice_checksums", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("p2g_file_hashes", C.c_int,

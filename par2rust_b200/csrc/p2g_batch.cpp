@@ -502,6 +502,31 @@ void fill_info(const p2g_batch* b, p2g_batch_info* out) {
 
 using namespace p2g;
 
+extern "C" p2g_status p2g_plan_device_job(uint64_t slice_size, uint32_t input_slices, uint32_t recovery_count,
+                                          uint32_t file_count, uint32_t with_chains, uint32_t ctas,
+                                          p2g_plan_item* items, uint32_t cap, uint32_t* n_items,
+                                          uint32_t* zero_from_symbol, uint32_t* band_count) {
+    clear_error();
+    if (!ctas || !input_slices || input_slices > P2G_MAX_INPUT_BLOCKS || (cap && !items))
+        return set_error(P2G_ERR_INVALID_ARGUMENT, "plan needs ctas > 0, 1..32768 input slices and an item array");
+    P2G_TRY(check_common(std::max(1u, file_count), recovery_count, slice_size));
+    // as run_device_job_persistent plans it (tail split on: it zeroes the columns)
+    const SingleJobPlan pl = plan_single_job(slice_size, input_slices, recovery_count, std::max(1u, file_count),
+                                             true, true, with_chains && recovery_count, ctas, 0, true);
+    uint32_t n = 0;
+    for (const BatchItem& it : pl.items) {
+        if ((it.kind_rg & kItemKindMask) != kItemEncode) continue;
+        if (n < cap)
+            items[n] = {(it.kind_rg >> 8) & 0xFFFFu, 1u << ((it.kind_rg >> 24) & 3u), it.a, it.b & 0xFFFFu,
+                        it.b >> 16, it.s0, it.sn ? it.sn : input_slices, (it.kind_rg & kItemAccumulate) ? 1u : 0u};
+        ++n;
+    }
+    if (n_items) *n_items = n;
+    if (zero_from_symbol) *zero_from_symbol = pl.zero_from_sym;
+    if (band_count) *band_count = (uint32_t)pl.band_items.size();
+    return P2G_OK;
+}
+
 extern "C" p2g_status p2g_batch_plan(const p2g_batch_shape* shapes, uint32_t n, uint32_t ctas, uint32_t flags,
                                      p2g_batch_info* info, uint32_t* tiles_out) {
     clear_error();

@@ -76,6 +76,60 @@ def test_plan_large_batch_is_near_its_bound(p2g):
     assert 250 < info.predicted_ms < 400
 
 
+SPLIT_SHAPES = [(524288, 1027, 200), (65536, 256, 32), (4100, 600, 100), (262144, 4096, 100), (16384, 6104, 1000),
+                (524288, 256, 200), (65540, 100, 30)]
+
+
+@pytest.mark.parametrize("slice_,S,R", SPLIT_SHAPES)
+def test_device_job_plan_covers_every_slice_of_every_tile_once(p2g, slice_, S, R):
+    """The single-job planner may cut encode items of the last bands into
+    slice ranges (tail split).  For every (row group, first symbol) the
+    pieces must tile the input slices exactly once; pieces are accumulating
+    exactly when they do not cover all slices, and start at or after the
+    zeroed columns; items with the same band share it, in symbol order."""
+    items, zero_from, bands = p2g.plan_device_job(slice_, S, R)
+    Np = (slice_ + 15) // 16 * 16 // 2
+    assert items and 0 <= zero_from <= Np
+    RG = (R + 31) // 32
+    pieces = {}
+    for it in items:
+        assert 0 <= it["row_group"] < RG and it["fold"] in (1, 2, 4)
+        assert it["fold"] == 1 or it["row_group"] == RG - 1
+        assert 0 < it["symbols"] and it["first_symbol"] + it["symbols"] <= Np
+        assert 0 <= it["first_slice"] and it["first_slice"] + it["slices"] <= S and it["slices"] > 0
+        assert it["accumulate"] == (0 if it["slices"] == S else 1)
+        if it["accumulate"]:
+            assert it["first_symbol"] >= zero_from
+        if bands:
+            assert it["band"] < bands
+        pieces.setdefault((it["row_group"], it["first_symbol"]), []).append((it["first_slice"], it["slices"]))
+    for key, ps in pieces.items():
+        ps.sort()
+        at = 0
+        for s0, sn in ps:
+            assert s0 == at, (key, ps)
+            at += sn
+        assert at == S, key
+    # every row group covers every symbol (a folded tail item covers `fold` tiles)
+    for rg in range(RG):
+        cover = sorted((it["first_symbol"], it["symbols"]) for it in items if it["row_group"] == rg and it["first_slice"] == 0)
+        at = 0
+        for n0, syms in cover:
+            assert n0 == at, (rg, n0, at)
+            at += syms
+        assert at == Np, rg
+    # the plan is cached: a second call returns the same items
+    again, z2, b2 = p2g.plan_device_job(slice_, S, R)
+    assert again == items and z2 == zero_from and b2 == bands
+
+
+def test_device_job_plan_splits_the_538mb_job(p2g):
+    items, zero_from, bands = p2g.plan_device_job(524288, 1027, 200)
+    acc = [it for it in items if it["accumulate"]]
+    assert bands > 1 and acc and zero_from < 262144
+    assert not any(it["accumulate"] for it in p2g.plan_device_job(524288, 1027, 200, with_chains=False)[0])
+
+
 def test_staged_groups_cover_jobs_in_order(p2g):
     # equal jobs: the first group gets about half of the others' share
     r = p2g.staged_groups([10] * 70, 4)
