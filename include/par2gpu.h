@@ -230,7 +230,17 @@ p2g_status p2g_gf_mul_xor(uint16_t coeff, const uint8_t *input, uint8_t *output,
  * src + s*src_stride (zero-padded slices), recovery row r is written at
  * recovery + r*recovery_stride.  With P2G_DEVICE_POINTERS, src_stride and
  * recovery_stride must be multiples of 16 and both pointers 16-byte
- * aligned, and the work is enqueued on `stream` (0 = legacy default). */
+ * aligned, and the work is enqueued on `stream` (0 = legacy default).
+ * Device rows are read and written in whole 16-byte units: bytes
+ * [slice_size, round_up(slice_size, 16)) of every source row are read --
+ * for the last row too, so src must be readable up to
+ * (input_count-1)*src_stride + round_up(slice_size, 16) -- and the same
+ * bytes of every recovery row receive unspecified values (bytes
+ * [0, slice_size) do not depend on them).  With P2G_ENCODE_WAIT the call
+ * waits for its work on `stream` and returns P2G_ERR_TIMEOUT when a
+ * bounded device wait gave up (the rows are then not valid); without it a
+ * device timeout is not reported. */
+#define P2G_ENCODE_WAIT 4u
 typedef struct p2g_encode_job {
     const uint8_t *src;
     uint64_t src_stride;
@@ -258,7 +268,11 @@ p2g_status p2g_encode(const p2g_encode_job *job);
  * looks up the scratch address; make that first call before any stream
  * capture.  All calls share the one scratch array, so calls whose work
  * overlaps on the GPU (other streams, other threads) race: order them on one
- * stream or synchronise between them.  Work is enqueued on `stream`. */
+ * stream or synchronise between them.  Work is enqueued on `stream`; the
+ * padding reads and writes of p2g_encode's device form apply.  Its device
+ * error flag is part of the shared scratch: P2G_ENCODE_WAIT waits for the
+ * call's work and reads the flag back into a local variable (no allocation),
+ * returning P2G_ERR_TIMEOUT when a bounded device wait gave up. */
 p2g_status p2g_encode_noalloc(const p2g_encode_job *job);
 
 /* The per-slice half of scan_via_mmap, src/source.rs:165-220: MD5 and
@@ -390,8 +404,12 @@ void p2g_batch_destroy(p2g_batch *batch);
 p2g_status p2g_batch_plan(const p2g_batch_shape *shapes, uint32_t n, uint32_t ctas, uint32_t flags,
                           p2g_batch_info *info, uint32_t *tiles_out);
 
-/* The plan one device job (p2g_run_device_job) runs, from the host-only
- * planner, for inspection: up to `cap` encode items as (row group, fold,
+/* The plan one device job (p2g_run_device_job) runs when it computes the
+ * slice checksums and derives the set id on the device and leaves hash_full
+ * to the host (P2G_JOB_SKIP_HASH_FULL, or a single large file), from the
+ * host-only planner, for inspection; P2G_TAIL_SPLIT=0 in the environment
+ * turns the tail split off here as it does for the job.  It returns up to
+ * `cap` encode items as (row group, fold,
  * first symbol, symbols, band, first slice, slice count, accumulate), the
  * number of encode items, and the first symbol of the columns that are
  * zeroed for accumulating items (the padded row width when there are none).

@@ -70,6 +70,7 @@ def lib() -> C.CDLL:
         L.or_create.argtypes = [C.POINTER(or_input), C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(or_scheme),
                                 C.POINTER(C.c_char_p), C.c_uint32, C.c_char_p, C.POINTER(C.c_void_p),
                                 C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+        L.or_set_fast_encode.argtypes = [C.c_int]
         L.or_gfni_matrices.argtypes = [C.c_uint16, C.c_void_p]
         L.or_gfni_apply.argtypes = [C.c_void_p, C.c_uint8, C.c_uint8, C.c_void_p, C.c_void_p]
         L.or_build_main_packet.restype = C.c_size_t
@@ -77,6 +78,7 @@ def lib() -> C.CDLL:
         L.or_build_recovery_packet.restype = C.c_size_t
         L.or_build_recovery_packet.argtypes = [C.c_char_p, C.c_uint16, C.c_void_p, C.c_uint64, C.c_void_p]
         L.cb_encode.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_void_p, C.c_int]
+        L.cb_encode_rows.argtypes = [C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]
         L.cb_scan.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.cb_create_timed.restype = C.c_double
         L.cb_create_timed.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_int, C.c_void_p,
@@ -201,6 +203,18 @@ def encode_fast(src, S: int, slice_size: int, R: int, threads: int = 0):
     return out
 
 
+def encode_rows(src, S: int, slice_size: int, exponents, threads: int = 0):
+    """Recovery rows for the listed exponents only (GFNI port, rows in
+    parallel) -> numpy uint8 len(exponents) x slice."""
+    import numpy as np
+
+    a, p = _addr(src)
+    ex = (C.c_uint32 * max(len(exponents), 1))(*exponents)
+    out = np.zeros(len(exponents) * slice_size, dtype=np.uint8)
+    lib().cb_encode_rows(p, S, slice_size, ex, len(exponents), out.ctypes.data, threads)
+    return out.reshape(len(exponents), slice_size)
+
+
 def scan(data: bytes, slice_size: int, name: bytes):
     """(status, [(md5, crc)], hash_full, hash16k, file_id)"""
     n = (len(data) + slice_size - 1) // slice_size if slice_size else 0
@@ -269,8 +283,10 @@ def volume_filename(index_path: str, first: int, count: int) -> str:
 
 
 def create(inputs, slice_size, R, kind=SCHEME_SINGLE, count=0, cap=0, inner=None, sizes=None, comments=(),
-           index_path="recovery.par2"):
-    """Whole create in memory: list of (file name, bytes), or a negative status."""
+           index_path="recovery.par2", fast=False):
+    """Whole create in memory: list of (file name, bytes), or a negative status.
+    fast=True encodes with the multi-threaded GFNI port (for checks at the
+    benchmark sizes, where the scalar encode would take hours)."""
     keep = []
     arr = (or_input * max(len(inputs), 1))()
     for i, (name, data) in enumerate(inputs):
@@ -283,8 +299,12 @@ def create(inputs, slice_size, R, kind=SCHEME_SINGLE, count=0, cap=0, inner=None
     cm = [c.encode() for c in comments]
     carr = (C.c_char_p * max(len(cm), 1))(*cm)
     blob, sizes_p, names = C.c_void_p(), C.c_void_p(), C.c_void_p()
-    n = lib().or_create(arr, len(inputs), slice_size, R, C.byref(s), carr, len(cm), os.fsencode(index_path),
-                        C.byref(blob), C.byref(sizes_p), C.byref(names))
+    lib().or_set_fast_encode(1 if fast else 0)
+    try:
+        n = lib().or_create(arr, len(inputs), slice_size, R, C.byref(s), carr, len(cm), os.fsencode(index_path),
+                            C.byref(blob), C.byref(sizes_p), C.byref(names))
+    finally:
+        lib().or_set_fast_encode(0)
     if n < 0:
         return n
     fs = C.cast(sizes_p, C.POINTER(C.c_uint64))

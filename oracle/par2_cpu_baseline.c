@@ -147,6 +147,28 @@ void cb_encode(const uint8_t *src, uint32_t s_begin, uint32_t s_end, uint64_t sl
     free(bases);
 }
 
+/* Selected recovery rows only: out row k = XOR_s gf_pow(base_s, exps[k]) *
+ * slice s over the S slices at src (back to back), i.e. row exps[k] of
+ * encode_all_recovery_blocks (src/creator.rs:931-1007) -- for spot checks of
+ * jobs whose full encode is too long for the CPU.  Rows run in parallel. */
+void cb_encode_rows(const uint8_t *src, uint32_t S, uint64_t slice_size, const uint32_t *exps, uint32_t n,
+                    uint8_t *out, int threads) {
+    int gfni = cb_have_gfni512();
+    if (threads <= 0) threads = omp_get_max_threads();
+    uint16_t *bases = (uint16_t *)malloc(sizeof(uint16_t) * (S ? S : 1));
+    or_input_bases(S, bases);
+    memset(out, 0, (size_t)n * slice_size);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (uint32_t k = 0; k < n; k++) {
+        cb_tables t;
+        for (uint32_t s = 0; s < S; s++) {
+            cb_build_tables(&t, or_gf_pow(bases[s], exps[k]), gfni);
+            cb_mul_xor(&t, src + (size_t)s * slice_size, out + (size_t)k * slice_size, slice_size, gfni);
+        }
+    }
+    free(bases);
+}
+
 static void cb_md5(const uint8_t *d, size_t n, uint8_t out[16]) {
     unsigned int l = 16;
     EVP_Digest(d, n, out, &l, EVP_md5(), NULL);

@@ -595,6 +595,13 @@ static void bappend(bytes_t *b, const uint8_t *src, size_t n) {
     b->n += n;
 }
 
+/* Large checks (hundreds of MB, hundreds of recovery rows) take hours on the
+ * scalar encode; with this set, or_create encodes with the multi-threaded
+ * GFNI port of par2_cpu_baseline.c instead (same bytes: the tests compare
+ * the two).  Everything else in or_create is unchanged. */
+static int g_fast_encode = 0;
+void or_set_fast_encode(int on) { g_fast_encode = on; }
+
 int64_t or_create(const or_input *inputs, uint32_t n, uint64_t slice_size, uint32_t R,
                   const or_scheme *scheme, const char *const *comments, uint32_t n_comments,
                   const char *index_path, uint8_t **out_blob, uint64_t **out_sizes, char **out_names) {
@@ -682,7 +689,11 @@ int64_t or_create(const or_input *inputs, uint32_t n, uint64_t slice_size, uint3
                 o += nsl[f];
             }
             uint8_t *rec = (uint8_t *)malloc((size_t)R * slice_size);
-            or_encode(src, (uint32_t)total_blocks, slice_size, R, rec);
+            if (g_fast_encode) { /* the multi-threaded GFNI port, pinned to or_encode by the tests */
+                memset(rec, 0, (size_t)R * slice_size);
+                cb_encode(src, 0, (uint32_t)total_blocks, slice_size, R, rec, 0);
+            } else
+                or_encode(src, (uint32_t)total_blocks, slice_size, R, rec);
             free(src);
             uint32_t first = 0;
             for (size_t v = 0; v < sizes.n; v++) { /* build_volume_packet, :1025-1042 */

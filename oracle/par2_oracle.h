@@ -46,6 +46,10 @@ void or_gfni_apply(const uint64_t mats[4], uint8_t lo, uint8_t hi, uint8_t *out_
  * src holds `S` zero-padded slices back to back (slice i at i*slice_size),
  * out receives R slices (recovery i = exponent i), zeroed first. */
 void or_encode(const uint8_t *src, uint32_t S, uint64_t slice_size, uint32_t R, uint8_t *out);
+/* or_create encodes with cb_encode (the multi-threaded port) when on != 0. */
+void or_set_fast_encode(int on);
+void cb_encode(const uint8_t *src, uint32_t s_begin, uint32_t s_end, uint64_t slice_size, uint32_t R, uint8_t *out,
+               int threads);
 
 /* ---- hashes ------------------------------------------------------------ */
 void or_md5(const uint8_t *data, size_t len, uint8_t out[16]);  /* md5_impl::digest */

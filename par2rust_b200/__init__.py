@@ -27,6 +27,7 @@ HASH16K_LEN = 16 * 1024
 HOST_POINTERS = 0
 DEVICE_POINTERS = 1
 JOB_SKIP_HASH_FULL = 2
+ENCODE_WAIT = 4  # p2g_encode / p2g_encode_noalloc: wait and report a device timeout
 
 
 # ---------------------------------------------------------------------------
@@ -495,10 +496,13 @@ def encode(src, slice_size: int, recovery_count: int, first_exponent: int = 0, i
 
 
 def encode_device(src_ptr: int, src_stride: int, input_count: int, slice_size: int, recovery_count: int,
-                  rec_ptr: int, rec_stride: int, stream: int = 0, first_exponent: int = 0) -> None:
+                  rec_ptr: int, rec_stride: int, stream: int = 0, first_exponent: int = 0, wait: bool = False) -> None:
+    """p2g_encode on device buffers, enqueued on `stream`; with wait=True
+    the call waits for it and raises DeviceTimeout if a device wait gave up."""
     job = _ffi.p2g_encode_job(src=src_ptr, src_stride=src_stride, input_count=input_count, slice_size=slice_size,
                               recovery_count=recovery_count, first_exponent=first_exponent, recovery=rec_ptr,
-                              recovery_stride=rec_stride, flags=DEVICE_POINTERS, stream=stream or None)
+                              recovery_stride=rec_stride, flags=DEVICE_POINTERS | (ENCODE_WAIT if wait else 0),
+                              stream=stream or None)
     _check(lib().p2g_encode(C.byref(job)))
 
 

@@ -510,9 +510,13 @@ extern "C" p2g_status p2g_plan_device_job(uint64_t slice_size, uint32_t input_sl
     if (!ctas || !input_slices || input_slices > P2G_MAX_INPUT_BLOCKS || (cap && !items))
         return set_error(P2G_ERR_INVALID_ARGUMENT, "plan needs ctas > 0, 1..32768 input slices and an item array");
     P2G_TRY(check_common(std::max(1u, file_count), recovery_count, slice_size));
-    // as run_device_job_persistent plans it (tail split on: it zeroes the columns)
+    // as run_device_job_persistent plans a job with device slice checksums, a
+    // device set id and hash_full off the device; P2G_TAIL_SPLIT=0 turns the
+    // tail split off there and here alike
+    const char* ts = getenv("P2G_TAIL_SPLIT");
+    const bool split_tail = !(ts && !strcmp(ts, "0"));
     const SingleJobPlan pl = plan_single_job(slice_size, input_slices, recovery_count, std::max(1u, file_count),
-                                             true, true, with_chains && recovery_count, ctas, 0, true);
+                                             true, true, with_chains && recovery_count, ctas, 0, split_tail);
     uint32_t n = 0;
     for (const BatchItem& it : pl.items) {
         if ((it.kind_rg & kItemKindMask) != kItemEncode) continue;

@@ -1082,8 +1082,14 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
             P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
             P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
         }
+        P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s));
         P2G_CU(launch_encode(jb.src, jb.src_stride, S, gen ? nullptr : c.basis.as<uint16_t>(), RG, R, jb.slice_size,
                              jb.recovery, jb.recovery_stride, c.err.as<int>(), s, jb.first_exponent));
+        if (jb.flags & P2G_ENCODE_WAIT) {
+            P2G_CU(cudaMemcpyAsync(c.h_err.p, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            P2G_CU(cudaStreamSynchronize(s));
+            return check_device_error(c);
+        }
         return P2G_OK;
     }
     // host pointers: stage through device buffers

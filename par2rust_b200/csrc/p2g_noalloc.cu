@@ -117,5 +117,14 @@ extern "C" p2g_status p2g_encode_noalloc(const p2g_encode_job* job) {
         (e = launch_encode_noheap(jb.src, jb.src_stride, S, d->basis, RG, R, jb.slice_size, jb.recovery,
                                   jb.recovery_stride, d->err, s)) != cudaSuccess)
         return set_error(P2G_ERR_CUDA, "CUDA error: %s", cudaGetErrorString(e));
+    if (jb.flags & P2G_ENCODE_WAIT) {
+        // read the flag into a local: a pageable copy after the stream's work
+        int flag = 0;
+        if ((e = cudaMemcpyAsync(&flag, d->err, sizeof flag, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return set_error(P2G_ERR_CUDA, "CUDA error: %s", cudaGetErrorString(e));
+        if (flag)
+            return set_error(P2G_ERR_TIMEOUT, "a bounded device wait gave up; the recovery rows are not valid");
+    }
     return P2G_OK;
 }

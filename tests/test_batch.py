@@ -102,14 +102,27 @@ def test_device_job_plan_covers_every_slice_of_every_tile_once(p2g, slice_, S, R
             assert it["first_symbol"] >= zero_from
         if bands:
             assert it["band"] < bands
-        pieces.setdefault((it["row_group"], it["first_symbol"]), []).append((it["first_slice"], it["slices"]))
+        pieces.setdefault((it["row_group"], it["first_symbol"]), []).append(
+            (it["first_slice"], it["slices"], it["symbols"], it["fold"], it["band"]))
     for key, ps in pieces.items():
         ps.sort()
+        # the pieces of one tile are cut only along the slices
+        assert len({(syms, fold, band) for _, _, syms, fold, band in ps}) == 1, (key, ps)
         at = 0
-        for s0, sn in ps:
+        for s0, sn, *_ in ps:
             assert s0 == at, (key, ps)
             at += sn
         assert at == S, key
+    if bands:
+        # bands follow the symbols: within a row group, a later tile never has an
+        # earlier band, and unfolded tiles at one symbol share a band across groups
+        band_at = {}
+        for rg in range(RG):
+            seq = sorted((n0, ps[0][4]) for (g, n0), ps in pieces.items() if g == rg)
+            assert all(a[1] <= b[1] for a, b in zip(seq, seq[1:])), (rg, seq)
+        for (g, n0), ps in pieces.items():
+            if ps[0][3] == 1:
+                assert band_at.setdefault(n0, ps[0][4]) == ps[0][4], (g, n0)
     # every row group covers every symbol (a folded tail item covers `fold` tiles)
     for rg in range(RG):
         cover = sorted((it["first_symbol"], it["symbols"]) for it in items if it["row_group"] == rg and it["first_slice"] == 0)

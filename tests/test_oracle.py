@@ -161,6 +161,26 @@ def test_cpu_baseline_encode_matches_scalar(oracle):
         assert (a == b).all(), (S, slice_, R)
 
 
+def test_encode_rows_matches_full_encode(oracle):
+    S, slice_, R = 7, 4096, 40
+    src = np.frombuffer(deterministic_bytes(77, S * slice_), dtype=np.uint8)
+    full = oracle.encode(src, S, slice_, R).reshape(R, slice_)
+    rows = [0, 1, 17, 39]
+    assert (oracle.encode_rows(src, S, slice_, rows) == full[rows]).all()
+
+
+def test_fast_create_matches_scalar_create(oracle):
+    """create(fast=True) (the GFNI port as encoder) gives the scalar create's
+    files byte for byte, multi-file and ragged tails included; the GPU tests
+    at benchmark sizes compare against the fast form."""
+    files = [(b"a.bin", deterministic_bytes(11, 70_001)), (b"b.bin", deterministic_bytes(12, 4096 * 3)),
+             (b"c.bin", deterministic_bytes(13, 17))]
+    for kind, count in [(oracle.SCHEME_EXPONENTIAL, 0), (oracle.SCHEME_UNIFORM, 3)]:
+        a = oracle.create(files, 4096, 21, kind=kind, count=count)
+        b = oracle.create(files, 4096, 21, kind=kind, count=count, fast=True)
+        assert a == b
+
+
 # ---- MD5 / CRC32 -------------------------------------------------------------
 def test_md5_known_vectors(oracle):
     assert oracle.md5(b"").hex() == "d41d8cd98f00b204e9800998ecf8427e"
