@@ -68,6 +68,12 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the device MD5-chain rate probe")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-vs-plain section of the default (single-file) run")
+    ap.add_argument("--no-many", action="store_true", help="skip the many_2000 section of the default run")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the timed step's outputs")
+    ap.add_argument("--serve-requests", type=int, default=2_000,
+                    help="serving section of the default run: requests per arrival rate (0 skips it)")
+    ap.add_argument("--serve-fracs", default="0.5,0.85",
+                    help="serving section of the default run: arrival rates as fractions of the probed capacity")
     ap.add_argument("--batch-jobs", type=int, default=256, help="jobs in the batched comparison")
     ap.add_argument("--requests", type=int, default=2_000,
                     help="serving: requests per arrival rate (the full mix is 10,000: ~8-13 min per rate)")
@@ -75,114 +81,7 @@ def parse():
                                                 "0.5,0.8,0.95 x the capacity measured by a closed-batch probe")
     ap.add_argument("--probe-jobs", type=int, default=200, help="serving: jobs in the capacity probe")
     ap.add_argument("--wave-ms", type=float, default=20.0, help="serving: target device time per wave")
-    ap.add_argument("--only-step", action="store_true",
-                    help="profiling aid: run only the device-job steps (no JSON line)")
-    ap.add_argument("--only-encode", action="store_true",
-                    help="profiling aid: run only the single-launch encode kernel loop (no JSON line)")
-    ap.add_argument("--int8-ceiling", action="store_true",
-                    help="print the library int8 / bf16 GEMM rates on this GPU and the GF(2^16) MAC ceiling "
-                         "that a bit-sliced int8 tensor-core encode could reach (int8 ops / 512)")
     return ap.parse_args()
-
-
-def int8_ceiling():
-    """A bit-sliced GF(2^16) product spends 16 x 16 binary products, i.e. 512
-    int8 tensor ops, on every GF MAC, so the best int8 GEMM rate / 512 bounds
-    any tensor-core form of the encode (before its operand expansion and
-    parity reduction).  Timed with CUDA events on cuBLAS (torch._int_mm)."""
-    import torch
-
-    dev = torch.device("cuda:0")
-    out = {"metric": "int8 tensor-core ceiling for the GF(2^16) encode", "int8": [], "unit": "GF(2^16) MAC/s"}
-
-    def timed(fn, n=20):
-        for _ in range(3):
-            fn()
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(n):
-            fn()
-        b.record()
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / n
-
-    for M, N, K in [(8192, 8192, 8192), (16384, 16384, 8192), (4096, 16384, 16384)]:
-        x = torch.randint(-128, 127, (M, K), dtype=torch.int8, device=dev)
-        y = torch.randint(-128, 127, (K, N), dtype=torch.int8, device=dev).t().contiguous().t()
-        ms = timed(lambda: torch._int_mm(x, y))
-        tops = 2 * M * N * K / (ms * 1e-3)
-        out["int8"].append({"shape": [M, N, K], "ms": ms, "tops": tops / 1e12, "gf_mac_ceiling": tops / 512})
-    x = torch.randn(8192, 8192, dtype=torch.bfloat16, device=dev)
-    ms = timed(lambda: x @ x)
-    out["bf16_tflops"] = 2 * 8192 ** 3 / (ms * 1e-3) / 1e12
-    out["value"] = max(r["gf_mac_ceiling"] for r in out["int8"])
-    out["bitsliced_encode"] = bitsliced_encode_probe(timed)
-    print(json.dumps(out))
-    return 0
-
-
-def bitsliced_encode_probe(timed, S=256, slice_=65536, R=200):
-    """The encode as a bit-sliced GF(2) product on the int8 tensor cores
-    (cuBLAS through torch._int_mm), checked bit-exact against the library's
-    LUT encode on the same device slices and timed beside it.
-
-    Coefficient c(r,s) becomes a 16 x 16 bit matrix (column j = the bits of
-    c*2^j), so A[16r+i, 16s+j] = bit i of c(r,s)*2^j; the sources become bit
-    planes B[16s+j, n] = bit j of symbol n of slice s; bit i of recovery
-    symbol (r, n) is the parity of (A @ B)[16r+i, n]."""
-    import numpy as np
-    import torch
-
-    import par2rust_b200 as p2g
-
-    dev = torch.device("cuda:0")
-    N = slice_ // 2
-    g = torch.Generator(device=dev)
-    g.manual_seed(5)
-    src = torch.randint(0, 256, (S * slice_,), dtype=torch.uint8, device=dev, generator=g)
-    rec = torch.empty(R * slice_, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream().cuda_stream
-    lut_ms = timed(lambda: p2g.encode_device(src.data_ptr(), slice_, S, slice_, R, rec.data_ptr(), slice_, stream))
-    # GF(2^16) tables (generator 2, polynomial 0x1100B) and the coefficient bit matrices
-    al = np.zeros(65536, np.int64)
-    v = 1
-    for k in range(65535):
-        al[k] = v
-        v <<= 1
-        if v & 0x10000:
-            v ^= 0x1100B
-    lg = np.zeros(65536, np.int64)
-    lg[al[:65535]] = np.arange(65535)
-    bases = p2g.input_bases(S)
-    coef = np.array([[p2g.gf_pow(b, r) for b in bases] for r in range(R)], np.int64)
-    prod = al[(lg[coef][:, :, None] + np.arange(16)) % 65535]          # [R, S, j]
-    bits = ((prod[:, :, :, None] >> np.arange(16)) & 1).astype(np.int8)  # [R, S, j, i]
-    A = torch.from_numpy(np.ascontiguousarray(bits.transpose(0, 3, 1, 2).reshape(16 * R, 16 * S))).to(dev)
-    b2 = src.view(S, N, 2).to(torch.int32)
-    sym = b2[:, :, 0] | (b2[:, :, 1] << 8)                               # [S, N]
-    sh = torch.arange(16, device=dev, dtype=torch.int32)
-    st = {}
-
-    def expand():
-        st["Bt"] = ((sym.t()[:, :, None] >> sh) & 1).to(torch.int8).reshape(N, 16 * S)
-
-    def gemm():
-        st["C"] = torch._int_mm(A, st["Bt"].t())
-
-    def reduce():
-        par = (st["C"] & 1).view(R, 16, N)
-        st["out"] = (par << sh[None, :, None]).sum(1, dtype=torch.int32)
-
-    ms_e, ms_g, ms_r = timed(expand, 5), timed(gemm, 5), timed(reduce, 5)
-    r2 = rec.view(R, N, 2).to(torch.int32)
-    identical = bool(torch.equal(st["out"], r2[:, :, 0] | (r2[:, :, 1] << 8)))
-    macs = R * S * N
-    total = ms_e + ms_g + ms_r
-    return {"shape": {"slices": S, "slice_bytes": slice_, "recovery": R}, "identical_to_lut": identical,
-            "expand_ms": ms_e, "gemm_ms": ms_g, "parity_pack_ms": ms_r, "total_ms": total,
-            "gf_mac_per_s": macs / (total * 1e-3), "gemm_only_gf_mac_per_s": macs / (ms_g * 1e-3),
-            "lut_encode_ms": lut_ms, "lut_gf_mac_per_s": macs / (lut_ms * 1e-3)}
 
 
 def dist_env():
@@ -328,6 +227,36 @@ def batch_specs(dev, n_jobs=256, seed=4):
     return jobs, specs
 
 
+def batch_parity(jobs, specs, snap, seed=4, n_sample=8, max_macs=3e11):
+    """Oracle check of a seeded sample of the batch's jobs (every recovery
+    row, slice checksum, hash16k, set id and packet MD5 of each), drawn
+    among jobs whose CPU encode stays within the budget."""
+    import random
+
+    from oracle import parity
+    from par2rust_b200 import workloads as W
+
+    cost = lambda j: j.slices * j.recovery * (j.slice_size // 2)
+    cand = [k for k, j in enumerate(jobs) if cost(j) <= max_macs / n_sample]
+    pick = sorted(random.Random(seed).sample(cand, min(n_sample, len(cand))))
+    t0 = time.perf_counter()
+    bad = {}
+    for k in pick:
+        j, sp = jobs[k], specs[k]
+        rec, ck, h16, pkt, sid = snap[k]
+        R, S, n = j.recovery, j.slices, len(j.file_lengths)
+        files = [W.file_bytes(sd, ln) for ln, sd in zip(j.file_lengths, j.seeds)]
+        rows = rec.view(-1, sp.bufs.rec_stride)[:R, :j.slice_size].cpu().numpy()
+        b = parity.check_device_job(files, sp.names, j.slice_size, R, rows, ck[:20 * S].cpu().numpy(),
+                                    h16[:16 * n].cpu().numpy().reshape(n, 16), sid, pkt[:16 * R].cpu().numpy())
+        if b:
+            bad[k] = b[:5]
+    return {"result": "bit-exact" if not bad else "MISMATCH", "jobs_checked": pick,
+            "macs_checked": sum(cost(jobs[k]) for k in pick), "seconds": time.perf_counter() - t0,
+            "what": "every recovery row (GFNI port), slice MD5/CRC32, hash16k, set id and packet MD5 of each "
+                    "sampled job against the oracle", "mismatches": bad}
+
+
 def bench_batch(dev, steps, warmup, plain_steps=1, n_jobs=256, e2e_steps=0):
     """Batched persistent launch vs the same jobs run one after another through
     the plain per-job device path (p2g_run_device_job), both with the sources
@@ -384,7 +313,9 @@ def bench_batch(dev, steps, warmup, plain_steps=1, n_jobs=256, e2e_steps=0):
         same &= torch.equal(rec.view(-1, rs)[:R, :s.slice_size], s.bufs.recovery.view(-1, rs)[:R, :s.slice_size])
         same &= torch.equal(ck, s.bufs.checksums) and torch.equal(h16, s.bufs.hash16k)
         same &= torch.equal(pkt[:16 * R], s.bufs.packet_md5[:16 * R]) and sid == s.bufs.set_id
+    par = batch_parity(jobs, specs, snap)
     out = {
+        "parity": par,
         "workload": f"batch_{n_jobs} (mixed jobs: 1-16 files log-uniform in [4 KiB, 64 MiB], slice in "
                     "{16K,64K,256K,1M}, R 1-20% of slices, seed 4)",
         "jobs": n_jobs, "files": sum(len(j.file_lengths) for j in jobs), "source_bytes": total,
@@ -536,24 +467,23 @@ def serve_run(srv, jobs, arrivals, p2g):
             "mean_ms": sum(lat) / len(lat) * 1e3, "max_ms": lat[-1] * 1e3, "d2h_bytes": d2h[0]}
 
 
-def run_serve(args, wl):
-    import torch
-
+def bench_serve(requests, rate_fracs=(0.5, 0.8, 0.95), rates=None, probe_jobs=200, wave_ms=20.0, seed=5,
+                local=0):
+    """The serving loop on the request mix: a closed-batch capacity probe,
+    then open-loop Poisson arrivals at each rate (fractions of that capacity
+    unless explicit rates are given).  Returns the sweep and its clocks."""
     import par2rust_b200 as p2g
     from par2rust_b200 import workloads as W
 
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    jobs = W.serve_requests(args.requests, seed=wl["seed"])
+    jobs = W.serve_requests(requests, seed=seed)
     budget = 120_000_000_000
-    srv = p2g.Server(hbm_budget=budget, wave_ms=args.wave_ms)
+    srv = p2g.Server(hbm_budget=budget, wave_ms=wave_ms)
     clocks = ClockSampler(local)
     clocks.start()
-    # capacity: a closed batch of the first probe jobs, all submitted at once
-    probe = jobs[:min(args.probe_jobs, len(jobs))]
+    probe = jobs[:min(probe_jobs, len(jobs))]
     pr = serve_run(srv, probe, [0.0] * len(probe), p2g)
     cap_jobs = pr["jobs_per_s"]
-    rates = [float(x) for x in args.rates.split(",") if x] or [f * cap_jobs for f in (0.5, 0.8, 0.95)]
+    rates = list(rates) if rates else [f * cap_jobs for f in rate_fracs]
     sweep = []
     for ri, rate in enumerate(rates):
         arr = W.poisson_arrivals(len(jobs), rate, seed=100 + ri)
@@ -566,44 +496,60 @@ def run_serve(args, wl):
         sweep.append(res)
         print(json.dumps({"serve_point": res}), file=sys.stderr, flush=True)
     clk = clocks.stop()
-    launches = srv.stats()["waves"]
+    waves = srv.stats()["waves"]
     srv.close()
+    return {
+        "workload": f"serve: {len(jobs)} requests per rate, totals log-uniform [1 MiB, 2 GiB] in 1-32 files, "
+                    "slice {16K,64K,256K,1M} (smallest with <= 32768 slices), R 1-20% of slices, Poisson arrivals",
+        "hbm_budget_bytes": budget, "wave_ms": wave_ms, "requests_per_rate": len(jobs),
+        "total_source_bytes": sum(j.source_bytes for j in jobs), "capacity_probe": pr, "sweep": sweep,
+        "p50_ms": [r["p50_ms"] for r in sweep], "p99_ms": [r["p99_ms"] for r in sweep],
+        "rates_jobs_per_s": [r["rate_jobs_per_s"] for r in sweep], "gbs": [r["gbs"] for r in sweep],
+        "clocks": clk, "waves": waves, "jobs": jobs,
+    }
+
+
+def run_serve(args, wl):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rates = [float(x) for x in args.rates.split(",") if x]
+    res = bench_serve(args.requests, rates=rates, probe_jobs=args.probe_jobs, wave_ms=args.wave_ms, seed=wl["seed"],
+                      local=local)
+    jobs = res.pop("jobs")
     cb = None
     if not args.no_cpu_baseline:
         cb, _ = serve_cpu_baseline(jobs, args.cpu_seconds)
-    top = sweep[-1]
+    top = res["sweep"][-1]
     line = {
         "metric": "serving: source GB/s and p50/p99 job latency per arrival rate", "value": top["gbs"],
-        "unit": "GB/s", "n_gpus": 1, "steps": len(rates), "warmup": 1, "ms_per_step": top["seconds"] * 1e3,
+        "unit": "GB/s", "n_gpus": 1, "steps": len(res["sweep"]), "warmup": 1, "ms_per_step": top["seconds"] * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
         "data": "synthetic (request bytes generated on the device from per-file seeds)",
-        "config": {"workload": f"serve: {len(jobs)} requests, totals log-uniform [1 MiB, 2 GiB] in 1-32 files, "
-                               "slice {16K,64K,256K,1M} (smallest with <= 32768 slices), R 1-20% of slices, "
-                               "Poisson arrivals", "hbm_budget_bytes": budget, "wave_ms": args.wave_ms,
-                   "total_source_bytes": sum(j.source_bytes for j in jobs), "parallelism": "1 GPU"},
-        "capacity_probe": pr, "sweep": sweep,
+        "config": {"workload": res["workload"], "hbm_budget_bytes": res["hbm_budget_bytes"], "wave_ms": args.wave_ms,
+                   "total_source_bytes": res["total_source_bytes"], "parallelism": "1 GPU"},
+        "capacity_probe": res["capacity_probe"], "sweep": res["sweep"],
         "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
         "e2e": {"value": top["gbs"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": top["d2h_bytes"],
                 "note": "host clock from each request's submit to its completion; sources generated on the device"},
-        "roofline": None, "cpu_baseline": cb, "clocks": clk, "gpu_launches": launches,
+        "roofline": None, "cpu_baseline": cb, "clocks": res["clocks"], "gpu_launches": res["waves"],
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_many(args, wl):
-    """--workload many_2000: one create job over 2,000 files with 2,000
-    recovery blocks through the plain per-job device path."""
+def bench_many(dev, steps, warmup, e2e_steps, cpu_seconds, no_cpu_baseline=False, seed=3, parity_rows=32):
+    """many_2000: one create job over 2,000 files with 2,000 recovery blocks
+    through the plain per-job device path; its encode alone with both
+    kernels; e2e through p2g_create_in_memory; a sampled oracle check."""
     import numpy as np
     import torch
 
     import par2rust_b200 as p2g
     from par2rust_b200 import workloads as W
 
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    job = W.many_2000(seed=wl["seed"])
+    job = W.many_2000(seed=seed)
     sl, R, S = job.slice_size, job.recovery, job.slices
     names = [f"file{i:04d}.bin".encode() for i in range(len(job.file_lengths))]
     src = torch.zeros(S * sl, dtype=torch.uint8, device=dev)
@@ -613,84 +559,109 @@ def run_many(args, wl):
         off += (n + sl - 1) // sl * sl
     bufs = p2g.DeviceJobBuffers(S, len(names), sl, R, dev)
     stream = torch.cuda.current_stream(dev)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         p2g.run_device_job(src, job.file_lengths, names, sl, R, bufs, skip_hash_full=True)
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(dev.index or 0)
     clocks.start()
     l0 = p2g.kernel_launch_count()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         p2g.run_device_job(src, job.file_lengths, names, sl, R, bufs, skip_hash_full=True)
     b.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
     launches = p2g.kernel_launch_count() - l0
-    ms = a.elapsed_time(b) / args.steps
+    ms = a.elapsed_time(b) / steps
     total = job.source_bytes
     macs = S * R * (sl // 2)
-    # the encode alone (basis + encode kernels)
-    enc = []
-    for i in range(args.warmup + args.steps):
-        x, y = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        x.record(stream)
-        p2g.encode_device(src.data_ptr(), sl, S, sl, R, bufs.recovery.data_ptr(), bufs.rec_stride, stream.cuda_stream)
-        y.record(stream)
-        torch.cuda.synchronize()
-        if i >= args.warmup:
-            enc.append(x.elapsed_time(y))
-    enc_ms = sum(enc) / len(enc)
-    # e2e: the public in-memory create with pinned host files
-    host = [torch.empty(n, dtype=torch.uint8, pin_memory=True) for n in job.file_lengths]
-    off = 0
-    for h, n in zip(host, job.file_lengths):
-        h.copy_(src[off:off + n])
-        off += (n + sl - 1) // sl * sl
-    opts = p2g.CreateOptions(output="many.par2", slice_size=sl, recovery_block_count=R,
-                             volume_scheme=p2g.VolumeScheme.Uniform(15))
+    # parity of the timed job's outputs (hash_full runs on the host in the timed step)
+    from oracle import parity
+
+    files = [W.file_bytes(sd, n) for n, sd in zip(job.file_lengths, job.seeds)]
+    out = parity.device_outputs(bufs, S, len(names), sl, R)
+    rows = parity.sample_rows(R, parity_rows, seed=seed)
+    t0 = time.perf_counter()
+    bad = parity.check_device_job(files, names, sl, R, out["rec"], out["checks"], out["hash16k"], bufs.set_id,
+                                  out["packet_md5"], rows=rows)
+    par = {"result": "bit-exact" if not bad else "MISMATCH", "rows_checked": rows, "seconds": time.perf_counter() - t0,
+           "what": f"{len(rows)} sampled recovery rows (0, 1 and {R - 1} always), every slice MD5/CRC32, hash16k, "
+                   "the set id and every packet MD5", "mismatches": bad[:10]}
+    # the encode alone, each kernel
+    enc = {}
+    for label, variant in (("lut", p2g.ENCODE_LUT), ("tensor", p2g.ENCODE_TENSOR)):
+        ts = []
+        for i in range(warmup + steps):
+            x, y = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            x.record(stream)
+            p2g.encode_device(src.data_ptr(), sl, S, sl, R, bufs.recovery.data_ptr(), bufs.rec_stride,
+                              stream.cuda_stream, variant=variant)
+            y.record(stream)
+            torch.cuda.synchronize()
+            if i >= warmup:
+                ts.append(x.elapsed_time(y))
+        enc[label] = sum(ts) / len(ts)
     e2e = None
-    if args.e2e_steps:
+    if e2e_steps:
+        host = [torch.empty(n, dtype=torch.uint8, pin_memory=True) for n in job.file_lengths]
+        for h, f in zip(host, files):
+            h.numpy()[:] = f
+        opts = p2g.CreateOptions(output="many.par2", slice_size=sl, recovery_block_count=R,
+                                 volume_scheme=p2g.VolumeScheme.Uniform(15))
         inputs = list(zip(names, host))
         p2g.create_in_memory(opts, inputs, copy=False)
         t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            files = None  # the previous step's outputs are freed before the next step
-            files = p2g.create_in_memory(opts, inputs, copy=False)
-        es = (time.perf_counter() - t0) / args.e2e_steps
+        for _ in range(e2e_steps):
+            got = None  # the previous step's outputs are freed before the next step
+            got = p2g.create_in_memory(opts, inputs, copy=False)
+        es = (time.perf_counter() - t0) / e2e_steps
         e2e = {"value": total / es / 1e9, "unit": "GB/s", "h2d_bytes_per_step": total,
                "d2h_bytes_per_step": R * sl + S * 20 + 16 * R, "seconds_per_step": es,
                "api": "p2g_create_in_memory (2,000 pinned host files; volumes returned as views "
-                      "of the library's buffers, copy=False)", "output_files": len(files)}
+                      "of the library's buffers, copy=False)", "output_files": len(got)}
+        del host, got
     cb = None
-    if not args.no_cpu_baseline:
+    if not no_cpu_baseline:
         from oracle import oracle as orc
 
-        # a bounded prefix of the concatenated files, same slice and R
-        data = np.concatenate([h.numpy() for h in host[:200]])
-        n_sl = max(1, min(len(data) // sl, int(args.cpu_seconds * 4)))
+        data = np.concatenate(files[:200])
+        n_sl = max(1, min(len(data) // sl, int(cpu_seconds * 4)))
         sample = data[:n_sl * sl]
         t, *_ = orc.create_timed(sample, sl, R, 0)
         cb = {"value": len(sample) / t / 1e9, "unit": "GB/s", "cores": orc.max_threads(), "kind": "port",
               "sample": f"{n_sl} slices ({len(sample)} B) of the first files, R={R}", "seconds": t}
-    hbm_peak, peak_kind = measured_peaks()
-    alg = S * sl + R * sl
+    del src, bufs
+    torch.cuda.empty_cache()
+    lut_peak = 32 * 148 * 1965e6
+    return {
+        "workload": "many_2000: 2,000 files log-uniform [1 KiB, 8 MiB], slice 262,144, R 2,000, Uniform{15}",
+        "files": len(names), "source_bytes": total, "input_slices": S, "recovery_blocks": R, "gf_macs": macs,
+        "value": total / (ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": ms, "steps": steps,
+        "encode_only_ms": enc, "encode_gf_mac_per_s": {k: macs / (v * 1e-3) for k, v in enc.items()},
+        "lut_frac_of_lookup_bound": macs / (enc["lut"] * 1e-3) / lut_peak,
+        "e2e": e2e, "parity": par, "cpu_baseline": cb, "clocks": clk, "gpu_launches": launches,
+    }
+
+
+def run_many(args, wl):
+    """--workload many_2000: the dense-contraction job as the measured step."""
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    res = bench_many(dev, args.steps, args.warmup, args.e2e_steps, args.cpu_seconds, args.no_cpu_baseline,
+                     seed=wl["seed"])
     line = {
-        "metric": "encode source GB/s", "value": total / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "metric": "encode source GB/s", "value": res["value"], "unit": "GB/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": {"workload": "many_2000: 2,000 files log-uniform [1 KiB, 8 MiB], slice 262,144, R 2,000, "
-                               "Uniform{15}", "files": len(names), "source_bytes": total, "input_slices": S,
-                   "recovery_blocks": R, "parallelism": "1 GPU"},
-        "e2e": e2e,
-        "roofline": {"bound": "hbm", "achieved": alg / (enc_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": alg / (enc_ms * 1e-3) / 1e9 / hbm_peak, "traffic": None, "peak_source": peak_kind,
-                     "kernel": "basis_kernel + encode_lut_kernel", "kernel_ms": enc_ms, "algorithmic_bytes": alg},
-        "lut_roofline": {"achieved": macs / (enc_ms * 1e-3), "peak": 32 * 148 * 1965e6, "unit": "GF(2^16) MAC/s",
-                         "frac": macs / (enc_ms * 1e-3) / (32 * 148 * 1965e6), "macs_per_launch": macs},
-        "variant": "LUT (int8 bit-sliced tensor form not built: its shared-memory operand traffic per GF MAC is "
-                   "not below the packed LUT's)",
-        "cpu_baseline": cb, "clocks": clk, "gpu_launches": launches,
+        "config": {"workload": res["workload"], "files": res["files"], "source_bytes": res["source_bytes"],
+                   "input_slices": res["input_slices"], "recovery_blocks": res["recovery_blocks"],
+                   "parallelism": "1 GPU"},
+        "e2e": res["e2e"], "parity": res["parity"]["result"], "many_2000": res,
+        "cpu_baseline": res["cpu_baseline"], "clocks": res["clocks"], "gpu_launches": res["gpu_launches"],
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -802,8 +773,6 @@ def run_batch(args, wl):
 
 def main():
     args = parse()
-    if args.int8_ceiling:
-        return int8_ceiling()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         if wl.get("serve"):
@@ -883,17 +852,6 @@ def main():
         if world > 1:
             dist.barrier()
 
-    if args.only_encode:  # profiling aid: the encode kernel alone, warmup + steps launches
-        for _ in range(args.warmup + args.steps):
-            p2g.encode_device(src.data_ptr(), slice_, S, slice_, R, bufs.recovery.data_ptr(), bufs.rec_stride,
-                              stream.cuda_stream)
-        torch.cuda.synchronize()
-        return 0
-    if args.only_step:  # profiling aid: the device job alone (basis + batch_kernel per step)
-        for _ in range(args.warmup + args.steps):
-            p2g.run_device_job(src, [L], [name], slice_, R, bufs, skip_hash_full=True)
-        torch.cuda.synchronize()
-        return 0
 
     # ---- value: device-resident job ----
     for _ in range(args.warmup):
@@ -920,38 +878,46 @@ def main():
     ms_max = float(t.item())
     value = world * L / (ms_max * 1e-3) / 1e9
 
-    # ---- roofline: the encode kernel alone ----
-    enc_ms = []
-    for i in range(args.warmup + args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        p2g.encode_device(src.data_ptr(), slice_, S, slice_, R, bufs.recovery.data_ptr(), bufs.rec_stride,
-                          stream.cuda_stream)
-        b.record(stream)
-        torch.cuda.synchronize()
-        if i >= args.warmup:
-            enc_ms.append(a.elapsed_time(b))
-    enc = sum(enc_ms) / len(enc_ms)
-    # the same encode with the coefficient basis derived inside the kernel
-    # (P2G_ENCODE_BASIS=derive: no basis launch, no basis scratch)
-    os.environ["P2G_ENCODE_BASIS"] = "derive"
-    der_ms = []
-    for i in range(args.warmup + args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        p2g.encode_device(src.data_ptr(), slice_, S, slice_, R, bufs.recovery.data_ptr(), bufs.rec_stride,
-                          stream.cuda_stream)
-        b.record(stream)
-        torch.cuda.synchronize()
-        if i >= args.warmup:
-            der_ms.append(a.elapsed_time(b))
-    del os.environ["P2G_ENCODE_BASIS"]
-    enc_derive = sum(der_ms) / len(der_ms)
+    # ---- parity of the timed step: every output of the last step ----
+    parity_res = None
+    if rank == 0 and not args.no_parity:
+        from oracle import parity
+
+        t0 = time.perf_counter()
+        data_np = src[:L].cpu().numpy()
+        out = parity.device_outputs(bufs, S, 1, slice_, R)
+        bad = parity.check_device_job([data_np], [name], slice_, R, out["rec"], out["checks"], out["hash16k"],
+                                      bufs.set_id, out["packet_md5"])
+        parity_res = {"result": "bit-exact" if not bad else "MISMATCH", "seconds": time.perf_counter() - t0,
+                      "what": "the last timed step's outputs: all recovery rows (oracle GFNI port, pinned to the "
+                              "scalar restatement), every slice MD5/CRC32, hash16k, the set id and every packet MD5",
+                      "mismatches": bad[:10]}
+        del data_np, out
+
+    # ---- the encode alone, each kernel (CUDA events per launch) ----
+    def encode_ms(variant, env=None):
+        if env:
+            os.environ.update(env)
+        ts = []
+        for i in range(args.warmup + args.steps):
+            x, y = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            x.record(stream)
+            p2g.encode_device(src.data_ptr(), slice_, S, slice_, R, bufs.recovery.data_ptr(), bufs.rec_stride,
+                              stream.cuda_stream, variant=variant)
+            y.record(stream)
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                ts.append(x.elapsed_time(y))
+        for k in env or {}:
+            del os.environ[k]
+        return sum(ts) / len(ts)
+
+    enc_lut = encode_ms(p2g.ENCODE_LUT)
+    enc_derive = encode_ms(p2g.ENCODE_LUT, {"P2G_ENCODE_BASIS": "derive"})
+    enc_tensor = encode_ms(p2g.ENCODE_TENSOR)
     hbm_peak, peak_kind = measured_peaks()
     alg_bytes = S * slice_ + R * slice_  # padded source read once + recovery written once
-    achieved = alg_bytes / (enc * 1e-3) / 1e9
     macs = S * R * (slice_ // 2)
-    sm_mhz = clk.get("sm_mhz") or 1965.0
     lut_peak = 32 * 148 * 1965e6  # 2 shared-memory u16 lookups per MAC at 128 B/clk/SM, max clock
     traffic = None  # DRAM bytes per batch_kernel launch (ncu, profiles/)
     tp = os.path.join(ROOT, "profiles", "batch_kernel_traffic.json")
@@ -1015,11 +981,26 @@ def main():
         p2g.run_device_job(src[:64 * 1024 * 1024], [64 * 1024 * 1024], [name], slice_, 0, None)
         torch.cuda.synchronize()
         chain_gbs = 64 * 1024 * 1024 / (time.perf_counter() - t0) / 1e9
+    del src, bufs
+    torch.cuda.empty_cache()
 
     # ---- batched persistent launch vs the plain path on the mixed batch ----
     batched = None
     if world == 1 and not args.no_batch:
         batched = bench_batch(dev, args.steps, args.warmup, plain_steps=1, n_jobs=args.batch_jobs)
+
+    # ---- the dense contraction: 2,000 files, R 2,000 ----
+    many = None
+    if world == 1 and not args.no_many:
+        many = bench_many(dev, max(2, args.steps // 3), args.warmup, 1 if args.e2e_steps else 0,
+                          max(2.0, args.cpu_seconds / 3), args.no_cpu_baseline)
+
+    # ---- serving: p50/p99 job latency at two arrival rates ----
+    serving = None
+    if world == 1 and args.serve_requests > 0:
+        serving = bench_serve(args.serve_requests, rate_fracs=tuple(float(x) for x in args.serve_fracs.split(",")),
+                              local=local)
+        serving.pop("jobs")
 
     # ---- CPU baseline (rank 0, N=1) ----
     cb = None
@@ -1035,34 +1016,44 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    step_macs = macs / (ms_max * 1e-3)
     line = {
         "metric": "encode source GB/s", "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": value / PUBLISHED_E2E_GBS, "dtype": "u16", "data": "synthetic",
         "config": config_dict(args, wl),
+        "parity": parity_res["result"] if parity_res else None,
+        "parity_detail": parity_res,
         "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": L, "d2h_bytes_per_step": d2h,
                 "seconds_per_step": e2e_s, "api": "p2g_create_in_memory (pinned host source; volumes returned as views of "
                 "the library's buffers, copy=False)",
                 "output_files": len(files)},
         "e2e_files": e2e_files,
-        "roofline": {"bound": "hbm", "achieved": alg_bytes / (ms_max * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": alg_bytes / (ms_max * 1e-3) / 1e9 / hbm_peak, "traffic": traffic,
-                     "peak_source": peak_kind,
-                     "kernel": "batch_kernel (one launch per step: encode, slice MD5/CRC32, packet-MD5 chains) "
+        # the binding unit of the timed step: the encode items' shared-memory lookups
+        "roofline": {"bound": "smem", "achieved": step_macs, "peak": lut_peak, "unit": "GF(2^16) MAC/s",
+                     "frac": step_macs / lut_peak, "traffic": traffic,
+                     "peak_source": "computed: 2 shared-memory u16 lookups per GF MAC at 128 B/clk/SM, 148 SMs, "
+                                    "1965 MHz (the lookup kernel's design bound)",
+                     "kernel": "batch_kernel (one launch per step: encode items, slice MD5/CRC32, packet-MD5 chains) "
                                "+ basis_kernel; timed per step with events on the launching stream",
-                     "kernel_ms": ms_max, "algorithmic_bytes": alg_bytes},
-        "lut_roofline": {"bound": "shared-memory lookups (2 u16 per GF MAC, 128 B/clk/SM, 148 SMs, 1965 MHz)",
-                         "achieved": macs / (ms_max * 1e-3), "peak": lut_peak, "unit": "GF(2^16) MAC/s",
-                         "frac": macs / (ms_max * 1e-3) / lut_peak, "macs_per_launch": macs,
-                         "encode_only": {"kernel": "basis_kernel + encode_lut_kernel (p2g_encode, one launch)",
-                                         "kernel_ms": enc, "frac": macs / (enc * 1e-3) / lut_peak,
-                                         "hbm_achieved_gbs": achieved,
-                                         "kernel_ms_basis_derived": enc_derive}},
+                     "kernel_ms": ms_max, "macs_per_launch": macs},
+        "hbm_roofline": {"bound": "hbm", "achieved": alg_bytes / (ms_max * 1e-3) / 1e9, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": alg_bytes / (ms_max * 1e-3) / 1e9 / hbm_peak, "traffic": traffic,
+                         "peak_source": peak_kind, "algorithmic_bytes": alg_bytes},
+        "encode_only": {
+            "lut": {"kernel": "basis_kernel + encode_lut_kernel (p2g_encode, one launch)", "kernel_ms": enc_lut,
+                    "gf_mac_per_s": macs / (enc_lut * 1e-3), "frac_of_lookup_bound": macs / (enc_lut * 1e-3) / lut_peak,
+                    "kernel_ms_basis_derived": enc_derive},
+            "tensor": {"kernel": "tc_coef_kernel + encode_mma_kernel (tcgen05 kind::mxf4, p2g_encode)",
+                       "kernel_ms": enc_tensor, "gf_mac_per_s": macs / (enc_tensor * 1e-3),
+                       "e2m1_tflops": 2 * 256 * macs / (enc_tensor * 1e-3) / 1e12}},
         "cpu_baseline": cb,
         "clocks": clk,
         "gpu_launches": launches,
         "file_md5_device_chain_gbs": chain_gbs,
         "batched": batched,
+        "many_2000": many,
+        "serving": serving,
         "device": info,
         "baseline_note": "vs_baseline divides by the reference's published end-to-end create rate for this "
                          "shape (0.0975 GB/s, Apple M4, 10 threads)",

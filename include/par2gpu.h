@@ -241,6 +241,11 @@ p2g_status p2g_gf_mul_xor(uint16_t coeff, const uint8_t *input, uint8_t *output,
  * bounded device wait gave up (the rows are then not valid); without it a
  * device timeout is not reported. */
 #define P2G_ENCODE_WAIT 4u
+/* Encode kernel: by default chosen per shape; these force the shared-memory
+ * lookup kernel or the tensor-core (tcgen05) bit-sliced kernel.  Both give
+ * the same bytes. */
+#define P2G_ENCODE_LUT 8u
+#define P2G_ENCODE_TENSOR 16u
 typedef struct p2g_encode_job {
     const uint8_t *src;
     uint64_t src_stride;
@@ -522,6 +527,51 @@ void p2g_compute_file_id(const uint8_t hash16k[16], uint64_t length, const uint8
                          size_t name_len, uint8_t out[16]);
 /* host MD5 used for packet framing (md5_impl::digest, src/md5_impl.rs:24-48) */
 void p2g_md5(const uint8_t *data, size_t len, uint8_t out[16]);
+
+/* ---- create CLI glue (src/main.rs) ------------------------------------
+ * The argument semantics of `par2rust create`: they decide the bytes a
+ * create writes (-r sets the recovery count, -l caps volume sizes).  The
+ * par2rust executable built beside libpar2gpu.so is a shell around these
+ * and the create entry points above.  Errors carry the reference's texts. */
+
+/* parse_slice_size, src/main.rs:464-487: a bare integer (bytes) or one with
+ * a suffix b/B (bytes), k/K (KiB), m/M (MiB), g/G (GiB).  Bad input:
+ * P2G_ERR_INVALID_ARGUMENT. */
+p2g_status p2g_parse_slice_size(const char *s, uint64_t *out);
+
+/* Redundancy, src/main.rs:489-531: the `-r` value, a percentage of the
+ * input ("10") or a target recovery-data size with a unit prefix ("k500",
+ * "m10", "g2"; case-insensitive).  Bad input: P2G_ERR_INVALID_ARGUMENT. */
+typedef struct p2g_redundancy {
+    uint32_t is_bytes;     /* 0: Percent(percent), 1: TargetBytes(target_bytes) */
+    uint32_t percent;
+    uint64_t target_bytes;
+} p2g_redundancy;
+p2g_status p2g_parse_redundancy(const char *s, p2g_redundancy *out);
+
+/* resolve_redundancy, src/main.rs:533-556: the recovery count for inputs of
+ * `total_input_blocks` slices: ceil(total * percent / 100) or
+ * ceil(target_bytes / slice_size), saturated to u32; 0 blocks is
+ * P2G_ERR_INVALID_VOLUME_SCHEME. */
+p2g_status p2g_resolve_redundancy(const p2g_redundancy *r, uint64_t total_input_blocks,
+                                  uint64_t slice_size, uint32_t *out);
+
+/* build_volume_scheme, src/main.rs:289-337: the VolumeScheme of the
+ * --single-volume / -u / -l / -n flags.  -u without -n uses
+ * clamp(recovery_count, 1, 15) volumes; -l wraps the scheme in Limited with
+ * max(largest_source_length / slice_size, 1) blocks per volume, its inner
+ * scheme written to *inner_out (out->inner points there).  Conflicting flags:
+ * P2G_ERR_INVALID_VOLUME_SCHEME. */
+typedef struct p2g_cli_volume_flags {
+    uint32_t single_volume;
+    uint32_t uniform;          /* -u */
+    uint32_t limit_size;       /* -l */
+    uint32_t has_volume_count; /* -n given */
+    uint32_t volume_count;
+} p2g_cli_volume_flags;
+p2g_status p2g_build_volume_scheme(const p2g_cli_volume_flags *flags, uint64_t largest_source_length,
+                                   uint64_t slice_size, uint32_t recovery_count,
+                                   p2g_volume_scheme *out, p2g_volume_scheme *inner_out);
 
 /* ---- device / runtime info ------------------------------------------- */
 /* Number of kernel launches this process has issued through the library

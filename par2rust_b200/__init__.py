@@ -28,6 +28,8 @@ HOST_POINTERS = 0
 DEVICE_POINTERS = 1
 JOB_SKIP_HASH_FULL = 2
 ENCODE_WAIT = 4  # p2g_encode / p2g_encode_noalloc: wait and report a device timeout
+ENCODE_LUT = 8  # p2g_encode: force the shared-memory lookup kernel
+ENCODE_TENSOR = 16  # p2g_encode: force the tensor-core (tcgen05) bit-sliced kernel
 
 
 # ---------------------------------------------------------------------------
@@ -479,7 +481,8 @@ def gf_mul_xor(coeff: int, input: bytes, output: bytearray) -> None:
     _check(lib().p2g_gf_mul_xor(int(coeff), inp.ctypes.data, out.ctypes.data, len(inp), HOST_POINTERS, None))
 
 
-def encode(src, slice_size: int, recovery_count: int, first_exponent: int = 0, input_count: Optional[int] = None):
+def encode(src, slice_size: int, recovery_count: int, first_exponent: int = 0, input_count: Optional[int] = None,
+           variant: int = 0):
     """encode_all_recovery_blocks over host memory: src holds input_count
     zero-padded slices back to back; returns recovery bytes (R*slice)."""
     import numpy as np
@@ -490,18 +493,21 @@ def encode(src, slice_size: int, recovery_count: int, first_exponent: int = 0, i
     out = np.zeros(recovery_count * slice_size, dtype=np.uint8)
     job = _ffi.p2g_encode_job(src=a.ctypes.data, src_stride=slice_size, input_count=S, slice_size=slice_size,
                               recovery_count=recovery_count, first_exponent=first_exponent,
-                              recovery=out.ctypes.data, recovery_stride=slice_size, flags=HOST_POINTERS, stream=None)
+                              recovery=out.ctypes.data, recovery_stride=slice_size, flags=HOST_POINTERS | variant,
+                              stream=None)
     _check(lib().p2g_encode(C.byref(job)))
     return out
 
 
 def encode_device(src_ptr: int, src_stride: int, input_count: int, slice_size: int, recovery_count: int,
-                  rec_ptr: int, rec_stride: int, stream: int = 0, first_exponent: int = 0, wait: bool = False) -> None:
+                  rec_ptr: int, rec_stride: int, stream: int = 0, first_exponent: int = 0, wait: bool = False,
+                  variant: int = 0) -> None:
     """p2g_encode on device buffers, enqueued on `stream`; with wait=True
-    the call waits for it and raises DeviceTimeout if a device wait gave up."""
+    the call waits for it and raises DeviceTimeout if a device wait gave up.
+    variant: 0 (chosen by shape), ENCODE_LUT or ENCODE_TENSOR."""
     job = _ffi.p2g_encode_job(src=src_ptr, src_stride=src_stride, input_count=input_count, slice_size=slice_size,
                               recovery_count=recovery_count, first_exponent=first_exponent, recovery=rec_ptr,
-                              recovery_stride=rec_stride, flags=DEVICE_POINTERS | (ENCODE_WAIT if wait else 0),
+                              recovery_stride=rec_stride, flags=DEVICE_POINTERS | (ENCODE_WAIT if wait else 0) | variant,
                               stream=stream or None)
     _check(lib().p2g_encode(C.byref(job)))
 
@@ -947,6 +953,71 @@ def batch_plan(shapes: Sequence[Tuple[int, int, int, int]], ctas: int = 148, fla
 # ---------------------------------------------------------------------------
 # Host helpers of the reference's public modules
 # ---------------------------------------------------------------------------
+# ---------------------------------------------------------------------------
+# Create CLI glue (src/main.rs): the par2rust executable beside the library
+# is a shell around these.
+# ---------------------------------------------------------------------------
+CLI_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "par2rust")
+
+
+def parse_slice_size(s: str) -> int:
+    """parse_slice_size (src/main.rs:464-487); InvalidArgument on bad input."""
+    v = C.c_uint64()
+    _check(lib().p2g_parse_slice_size(s.encode(), C.byref(v)))
+    return v.value
+
+
+@dataclass(frozen=True)
+class Redundancy:
+    """The -r value (src/main.rs:489-531): Percent(percent) or TargetBytes(target_bytes)."""
+    percent: Optional[int] = None
+    target_bytes: Optional[int] = None
+
+    @staticmethod
+    def parse(s: str) -> "Redundancy":
+        r = _ffi.p2g_redundancy()
+        _check(lib().p2g_parse_redundancy(s.encode(), C.byref(r)))
+        return Redundancy(target_bytes=r.target_bytes) if r.is_bytes else Redundancy(percent=r.percent)
+
+    def _to_c(self) -> "_ffi.p2g_redundancy":
+        r = _ffi.p2g_redundancy()
+        if self.target_bytes is not None:
+            r.is_bytes, r.target_bytes = 1, self.target_bytes
+        else:
+            r.percent = self.percent
+        return r
+
+
+def resolve_redundancy(r: Redundancy, total_input_blocks: int, slice_size: int) -> int:
+    """resolve_redundancy (src/main.rs:533-556) for inputs of this many slices."""
+    out = C.c_uint32()
+    c = r._to_c()
+    _check(lib().p2g_resolve_redundancy(C.byref(c), total_input_blocks, slice_size, C.byref(out)))
+    return out.value
+
+
+def build_volume_scheme(single_volume: bool = False, uniform: bool = False, limit_size: bool = False,
+                        volume_count: Optional[int] = None, largest_source_length: int = 0, slice_size: int = 4096,
+                        recovery_count: int = 0) -> VolumeScheme:
+    """build_volume_scheme (src/main.rs:289-337) from the CLI's volume flags."""
+    f = _ffi.p2g_cli_volume_flags(int(single_volume), int(uniform), int(limit_size), int(volume_count is not None),
+                                  volume_count or 0)
+    out, inner = _ffi.p2g_volume_scheme(), _ffi.p2g_volume_scheme()
+    _check(lib().p2g_build_volume_scheme(C.byref(f), largest_source_length, slice_size, recovery_count, C.byref(out),
+                                         C.byref(inner)))
+
+    def conv(sc):
+        if sc.kind == 0:
+            return VolumeScheme.Single()
+        if sc.kind == 1:
+            return VolumeScheme.Exponential()
+        if sc.kind == 2:
+            return VolumeScheme.Uniform(sc.count)
+        return VolumeScheme.Limited(sc.max_blocks_per_volume, conv(inner))
+
+    return conv(out)
+
+
 def input_bases(count: int) -> List[int]:
     arr = (C.c_uint16 * max(count, 1))()
     _check(lib().p2g_input_bases(count, arr))

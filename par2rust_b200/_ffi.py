@@ -241,6 +241,15 @@ class p2g_server_stats(C.Structure):
     ]
 
 
+class p2g_redundancy(C.Structure):
+    _fields_ = [("is_bytes", C.c_uint32), ("percent", C.c_uint32), ("target_bytes", C.c_uint64)]
+
+
+class p2g_cli_volume_flags(C.Structure):
+    _fields_ = [("single_volume", C.c_uint32), ("uniform", C.c_uint32), ("limit_size", C.c_uint32),
+                ("has_volume_count", C.c_uint32), ("volume_count", C.c_uint32)]
+
+
 # (name, restype, argtypes) for every entry point of include/par2gpu.h
 SIGNATURES = [
     ("p2g_last_error_message", C.c_char_p, []),
@@ -308,6 +317,12 @@ SIGNATURES = [
     ("p2g_build_main_packet", C.c_size_t, [C.c_uint64, C.c_char_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("p2g_compute_file_id", None, [C.c_char_p, C.c_uint64, C.c_char_p, C.c_size_t, C.c_void_p]),
     ("p2g_md5", None, [C.c_char_p, C.c_size_t, C.c_void_p]),
+    ("p2g_parse_slice_size", C.c_int, [C.c_char_p, C.POINTER(C.c_uint64)]),
+    ("p2g_parse_redundancy", C.c_int, [C.c_char_p, C.POINTER(p2g_redundancy)]),
+    ("p2g_resolve_redundancy", C.c_int, [C.POINTER(p2g_redundancy), C.c_uint64, C.c_uint64, C.POINTER(C.c_uint32)]),
+    ("p2g_build_volume_scheme", C.c_int,
+     [C.POINTER(p2g_cli_volume_flags), C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(p2g_volume_scheme),
+      C.POINTER(p2g_volume_scheme)]),
     ("p2g_kernel_launch_count", C.c_uint64, []),
     ("p2g_device_info", C.c_int, [C.c_char_p, C.c_size_t]),
 ]

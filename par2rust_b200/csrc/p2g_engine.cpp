@@ -90,6 +90,7 @@ struct Context {
     cudaStream_t st[kStreams] = {};
     cudaEvent_t ev_fork = nullptr, ev_h16k = nullptr, ev_join[kStreams] = {}, ev_band[kBandEvents] = {};
     DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out, md5_state;
+    DevBuf tcoef;      // coefficient trace strings of the tensor-core encode
     DevBuf persist;    // single-job persistent run: descriptor, items, chain state, tables
     PinBuf h_spans, h_h16k, h_err, h_stage, h_persist;
     PinBuf h_rec;   // host copy of the recovery rows (create calls)
@@ -203,6 +204,22 @@ static p2g_status join_into(Context& c, cudaStream_t caller) {
 // P2G_ENCODE_BASIS=derive has the encode kernel derive it (no scratch, ~6%
 // more encode time on B200: 512 extra lookups per slice in a loop that is
 // close to its issue limit).
+// Which encode kernel runs a job: the shared-memory lookup kernel or the
+// tensor-core bit-sliced one.  P2G_ENCODE_LUT / P2G_ENCODE_TENSOR (or
+// P2G_ENCODE_VARIANT=lut|tensor) force one; otherwise it is chosen by shape.
+static bool use_tensor_encode(uint32_t flags, uint32_t S, uint32_t R, uint64_t slice_size) {
+    if (flags & P2G_ENCODE_TENSOR) return true;
+    if (flags & P2G_ENCODE_LUT) return false;
+    if (const char* e = getenv("P2G_ENCODE_VARIANT")) {
+        if (!strcmp(e, "tensor")) return true;
+        if (!strcmp(e, "lut")) return false;
+    }
+    (void)S;
+    (void)R;
+    (void)slice_size;
+    return false;
+}
+
 static bool generate_basis() {
     const char* e = getenv("P2G_ENCODE_BASIS");
     return e && !strcmp(e, "derive");
@@ -1077,14 +1094,20 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
             P2G_CU(cudaMemset2DAsync(jb.recovery, jb.recovery_stride, 0, jb.slice_size, R, s));
             return P2G_OK;
         }
-        const bool gen = generate_basis();
-        if (!gen) {
-            P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
-            P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
-        }
         P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s));
-        P2G_CU(launch_encode(jb.src, jb.src_stride, S, gen ? nullptr : c.basis.as<uint16_t>(), RG, R, jb.slice_size,
-                             jb.recovery, jb.recovery_stride, c.err.as<int>(), s, jb.first_exponent));
+        if (use_tensor_encode(jb.flags, S, R, jb.slice_size)) {
+            P2G_CU(c.tcoef.ensure(mma_coef_bytes(S, R)));
+            P2G_CU(launch_encode_mma(jb.src, jb.src_stride, S, jb.slice_size, R, jb.first_exponent,
+                                     c.tcoef.as<uint32_t>(), jb.recovery, jb.recovery_stride, c.err.as<int>(), s));
+        } else {
+            const bool gen = generate_basis();
+            if (!gen) {
+                P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
+                P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
+            }
+            P2G_CU(launch_encode(jb.src, jb.src_stride, S, gen ? nullptr : c.basis.as<uint16_t>(), RG, R,
+                                 jb.slice_size, jb.recovery, jb.recovery_stride, c.err.as<int>(), s, jb.first_exponent));
+        }
         if (jb.flags & P2G_ENCODE_WAIT) {
             P2G_CU(cudaMemcpyAsync(c.h_err.p, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
             P2G_CU(cudaStreamSynchronize(s));
@@ -1100,13 +1123,21 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
     P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s));
     if (S) {
         P2G_CU(cudaMemcpy2DAsync(c.src.p, stride, jb.src, jb.src_stride, jb.slice_size, S, cudaMemcpyHostToDevice, s));
-        const bool gen = generate_basis();
-        if (!gen) {
-            P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
-            P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
+        if (stride != jb.slice_size)  // the 16-byte padding of each row is read: zero it
+            P2G_CU(cudaMemset2DAsync(c.src.as<uint8_t>() + jb.slice_size, stride, 0, stride - jb.slice_size, S, s));
+        if (use_tensor_encode(jb.flags, S, R, jb.slice_size)) {
+            P2G_CU(c.tcoef.ensure(mma_coef_bytes(S, R)));
+            P2G_CU(launch_encode_mma(c.src.as<uint8_t>(), stride, S, jb.slice_size, R, jb.first_exponent,
+                                     c.tcoef.as<uint32_t>(), c.rec.as<uint8_t>(), stride, c.err.as<int>(), s));
+        } else {
+            const bool gen = generate_basis();
+            if (!gen) {
+                P2G_CU(c.basis.ensure(basis_bytes(S, RG)));
+                P2G_CU(launch_basis(c.basis.as<uint16_t>(), S, RG, R, jb.first_exponent, s));
+            }
+            P2G_CU(launch_encode(c.src.as<uint8_t>(), stride, S, gen ? nullptr : c.basis.as<uint16_t>(), RG, R,
+                                 jb.slice_size, c.rec.as<uint8_t>(), stride, c.err.as<int>(), s, jb.first_exponent));
         }
-        P2G_CU(launch_encode(c.src.as<uint8_t>(), stride, S, gen ? nullptr : c.basis.as<uint16_t>(), RG, R,
-                             jb.slice_size, c.rec.as<uint8_t>(), stride, c.err.as<int>(), s, jb.first_exponent));
     } else {
         P2G_CU(cudaMemsetAsync(c.rec.p, 0, (size_t)stride * R, s));
     }

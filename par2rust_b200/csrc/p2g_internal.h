@@ -120,6 +120,19 @@ cudaError_t launch_encode_noheap(const uint8_t* src, uint64_t src_stride, uint32
                                  uint32_t RG, uint32_t R, uint64_t slice_size, uint8_t* rec, uint64_t rec_stride,
                                  int* err, cudaStream_t st);
 
+// Device addresses of the GF antilog and input-logbase tables (after upload_tables).
+cudaError_t gf_device_tables(const uint16_t** antilog, const uint16_t** logbase);
+
+// The encode on the tensor cores (p2g_mma.cu): tc_coef_kernel fills
+// `tcoef` (mma_coef_bytes(S, R) of scratch) with the coefficients' trace
+// strings, then the persistent tcgen05 kernel accumulates 16-row x
+// 240-symbol tiles over all S slices.  src rows are read in whole 16-byte
+// units, as by launch_encode.
+size_t mma_coef_bytes(uint32_t S, uint32_t R);
+cudaError_t launch_encode_mma(const uint8_t* src, uint64_t src_stride, uint32_t S, uint64_t slice_size, uint32_t R,
+                              uint32_t first_exp, uint32_t* tcoef, uint8_t* rec, uint64_t rec_stride, int* err,
+                              cudaStream_t st);
+
 // Size in bytes of the coefficient-basis scratch for S slices and RG groups.
 inline size_t basis_bytes(uint32_t S, uint32_t RG) { return (size_t)S * RG * 512 * sizeof(uint16_t); }
 

@@ -66,6 +66,18 @@ cudaError_t upload_tables() {
     return cudaSuccess;
 }
 
+// Device addresses of the antilog and input-logbase tables (for kernels in
+// other translation units, which cannot name these arrays directly).
+cudaError_t gf_device_tables(const uint16_t** antilog, const uint16_t** logbase) {
+    void* a = nullptr;
+    void* l = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&a, d_antilog);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress(&l, d_logbase);
+    *antilog = static_cast<const uint16_t*>(a);
+    *logbase = static_cast<const uint16_t*>(l);
+    return e;
+}
+
 // ---------------------------------------------------------------------------
 // PTX helpers: shared-memory addressing, mbarrier, 1-D bulk TMA copies.
 // ---------------------------------------------------------------------------
@@ -530,10 +542,13 @@ __device__ __forceinline__ uint32_t rotl32(uint32_t x, int s) { return __funnels
 #define P2G_G(x, y, z) ((y) ^ ((z) & ((x) ^ (y))))
 #define P2G_H(x, y, z) ((x) ^ (y) ^ (z))
 #define P2G_I(x, y, z) ((y) ^ ((x) | ~(z)))
-#define P2G_STEP(f, a, b, c, d, x, t, s) \
-    {                                    \
-        (a) += f((b), (c), (d)) + (x) + (t); \
-        (a) = rotl32((a), (s)) + (b);    \
+// a + x + t does not depend on the previous step's output (b), so it is
+// formed first; the chain through b is then round function -> add ->
+// rotate -> add.
+#define P2G_STEP(f, a, b, c, d, x, t, s)                    \
+    {                                                       \
+        const uint32_t _axt = (a) + ((x) + (t));            \
+        (a) = rotl32(_axt + f((b), (c), (d)), (s)) + (b);   \
     }
 
 __device__ __forceinline__ void md5_compress(uint32_t st[4], const uint32_t m[16]) {

@@ -1,0 +1,532 @@
+// p2g_mma.cu -- the Reed-Solomon accumulator on the tensor cores (tcgen05,
+// kind::mxf4), as a bit-sliced GF(2) product.
+//
+// recovery[r] = XOR_s c(r,s) * source[s] over GF(2^16) (src/reedsolomon.rs:
+// 87-126, src/creator.rs:934-1007).  Multiplication by a constant c is
+// GF(2)-linear on the 16 bits of a symbol.  With the trace form
+// G[i][j] = Tr(a^(i+j)) (a = 2) multiplication is self-adjoint, which gives
+//
+//     bits(c * x) = G^-1 H_c bits(x),   H_c[i][j] = Tr(c * a^(i+j)),
+//
+// and H_c is a Hankel matrix: its row i is bits i..i+15 of the 31-bit trace
+// string T_c = sum_{k<31} Tr(c a^k) 2^k.  So one recovery symbol is
+//
+//     rec[r][n] = G^-1 ( parity of  sum_s sum_j H_c(r,s)[i][j] * bit_j(src[s][n]) )_i ,
+//
+// an integer matrix product D = A * B^T with 0/1 entries:
+//     A[(r,i), (s,j)] = bit (i+j) of T_c(r,s)       (M = 16 rows per recovery row)
+//     B[n, (s,j)]     = bit j of src[s][n]           (N = symbols)
+// summed over K = 16 S, of which only the parity is kept.  0 and 1 are exact
+// e2m1 values (1.0 = 0x2), all scale factors are 1.0 (UE8M0 127), and the
+// fp32 accumulator holds the sums exactly (at most 16 * 32768 < 2^24).
+//
+// Tile: 16 recovery rows (two M = 128 MMAs, 8 rows x 16 bits each) x 240
+// symbols (N), accumulated in TMEM over all input slices, K-step = 4 slices
+// (K = 64 e2m1 values = 32 bytes per operand row).  Warp roles:
+//   warp 0       TMA producer: 1-D bulk copies of 4 source slices' tile bytes
+//                and of the 16 rows' trace strings of those slices
+//   warp 1       TMEM allocation; lane 0 issues the MMAs and commits
+//   warps 2..9   operand builders (A rows from T_c, B rows from source
+//                symbols, both spread to e2m1 in the canonical K-major
+//                layout), then the epilogue: tcgen05.ld of the sums, parity,
+//                one ballot per column (= two recovery symbols), G^-1, store.
+// Every mbarrier wait is bounded; a wait that gives up sets the error flag,
+// stops all roles, drains copies and MMAs in flight and frees TMEM.
+#include <mutex>
+
+#include "p2g_internal.h"
+
+namespace p2g {
+
+// T_c = d_trace_lo[c & 255] ^ d_trace_hi[c >> 8]; G^-1 y likewise from two
+// 256-entry tables of 16-bit columns.
+__device__ uint32_t d_trace_lo[256], d_trace_hi[256];
+__device__ uint16_t d_ginv_lo[256], d_ginv_hi[256];
+
+namespace {
+
+constexpr uint32_t kN = 240;            // symbols per tile (MMA N)
+constexpr uint32_t kTileRows = 16;      // recovery rows per tile (two M=128 MMAs)
+constexpr uint32_t kKSlices = 4;        // input slices per K-step (K = 64)
+constexpr int kOpStages = 8;            // operand ring (A0, A1, B)
+constexpr int kInStages = 8;            // source ring
+constexpr int kGenWarps = 8;
+constexpr int kThreads = 64 + 32 * kGenWarps;
+constexpr uint32_t kAccCol1 = 256;      // TMEM column of the second accumulator
+constexpr uint32_t kSfaCol = 496, kSfbCol = 504;  // scale factors (all 1.0)
+
+// shared memory layout (bytes)
+constexpr uint32_t kATileBytes = 4096;                  // 128 rows x 32 B
+constexpr uint32_t kBTileBytes = kN * 32;               // 7680
+constexpr uint32_t kOpStageBytes = 2 * kATileBytes + 8192;
+constexpr uint32_t kSrcSliceBytes = kN * 2;             // 480
+constexpr uint32_t kInCoefBytes = kKSlices * kTileRows * 4;  // T of 16 rows x 4 slices
+constexpr uint32_t kInStageBytes = 2304;                // T values, then 4 slices x 480, rounded
+constexpr uint32_t kOffOp = 0;
+constexpr uint32_t kOffIn = kOffOp + kOpStages * kOpStageBytes;
+constexpr uint32_t kOffGinv = kOffIn + kInStages * kInStageBytes;
+constexpr uint32_t kOffBars = kOffGinv + 1024;
+constexpr uint32_t kNumBars = 2 * kInStages + 2 * kOpStages + 3;
+constexpr uint32_t kOffMisc = kOffBars + kNumBars * 8;
+constexpr uint32_t kSmemBytes = kOffMisc + 16;
+static_assert(kSmemBytes > 116 * 1024, "one CTA per SM: TMEM is allocated whole");
+static_assert(kBTileBytes <= kOpStageBytes - 2 * kATileBytes, "B tile fits its stage");
+static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false when it gave up or another role has (abort flag set).
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, volatile uint32_t* abort_flag) {
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        if (bar_try_wait(bar, parity)) return true;
+        if ((it & 255u) == 255u && *abort_flag) return false;
+    }
+    *abort_flag = 1u;
+    return false;
+}
+__device__ __forceinline__ void tma_1d(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// --- tcgen05 -------------------------------------------------------------
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8
+// rows x 16 bytes; LBO = byte distance between the two 16-byte K halves,
+// SBO = byte distance between 8-row groups; version 1 (bits 46-47).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::mxf4 with UE8M0 block scales: A and B
+// e2m1 (format 1), K-major, N >> 3 at bit 17, scale format bit 23, M >> 4 at
+// bit 24, scale-factor ids 0, dense K = 64.
+constexpr uint32_t kIdesc = (1u << 7) | (1u << 10) | ((kN >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_mxf4(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t sfa,
+                                         uint32_t sfb, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %6, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%4], [%5], p;\n}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(kIdesc), "r"(sfa), "r"(sfb), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, uint32_t v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(taddr), "r"(v)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// 16 bits -> 16 e2m1 values (0 or 1.0 = 0x2), 8 bytes.  Bit pairs (4q, 4q+1)
+// go to byte q of the low word, pairs (4q+2, 4q+3) to byte q of the high
+// word, each pair through a 4-entry byte table (PRMT).  A and B go through
+// the same map, so K positions pair bit j with bit j.
+__device__ __forceinline__ uint2 spread16(uint32_t x) {
+    constexpr uint32_t kPairs = 0x22200200u;  // byte g = e2m1 pair of bits (g & 1, g >> 1)
+    return make_uint2(__byte_perm(kPairs, 0u, x & 0x3333u), __byte_perm(kPairs, 0u, (x >> 2) & 0x3333u));
+}
+__device__ __forceinline__ void sts64(uint32_t addr, uint2 v) {
+    asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(addr), "r"(v.x), "r"(v.y) : "memory");
+}
+__device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ uint32_t lds_u16(uint32_t addr) {
+    uint16_t v;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(addr));
+    return v;
+}
+
+}  // namespace
+
+// Coefficient trace strings: tcoef[s * Rpad + r] = T_c(r,s) for c(r,s) =
+// base_s ^ (first_exp + r) = 2^(logbase_s * (first_exp + r) mod 65535)
+// (RsEncoder::coefficient, src/reedsolomon.rs:56-60; gf_pow src/galois.rs:
+// 74-87); rows r >= R get 0.
+__global__ void tc_coef_kernel(uint32_t* __restrict__ tcoef, const uint16_t* __restrict__ antilog,
+                               const uint16_t* __restrict__ logbase, uint32_t S, uint32_t R, uint32_t Rpad,
+                               uint32_t first_exp) {
+    const uint64_t total = (uint64_t)S * Rpad;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = (uint32_t)(i / Rpad), r = (uint32_t)(i % Rpad);
+        uint32_t T = 0;
+        if (r < R) {
+            const uint32_t e = (first_exp + r) % kFieldLimit;
+            uint32_t k = (uint32_t)logbase[s] * e;  // < 2^32
+            k = (k & 0xFFFFu) + (k >> 16);
+            k = (k & 0xFFFFu) + (k >> 16);
+            if (k >= kFieldLimit) k -= kFieldLimit;
+            const uint32_t c = antilog[k];
+            T = d_trace_lo[c & 0xFFu] ^ d_trace_hi[c >> 8];
+        }
+        tcoef[i] = T;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    encode_mma_kernel(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S, uint32_t Np,
+                      const uint32_t* __restrict__ tcoef, uint32_t Rpad, uint32_t R, uint8_t* __restrict__ rec,
+                      uint64_t rec_stride, uint32_t n_row_tiles, uint32_t n_tiles, int* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = smem_addr(smem);
+    const uint32_t op0 = sbase + kOffOp, in0 = sbase + kOffIn;
+    uint16_t* ginv = reinterpret_cast<uint16_t*>(smem + kOffGinv);  // [0,256) lo, [256,512) hi
+    const uint32_t bars = sbase + kOffBars;
+    const uint32_t in_full = bars, in_empty = bars + 8 * kInStages;
+    const uint32_t op_full = bars + 16 * kInStages, op_empty = op_full + 8 * kOpStages;
+    const uint32_t acc_full = op_empty + 8 * kOpStages, acc_empty = acc_full + 8, drain = acc_full + 16;
+    uint32_t* misc = reinterpret_cast<uint32_t*>(smem + kOffMisc);  // [0] TMEM base, [1] abort
+    volatile uint32_t* abort_flag = misc + 1;
+    const uint32_t KS = (S + kKSlices - 1) / kKSlices;
+
+    if (tid == 0) {
+        for (int i = 0; i < kInStages; ++i) {
+            bar_init(in_full + 8 * i, 1);
+            bar_init(in_empty + 8 * i, kGenWarps);
+        }
+        for (int i = 0; i < kOpStages; ++i) {
+            bar_init(op_full + 8 * i, kGenWarps);
+            bar_init(op_empty + 8 * i, 1);
+        }
+        bar_init(acc_full, 1);
+        bar_init(acc_empty, kGenWarps);
+        bar_init(drain, 1);
+        misc[1] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < 256; i += kThreads) {
+        ginv[i] = d_ginv_lo[i];
+        ginv[256 + i] = d_ginv_hi[i];
+    }
+    if (warp == 1) {  // the whole of TMEM: two accumulators and the scale factors
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(sbase + kOffMisc)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = misc[0];
+    if (warp >= 2 && warp < 6) {  // scale factors 1.0 over all 128 lanes, columns 496..511
+        const uint32_t t = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + kSfaCol;
+        tmem_st8(t, 0x7F7F7F7Fu);
+        tmem_st8(t + 8, 0x7F7F7F7Fu);
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    if (warp == 0) {
+        // ---- producer: the tile's bytes of 4 source slices per K-step ----
+        if (lane == 0) {
+            uint32_t g = 0;
+            bool ok = true;
+            for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
+                const uint32_t n0 = (tile / n_row_tiles) * kN;
+                const uint32_t r0 = (tile % n_row_tiles) * kTileRows;
+                const uint32_t bytes = 2 * min(kN, Np - n0);
+                for (uint32_t k = 0; k < KS; ++k, ++g) {
+                    const uint32_t st = g % kInStages;
+                    if (!bar_wait(in_empty + 8 * st, ((g / kInStages) & 1u) ^ 1u, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t s0 = k * kKSlices, ns = min(kKSlices, S - s0);
+                    const uint32_t dst = in0 + st * kInStageBytes;
+                    bar_expect_tx(in_full + 8 * st, ns * (bytes + kTileRows * 4));
+                    for (uint32_t j = 0; j < ns; ++j) {
+                        tma_1d(dst + j * kTileRows * 4, tcoef + (size_t)(s0 + j) * Rpad + r0, kTileRows * 4,
+                               in_full + 8 * st);
+                        tma_1d(dst + kInCoefBytes + j * kSrcSliceBytes,
+                               src + (size_t)(s0 + j) * src_stride + (size_t)n0 * 2, bytes, in_full + 8 * st);
+                    }
+                }
+            }
+            // copies still in flight land before the CTA's shared memory goes away
+            for (uint32_t b = g > (uint32_t)kInStages ? g - kInStages : 0; b < g; ++b) {
+                const uint32_t st = b % kInStages;
+                for (uint32_t it = 0; it < (1u << 22) && !bar_try_wait(in_full + 8 * st, (b / kInStages) & 1u); ++it) {
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            uint32_t g = 0, tcount = 0;
+            bool ok = true;
+            for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, ++tcount) {
+                const uint32_t r0 = (tile % n_row_tiles) * kTileRows;
+                const bool two = R - r0 > 8;
+                if (!bar_wait(acc_empty, (tcount & 1u) ^ 1u, abort_flag)) break;
+                tc_fence_after();
+                for (uint32_t k = 0; k < KS; ++k, ++g) {
+                    const uint32_t so = g % kOpStages;
+                    if (!bar_wait(op_full + 8 * so, (g / kOpStages) & 1u, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a = op0 + so * kOpStageBytes;
+                    const uint64_t bdesc = smem_desc(a + 2 * kATileBytes, 128, 256);
+                    mma_mxf4(tmem, smem_desc(a, 128, 256), bdesc, tmem + kSfaCol, tmem + kSfbCol, k > 0);
+                    if (two)
+                        mma_mxf4(tmem + kAccCol1, smem_desc(a + kATileBytes, 128, 256), bdesc, tmem + kSfaCol,
+                                 tmem + kSfbCol, k > 0);
+                    mma_commit(op_empty + 8 * so);
+                }
+                if (ok) mma_commit(acc_full);
+            }
+            // every MMA issued has completed before TMEM is freed
+            mma_commit(drain);
+            for (uint32_t it = 0; it < (1u << 22) && !bar_try_wait(drain, 0); ++it) {
+            }
+        }
+    } else {
+        // ---- operand builders, then the epilogue of each tile ----
+        const int gw = warp - 2;
+        const uint32_t m8 = (uint32_t)lane >> 2, sl = (uint32_t)lane & 3u;
+        const uint32_t lane_off = (sl >> 1) * 128 + m8 * 16 + (sl & 1u) * 8;  // canonical K-major position
+        uint32_t g = 0, tcount = 0;
+        bool ok = true;
+        for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, ++tcount) {
+            const uint32_t r0 = (tile % n_row_tiles) * kTileRows;
+            const uint32_t n0 = (tile / n_row_tiles) * kN;
+            const uint32_t syms = min(kN, Np - n0);
+            for (uint32_t k = 0; k < KS; ++k, ++g) {
+                const uint32_t si = g % kInStages, so = g % kOpStages;
+                if (!bar_wait(in_full + 8 * si, (g / kInStages) & 1u, abort_flag) ||
+                    !bar_wait(op_empty + 8 * so, ((g / kOpStages) & 1u) ^ 1u, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t a = op0 + so * kOpStageBytes;
+                const uint32_t s = k * kKSlices + sl;
+                const uint32_t ins = in0 + si * kInStageBytes;
+                // A: 2 tiles x 16 groups of 8 rows; row m = 16*rl + i of tile t
+                // is bits i..i+15 of T for recovery row r0 + 8t + rl (rows past
+                // R have T = 0; slices past S were not loaded)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint32_t it = (uint32_t)gw + 8u * j, t = it >> 4, grp = it & 15u;
+                    const uint32_t m = grp * 8 + m8;
+                    const uint32_t T = s < S ? lds_u32(ins + (sl * kTileRows + 8 * t + (m >> 4)) * 4) : 0u;
+                    sts64(a + t * kATileBytes + grp * 256 + lane_off, spread16((T >> (m & 15u)) & 0xFFFFu));
+                }
+                // B: 30 groups of 8 symbols
+                const uint32_t srcst = ins + kInCoefBytes + sl * kSrcSliceBytes;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint32_t grp = (uint32_t)gw + 8u * j;
+                    if (grp < kN / 8) {
+                        const uint32_t n = grp * 8 + m8;
+                        const uint32_t x = (n < syms && s < S) ? lds_u16(srcst + n * 2) : 0u;
+                        sts64(a + 2 * kATileBytes + grp * 256 + lane_off, spread16(x));
+                    }
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    bar_arrive(op_full + 8 * so);
+                    bar_arrive(in_empty + 8 * si);
+                }
+            }
+            if (!ok) break;
+            // epilogue: warp (t, q) reads lanes 32q.. of accumulator t
+            if (!bar_wait(acc_full, tcount & 1u, abort_flag)) break;
+            tc_fence_after();
+            const uint32_t q = (uint32_t)warp & 3u, t = (uint32_t)gw >> 2;
+            const uint32_t ra = r0 + 8 * t + 2 * q, rb = ra + 1;
+            if (ra < R) {
+                for (uint32_t c0 = 0; c0 < kN; c0 += 32) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem + ((32 * q) << 16) + t * kAccCol1 + c0, v);
+                    uint32_t mine = 0;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const uint32_t b = __ballot_sync(0xFFFFFFFFu, __float2uint_rz(__uint_as_float(v[j])) & 1u);
+                        if (lane == j) mine = b;
+                    }
+                    // lanes 0-15 of the ballot: bits of row ra, lanes 16-31: row rb
+                    const uint32_t col = c0 + (uint32_t)lane;
+                    if (col < syms) {
+                        const uint32_t ya = mine & 0xFFFFu, yb = mine >> 16;
+                        const uint16_t va = ginv[ya & 0xFFu] ^ ginv[256 + (ya >> 8)];
+                        const uint16_t vb = ginv[yb & 0xFFu] ^ ginv[256 + (yb >> 8)];
+                        uint8_t* p = rec + (size_t)ra * rec_stride + (size_t)(n0 + col) * 2;
+                        *reinterpret_cast<uint16_t*>(p) = va;
+                        if (rb < R) *reinterpret_cast<uint16_t*>(p + rec_stride) = vb;
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(acc_empty);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0 && *abort_flag) atomicOr(err, 1);
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+// Trace strings and G^-1 from the field itself (polynomial 0x1100B,
+// generator 2).  Returns false if G were singular (it never is).
+bool build_trace_tables(uint32_t tlo[256], uint32_t thi[256], uint16_t glo[256], uint16_t ghi[256]) {
+    std::vector<uint32_t> al(65536), lg(65536);
+    uint32_t b = 1;
+    for (uint32_t l = 0; l < kFieldLimit; ++l) {
+        al[l] = b;
+        lg[b] = l;
+        b <<= 1;
+        if (b & 0x10000u) b ^= kFieldGenerator;
+    }
+    auto mul = [&](uint32_t x, uint32_t y) -> uint32_t {
+        return (x && y) ? al[(lg[x] + lg[y]) % kFieldLimit] : 0u;
+    };
+    auto trace = [&](uint32_t y) {  // y + y^2 + ... + y^(2^15), in {0, 1}
+        uint32_t acc = y, z = y;
+        for (int i = 0; i < 15; ++i) {
+            z = mul(z, z);
+            acc ^= z;
+        }
+        return acc;
+    };
+    uint32_t tr[47];
+    for (uint32_t k = 0; k < 47; ++k) tr[k] = trace(al[k]);
+    uint32_t tbit[16];  // T of the basis element 2^b
+    for (uint32_t bb = 0; bb < 16; ++bb) {
+        tbit[bb] = 0;
+        for (uint32_t k = 0; k < 31; ++k) tbit[bb] |= (tr[bb + k] & 1u) << k;
+    }
+    // G[i][j] = Tr(a^(i+j)); invert over GF(2): rows as 32-bit [G | I]
+    uint32_t rows[16];
+    for (uint32_t i = 0; i < 16; ++i) {
+        rows[i] = 1u << (16 + i);
+        for (uint32_t j = 0; j < 16; ++j) rows[i] |= (tr[i + j] & 1u) << j;
+    }
+    for (uint32_t c = 0; c < 16; ++c) {
+        uint32_t p = c;
+        while (p < 16 && !((rows[p] >> c) & 1u)) ++p;
+        if (p == 16) return false;
+        std::swap(rows[c], rows[p]);
+        for (uint32_t r = 0; r < 16; ++r)
+            if (r != c && ((rows[r] >> c) & 1u)) rows[r] ^= rows[c];
+    }
+    uint16_t gcol[16];  // column j of G^-1 as a 16-bit vector over i
+    for (uint32_t j = 0; j < 16; ++j) {
+        gcol[j] = 0;
+        for (uint32_t i = 0; i < 16; ++i) gcol[j] |= (uint16_t)(((rows[i] >> (16 + j)) & 1u) << i);
+    }
+    for (uint32_t v = 0; v < 256; ++v) {
+        tlo[v] = thi[v] = 0;
+        glo[v] = ghi[v] = 0;
+        for (uint32_t bb = 0; bb < 8; ++bb)
+            if ((v >> bb) & 1u) {
+                tlo[v] ^= tbit[bb];
+                thi[v] ^= tbit[bb + 8];
+                glo[v] ^= gcol[bb];
+                ghi[v] ^= gcol[bb + 8];
+            }
+    }
+    return true;
+}
+
+cudaError_t mma_prepare() {
+    static std::mutex mu;
+    static bool done[256] = {false};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev >= 0 && dev < 256 && done[dev]) return cudaSuccess;
+    static uint32_t tlo[256], thi[256];
+    static uint16_t glo[256], ghi[256];
+    if (!build_trace_tables(tlo, thi, glo, ghi)) return cudaErrorInvalidValue;
+    if ((e = cudaMemcpyToSymbol(d_trace_lo, tlo, sizeof tlo)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(d_trace_hi, thi, sizeof thi)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(d_ginv_lo, glo, sizeof glo)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(d_ginv_hi, ghi, sizeof ghi)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(encode_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes)) !=
+        cudaSuccess)
+        return e;
+    if (dev >= 0 && dev < 256) done[dev] = true;
+    return cudaSuccess;
+}
+}  // namespace
+
+size_t mma_coef_bytes(uint32_t S, uint32_t R) {
+    const uint64_t Rpad = (uint64_t)(R + kTileRows - 1) / kTileRows * kTileRows;
+    return (size_t)S * Rpad * sizeof(uint32_t);
+}
+
+cudaError_t launch_encode_mma(const uint8_t* src, uint64_t src_stride, uint32_t S, uint64_t slice_size, uint32_t R,
+                              uint32_t first_exp, uint32_t* tcoef, uint8_t* rec, uint64_t rec_stride, int* err,
+                              cudaStream_t st) {
+    if (!S || !R) return cudaSuccess;
+    cudaError_t e = mma_prepare();
+    if (e != cudaSuccess) return e;
+    const uint16_t *antilog = nullptr, *logbase = nullptr;
+    if ((e = gf_device_tables(&antilog, &logbase)) != cudaSuccess) return e;
+    const uint32_t Np = (uint32_t)(((slice_size + 15) & ~15ull) / 2);
+    const uint32_t n_row = (R + kTileRows - 1) / kTileRows, Rpad = n_row * kTileRows;
+    const uint32_t n_sym = (Np + kN - 1) / kN;
+    const uint64_t total = (uint64_t)S * Rpad;
+    const int sms = device_sm_count();
+    const unsigned cb = (unsigned)std::min<uint64_t>((total + 255) / 256, (uint64_t)sms * 8);
+    tc_coef_kernel<<<cb, 256, 0, st>>>(tcoef, antilog, logbase, S, R, Rpad, first_exp);
+    add_launches(1);
+    const uint64_t tiles = (uint64_t)n_sym * n_row;
+    const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms);
+    encode_mma_kernel<<<grid, kThreads, kSmemBytes, st>>>(src, src_stride, S, Np, tcoef, Rpad, R, rec, rec_stride,
+                                                          n_row, (uint32_t)tiles, err);
+    add_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace p2g

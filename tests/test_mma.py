@@ -1,0 +1,61 @@
+"""The tensor-core (tcgen05, kind::mxf4) encode against the oracle and the
+lookup kernel.
+
+Shapes cover a single slice, R = 1, one and two 8-row halves of a 16-row
+tile (R = 8, 9, 16, 17), a last symbol tile of 8 symbols (Np = 248), ragged
+slices (4,100 B: 2,056 symbols), slice counts that are not a multiple of the
+4-slice K-step, non-zero first exponents, and a 538 MB-like slice size.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [  # (S, slice, R, first_exponent)
+    (1, 64, 1, 0), (1, 496, 8, 0), (2, 496, 9, 0), (3, 4096, 16, 0), (5, 4096, 17, 0), (6, 960, 33, 0),
+    (7, 4100, 20, 0), (9, 2048, 48, 7), (13, 65536, 3, 65530), (37, 65536, 200, 0), (64, 8192, 129, 100),
+]
+
+
+@pytest.mark.parametrize("S,slice_,R,fe", SHAPES)
+def test_tensor_encode_matches_oracle(p2g, gpu, oracle, S, slice_, R, fe):
+    from par2rust_b200.workloads import file_bytes
+
+    src = file_bytes(7 * S + R, S * slice_)
+    got = p2g.encode(src, slice_, R, first_exponent=fe, variant=p2g.ENCODE_TENSOR).reshape(R, slice_)
+    if fe == 0:
+        want = oracle.encode_fast(src, S, slice_, R).reshape(R, slice_)
+    else:
+        want = oracle.encode_rows(src, S, slice_, [fe + r for r in range(R)])
+    assert np.array_equal(got, want)
+
+
+def test_tensor_encode_equals_lut_on_device(p2g, gpu):
+    """Device pointers, 256 slices x 512 KiB, R 200: both kernels, same bytes,
+    and bytes past the padded row untouched."""
+    import torch
+
+    S, sl, R = 256, 524288, 200
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    src = torch.randint(0, 256, (S * sl,), dtype=torch.uint8, device="cuda", generator=g)
+    rs = sl + 64
+    a = torch.full((R * rs,), 0x33, dtype=torch.uint8, device="cuda")
+    b = torch.full((R * rs,), 0x33, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    p2g.encode_device(src.data_ptr(), sl, S, sl, R, a.data_ptr(), rs, stream, variant=p2g.ENCODE_LUT, wait=True)
+    p2g.encode_device(src.data_ptr(), sl, S, sl, R, b.data_ptr(), rs, stream, variant=p2g.ENCODE_TENSOR, wait=True)
+    torch.cuda.synchronize()
+    assert torch.equal(a.view(R, rs)[:, :sl], b.view(R, rs)[:, :sl])
+    assert bool((b.view(R, rs)[:, sl:] == 0x33).all())
+
+
+def test_tensor_encode_large_sums_stay_exact(p2g, gpu, oracle):
+    """All-ones sources make every product sum as large as the data allows
+    (about half of the 16 S terms of each dot product): 8,192 slices take the
+    fp32 sums to ~65,000, where a lossy accumulator would flip parities."""
+    S, sl, R = 8192, 64, 40
+    src = np.full(S * sl, 0xFF, dtype=np.uint8)
+    got = p2g.encode(src, sl, R, variant=p2g.ENCODE_TENSOR).reshape(R, sl)
+    want = oracle.encode_fast(src, S, sl, R).reshape(R, sl)
+    assert np.array_equal(got, want)
