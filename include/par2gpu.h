@@ -313,6 +313,8 @@ p2g_status p2g_recovery_packet_md5(const uint8_t set_id[16], const uint8_t *reco
  * src/packet/main_packet.rs:25-42); names are the files' display names.
  * All work is ordered on `stream`. */
 #define P2G_JOB_SKIP_HASH_FULL 2u
+/* p2g_device_job.flags may also carry P2G_ENCODE_LUT or P2G_ENCODE_TENSOR
+ * to force the encode kernel (by default it is chosen by shape). */
 typedef struct p2g_device_job {
     const uint8_t *src;
     uint32_t file_count;
@@ -390,6 +392,9 @@ typedef struct p2g_batch_shape {
 #define P2G_BATCH_NO_GRAPH 1u           /* launch directly instead of replaying a CUDA graph */
 #define P2G_BATCH_NO_AUTOTUNE 2u        /* widest tiles and cost order, no tile search */
 #define P2G_BATCH_DERIVE_BASIS 4u       /* no basis scratch: encode items derive their bases */
+#define P2G_BATCH_TENSOR 8u             /* every job's encode on the tensor cores (tcgen05) */
+#define P2G_BATCH_LUT 16u               /* every job's encode on the shared-memory lookup kernel
+                                           (neither flag: chosen per job shape) */
 
 /* Validate the jobs (the checks of p2g_run_device_job), plan the items and
  * allocate the batch's device scratch.  The job buffers must stay valid
@@ -413,8 +418,11 @@ p2g_status p2g_batch_plan(const p2g_batch_shape *shapes, uint32_t n, uint32_t ct
  * slice checksums and derives the set id on the device and leaves hash_full
  * to the host (P2G_JOB_SKIP_HASH_FULL, or a single large file), from the
  * host-only planner, for inspection; P2G_TAIL_SPLIT=0 in the environment
- * turns the tail split off here as it does for the job.  It returns up to
- * `cap` encode items as (row group, fold,
+ * turns the tail split off here as it does for the job, and the encode
+ * kernel is chosen as for the job (P2G_ENCODE_VARIANT, else by shape).  Lookup
+ * kernel items cover 32-row groups (fold 1, 2 or 4 for a short last group);
+ * tensor-core items have fold 0 and cover 16-row tiles of at most 240
+ * symbols.  It returns up to `cap` encode items as (row group, fold,
  * first symbol, symbols, band, first slice, slice count, accumulate), the
  * number of encode items, and the first symbol of the columns that are
  * zeroed for accumulating items (the padded row width when there are none).

@@ -564,7 +564,7 @@ class DeviceJobBuffers:
 
 def run_device_job(src, file_lengths: Sequence[int], names: Sequence[bytes], slice_size: int, recovery_count: int,
                    bufs: Optional[DeviceJobBuffers] = None, stream: Optional[int] = None,
-                   skip_hash_full: bool = False) -> DeviceJobBuffers:
+                   skip_hash_full: bool = False, variant: int = 0) -> DeviceJobBuffers:
     """The device work of one create job over a device-resident source.
 
     ``src`` is a CUDA uint8 tensor holding the files back to back, each
@@ -597,7 +597,7 @@ def run_device_job(src, file_lengths: Sequence[int], names: Sequence[bytes], sli
     job.hash_full = bufs.hash_full.data_ptr()
     job.hash16k = bufs.hash16k.data_ptr()
     job.packet_md5 = bufs.packet_md5.data_ptr()
-    job.flags = JOB_SKIP_HASH_FULL if skip_hash_full else 0
+    job.flags = (JOB_SKIP_HASH_FULL if skip_hash_full else 0) | variant
     job.stream = stream
     _check(lib().p2g_run_device_job(C.byref(job)))
     bufs.set_id = bytes(job.set_id_out)
@@ -611,6 +611,8 @@ def run_device_job(src, file_lengths: Sequence[int], names: Sequence[bytes], sli
 BATCH_NO_GRAPH = 1
 BATCH_NO_AUTOTUNE = 2
 BATCH_DERIVE_BASIS = 4
+BATCH_TENSOR = 8  # every job's encode on the tensor cores
+BATCH_LUT = 16  # every job's encode on the lookup kernel (neither: by job shape)
 
 
 @dataclass

@@ -69,10 +69,15 @@ struct PlanJob {
     // into split_chunks slice ranges that XOR-accumulate into the rows.
     // split_chunks 0: the caller does not zero, never split.
     uint32_t split_bands = 0, split_chunks = 0;
+    // Encode on the tensor cores: 16-row x 240-symbol items (kItemEncodeMma);
+    // RG then counts 16-row tiles and ts is fixed at 240.
+    bool mma = false;
 };
 
 double finish_ms(const PlanJob& j) { return est_set_id_ms(j.n) + est_packet_item_ms(j.slice, j.R); }
-inline double encode_ms(const PlanJob& j, uint32_t syms) { return est_encode_item_ms(j.S, syms); }
+inline double encode_ms(const PlanJob& j, uint32_t syms) {
+    return j.mma ? est_mma_item_ms(j.S) : est_encode_item_ms(j.S, syms);
+}
 inline double scan_ms(const PlanJob& j, uint32_t count) { return est_scan_item_ms(j.slice, count); }
 
 void set_tiling(PlanJob& j, uint32_t tiles) {
@@ -95,7 +100,7 @@ constexpr uint32_t kMaxBands = 64;  // packet-MD5 chain segments per job (64: 10
 // Bands of job j: runs of band_tiles consecutive tiles, a multiple of the
 // tail fold so that no folded item straddles two bands.
 void job_bands(const PlanJob& j, uint32_t* band_tiles, uint32_t* n_bands) {
-    const uint32_t F = tail_fold(j.R);
+    const uint32_t F = j.mma ? 1u : tail_fold(j.R);
     uint32_t bt = std::max<uint32_t>(1, (j.tiles + kMaxBands - 1) / kMaxBands);
     bt = (bt + F - 1) / F * F;
     *band_tiles = bt;
@@ -145,7 +150,7 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
         if (!j.R) continue;
         uint32_t bt = 0, nb = 0;
         job_bands(j, &bt, &nb);
-        const uint32_t F = tail_fold(j.R);
+        const uint32_t F = j.mma ? 1u : tail_fold(j.R);
         p.band_syms[ji] = bt * j.ts;
         p.band_items[ji].assign(nb, 0);
         std::vector<uint32_t>& counts = p.band_items[ji];
@@ -164,6 +169,19 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
                     counts[b]++;
                 }
             };
+            if (j.mma) {  // tile-major: the row tiles of one symbol tile share its source reads in L2
+                for (uint32_t t = t0; t < t1; ++t) {
+                    const uint32_t n0 = t * j.ts, syms = std::min(j.ts, j.Np - n0);
+                    for (uint32_t rt = 0; rt < j.RG; ++rt)
+                        for (uint32_t s0 = 0; s0 < j.S; s0 += cs) {
+                            const uint32_t sn = C > 1 ? std::min(cs, j.S - s0) : 0;
+                            e.items.push_back({ji, encode_mma_kind(rt, C > 1), n0, (b << 16) | syms, s0, sn});
+                            e.key += est_mma_item_ms(sn ? sn : j.S);
+                            counts[b]++;
+                        }
+                }
+                continue;
+            }
             for (uint32_t t = t0; t < t1; ++t) {
                 const uint32_t n0 = t * j.ts, syms = std::min(j.ts, j.Np - n0);
                 for (uint32_t rg = 0; rg + 1 < j.RG; ++rg) push(rg, 1, n0, syms);
@@ -199,6 +217,8 @@ double item_ms(const PlanJob& j, const BatchItem& it) {
     case kItemScan: return scan_ms(j, it.b);
     case kItemCrc: return est_crc_item_ms(j.slice, it.b);
     case kItemFileHash: return md5_ms(j.file_bytes) + kItemMs;
+    case kItemEncodeMma:
+        return est_mma_item_ms(it.sn ? it.sn : j.S) * ((it.kind_rg & kItemAccumulate) ? kAccCost : 1.0);
     case kItemEncode: {
         double ms = est_encode_item_ms(it.sn ? it.sn : j.S, std::min(j.ts, it.b & 0xFFFFu));
         if ((it.kind_rg >> 24) & 3u) ms *= kFoldCost;
@@ -227,7 +247,8 @@ double simulate(const std::vector<PlanJob>& jobs, const Plan& p, uint32_t ctas) 
         free_at.pop();
         const PlanJob& j = jobs[it.job];
         t += item_ms(j, it);
-        if ((it.kind_rg & kItemKindMask) == kItemEncode && !left[it.job].empty()) {
+        const uint32_t kd = it.kind_rg & kItemKindMask;
+        if ((kd == kItemEncode || kd == kItemEncodeMma) && !left[it.job].empty()) {
             const uint32_t b = it.b >> 16;
             done[it.job][b] = std::max(done[it.job][b], t);
             --left[it.job][b];
@@ -287,9 +308,15 @@ Plan plan_tiles(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
     for (PlanJob& j : jobs) {
         j.split_bands = 0;  // tiles are chosen unsplit
 
-        j.RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
         j.Np = (uint32_t)(round_up(j.slice, 16) / 2);
         j.finish = finish_ms(j);
+        if (j.mma) {  // fixed tile: one MMA N wide, 16 rows (two M = 128 halves) high
+            j.RG = (j.R + kMmaTileRows - 1) / kMmaTileRows;
+            j.ts = kMmaTileSymbols;
+            j.tiles = (j.Np + j.ts - 1) / j.ts;
+            continue;
+        }
+        j.RG = (j.R + kRowsPerGroup - 1) / kRowsPerGroup;
         set_tiling(j, min_tiles(j));
         if (jobs.size() == 1 && j.R && !(flags & P2G_BATCH_NO_AUTOTUNE)) {
             // alone on the GPU, equal items run in rounds of the CTAs that
@@ -316,7 +343,7 @@ Plan plan_tiles(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
     // try finer tilings for the jobs with the longest encode items
     std::vector<uint32_t> order;
     for (uint32_t i = 0; i < (uint32_t)jobs.size(); ++i)
-        if (jobs[i].R) order.push_back(i);
+        if (jobs[i].R && !jobs[i].mma) order.push_back(i);
     std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
         return encode_ms(jobs[a], jobs[a].ts) > encode_ms(jobs[b], jobs[b].ts);
     });
@@ -345,6 +372,23 @@ Plan plan_tiles(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
 }  // namespace
 
 double est_md5_ms(uint64_t bytes) { return md5_ms(bytes); }
+// A tensor-core item: one K-step (4 slices) of operand building and two
+// MMAs, plus the pipeline fill and the epilogue.
+constexpr double kMmaStepMs = 1.6e-4, kMmaFixedMs = 0.004;
+double est_mma_item_ms(uint32_t slices) { return (slices + 3) / 4 * kMmaStepMs + kMmaFixedMs + kItemMs; }
+// Whether a job's encode runs on the tensor cores: by the cost of its items
+// on a full GPU (the lookup kernel folds a short last row group; the tensor
+// tiles are 16 rows high and 240 symbols wide).
+bool prefer_mma(uint64_t slice, uint32_t S, uint32_t R) {
+    if (!R || !S) return false;
+    const uint32_t Np = (uint32_t)(round_up(slice, 16) / 2);
+    const uint32_t RG = (R + kRowsPerGroup - 1) / kRowsPerGroup, F = tail_fold(R);
+    const double lut = (double)((Np + kEncTileSymbols - 1) / kEncTileSymbols) * (RG - 1 + 1.0 / F) *
+                       est_encode_item_ms(S, std::min<uint32_t>(Np, kEncTileSymbols)) * (F > 1 ? kFoldCost : 1.0);
+    const double mma = (double)((Np + kMmaTileSymbols - 1) / kMmaTileSymbols) *
+                       ((R + kMmaTileRows - 1) / kMmaTileRows) * est_mma_item_ms(S);
+    return mma < lut;
+}
 double est_encode_item_ms(uint32_t slices, uint32_t syms) {
     return (double)slices * (round_up(syms, 8) + kBuildCost) / kEncRate + kItemMs;
 }
@@ -380,19 +424,21 @@ constexpr size_t kMaxCachedPlans = 256;
 constexpr size_t kMaxCachedItems = 1u << 20;  // 24 MiB of items
 SingleJobPlan plan_single_job_uncached(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans,
                                        bool set_id, bool chains, uint32_t ctas, uint64_t file_bytes,
-                                       bool split_tail);
+                                       bool split_tail, bool mma);
 }  // namespace
 
 SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans, bool set_id,
-                              bool chains, uint32_t ctas, uint64_t file_bytes, bool split_tail) {
+                              bool chains, uint32_t ctas, uint64_t file_bytes, bool split_tail, bool mma) {
     const PlanKey key{slice, file_bytes, S, R, n_files, ctas,
-                      (scans ? 1u : 0u) | (set_id ? 2u : 0u) | (chains ? 4u : 0u) | (split_tail ? 8u : 0u)};
+                      (scans ? 1u : 0u) | (set_id ? 2u : 0u) | (chains ? 4u : 0u) | (split_tail ? 8u : 0u) |
+                          (mma ? 16u : 0u)};
     {
         std::lock_guard<std::mutex> lk(g_plan_mu);
         auto it = g_plans.find(key);
         if (it != g_plans.end()) return it->second;
     }
-    SingleJobPlan p = plan_single_job_uncached(slice, S, R, n_files, scans, set_id, chains, ctas, file_bytes, split_tail);
+    SingleJobPlan p =
+        plan_single_job_uncached(slice, S, R, n_files, scans, set_id, chains, ctas, file_bytes, split_tail, mma);
     std::lock_guard<std::mutex> lk(g_plan_mu);
     if (g_plans.size() >= kMaxCachedPlans || g_plan_items + p.items.size() > kMaxCachedItems) {
         g_plans.clear();
@@ -405,8 +451,9 @@ SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n
 namespace {
 SingleJobPlan plan_single_job_uncached(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans,
                                        bool set_id, bool chains, uint32_t ctas, uint64_t file_bytes,
-                                       bool split_tail) {
+                                       bool split_tail, bool mma) {
     std::vector<PlanJob> jobs(1);
+    jobs[0].mma = mma && R;
     jobs[0].slice = slice;
     jobs[0].S = S;
     jobs[0].R = R;
@@ -451,6 +498,7 @@ struct p2g_batch {
     uint64_t err_word = 0;      // index of the error word in d_ctl
     size_t ctl_bytes = 0;
     uint64_t max_basis_words = 0;
+    uint64_t max_tcoef_words = 0;  // tensor-core jobs: trace strings to fill per run
     struct Realign {
         const uint8_t* src;
         uint8_t* dst;
@@ -471,8 +519,9 @@ p2g_status enqueue_run(p2g_batch* b, cudaStream_t st) {
     int* err = reinterpret_cast<int*>(b->d_ctl + b->err_word);
     P2G_CU(cudaMemsetAsync(b->d_ctl, 0, b->ctl_bytes, st));
     if (b->max_basis_words) P2G_CU(launch_basis_batch(b->d_jobs, b->n_jobs, b->max_basis_words, st));
+    if (b->max_tcoef_words) P2G_CU(launch_tc_coef_batch(b->d_jobs, b->n_jobs, b->max_tcoef_words, st));
     for (const auto& r : b->realigns) P2G_CU(launch_realign(r.src, r.slice, r.dst, r.estride, r.S, r.slice, st));
-    P2G_CU(launch_batch(b->d_jobs, b->d_items, b->n_items, b->d_ctl, err, b->ctas, st));
+    P2G_CU(launch_batch(b->d_jobs, b->d_items, b->n_items, b->d_ctl, err, b->ctas, st, b->max_tcoef_words != 0));
     return P2G_OK;
 }
 
@@ -515,14 +564,22 @@ extern "C" p2g_status p2g_plan_device_job(uint64_t slice_size, uint32_t input_sl
     // tail split off there and here alike
     const char* ts = getenv("P2G_TAIL_SPLIT");
     const bool split_tail = !(ts && !strcmp(ts, "0"));
+    // the encode kernel the job would use (P2G_ENCODE_VARIANT, else the cost model)
+    const char* ev = getenv("P2G_ENCODE_VARIANT");
+    const bool mma = ev && !strcmp(ev, "tensor") ? true
+                     : ev && !strcmp(ev, "lut")  ? false
+                                                 : prefer_mma(slice_size, input_slices, recovery_count);
     const SingleJobPlan pl = plan_single_job(slice_size, input_slices, recovery_count, std::max(1u, file_count),
-                                             true, true, with_chains && recovery_count, ctas, 0, split_tail);
+                                             true, true, with_chains && recovery_count, ctas, 0, split_tail,
+                                             mma && recovery_count);
     uint32_t n = 0;
     for (const BatchItem& it : pl.items) {
-        if ((it.kind_rg & kItemKindMask) != kItemEncode) continue;
+        const uint32_t kind = it.kind_rg & kItemKindMask;
+        if (kind != kItemEncode && kind != kItemEncodeMma) continue;
         if (n < cap)
-            items[n] = {(it.kind_rg >> 8) & 0xFFFFu, 1u << ((it.kind_rg >> 24) & 3u), it.a, it.b & 0xFFFFu,
-                        it.b >> 16, it.s0, it.sn ? it.sn : input_slices, (it.kind_rg & kItemAccumulate) ? 1u : 0u};
+            items[n] = {(it.kind_rg >> 8) & 0xFFFFu, kind == kItemEncodeMma ? 0u : 1u << ((it.kind_rg >> 24) & 3u),
+                        it.a, it.b & 0xFFFFu, it.b >> 16, it.s0, it.sn ? it.sn : input_slices,
+                        (it.kind_rg & kItemAccumulate) ? 1u : 0u};
         ++n;
     }
     if (n_items) *n_items = n;
@@ -602,6 +659,16 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
                 shape[i].file_bytes = std::max<uint64_t>(shape[i].file_bytes, jb.file_lengths[f]);
         }
     }
+    // encode kernel per job: forced by the flags (or P2G_ENCODE_VARIANT), else by the cost model
+    const char* ev = getenv("P2G_ENCODE_VARIANT");
+    for (uint32_t i = 0; i < n; ++i) {
+        bool m = prefer_mma(shape[i].slice, shape[i].S, shape[i].R);
+        if (ev && !strcmp(ev, "tensor")) m = true;
+        if (ev && !strcmp(ev, "lut")) m = false;
+        if (flags & P2G_BATCH_TENSOR) m = true;
+        if (flags & P2G_BATCH_LUT) m = false;
+        shape[i].mma = m && shape[i].R;
+    }
     P2G_TRY(ensure_device_ready());
     p2g_batch* b = new p2g_batch();
     cudaGetDevice(&b->device);
@@ -646,12 +713,13 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
     // item) but take S x row groups x 1 KiB each: keep them while they fit.
     uint64_t basis_total = 0;
     for (uint32_t i = 0; i < n; ++i)
-        if (shape[i].R) basis_total += basis_bytes(shape[i].S, shape[i].RG);
+        if (shape[i].R && !shape[i].mma) basis_total += basis_bytes(shape[i].S, shape[i].RG);
     const bool load_basis = !(flags & P2G_BATCH_DERIVE_BASIS) && basis_total <= basis_budget();
-    std::vector<size_t> o_scratch(n), o_basis(n, 0), o_real(n, 0);
+    std::vector<size_t> o_scratch(n), o_basis(n, 0), o_real(n, 0), o_tcoef(n, 0);
     for (uint32_t i = 0; i < n; ++i) {
         o_scratch[i] = take(32ull * shape[i].n + 12);
-        if (load_basis && shape[i].R) o_basis[i] = take(basis_bytes(shape[i].S, shape[i].RG));
+        if (shape[i].mma) o_tcoef[i] = take(mma_coef_bytes(shape[i].S, shape[i].R));
+        if (load_basis && shape[i].R && !shape[i].mma) o_basis[i] = take(basis_bytes(shape[i].S, shape[i].RG));
         if (shape[i].R && jobs[i].slice_size % 16) o_real[i] = take(round_up(jobs[i].slice_size, 16) * shape[i].S);
     }
     b->arena_bytes = off;
@@ -700,7 +768,13 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         d.chain = reinterpret_cast<uint32_t*>(A + o_chain[i]);
         d.first_exp = 0;
         d.vec = jb.slice_size % 16 == 0 ? 1u : 0u;
-        d.basis = load_basis && d.R ? reinterpret_cast<uint16_t*>(A + o_basis[i]) : nullptr;
+        d.basis = load_basis && d.R && !shape[i].mma ? reinterpret_cast<uint16_t*>(A + o_basis[i]) : nullptr;
+        if (shape[i].mma) {
+            d.mma = 1;
+            d.Rpad = (d.R + kMmaTileRows - 1) / kMmaTileRows * kMmaTileRows;
+            d.tcoef = reinterpret_cast<uint32_t*>(A + o_tcoef[i]);
+            b->max_tcoef_words = std::max<uint64_t>(b->max_tcoef_words, (uint64_t)d.S * d.Rpad);
+        }
         if (d.R && jb.slice_size % 16) {
             d.esrc = A + o_real[i];
             d.estride = round_up(jb.slice_size, 16);
@@ -736,7 +810,7 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         release(b);
         return cuda_fail(e, "batch tables upload");
     }
-    b->kernels_per_run = 1 + (b->max_basis_words ? 1 : 0) + (uint32_t)b->realigns.size();
+    b->kernels_per_run = 1 + (b->max_basis_words ? 1 : 0) + (b->max_tcoef_words ? 1 : 0) + (uint32_t)b->realigns.size();
 
     // ---- capture the run into a CUDA graph ----
     if (!(flags & P2G_BATCH_NO_GRAPH)) {

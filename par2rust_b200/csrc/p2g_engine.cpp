@@ -206,7 +206,8 @@ static p2g_status join_into(Context& c, cudaStream_t caller) {
 // close to its issue limit).
 // Which encode kernel runs a job: the shared-memory lookup kernel or the
 // tensor-core bit-sliced one.  P2G_ENCODE_LUT / P2G_ENCODE_TENSOR (or
-// P2G_ENCODE_VARIANT=lut|tensor) force one; otherwise it is chosen by shape.
+// P2G_ENCODE_VARIANT=lut|tensor) force one; otherwise the planner's cost
+// model picks by shape (prefer_mma).
 static bool use_tensor_encode(uint32_t flags, uint32_t S, uint32_t R, uint64_t slice_size) {
     if (flags & P2G_ENCODE_TENSOR) return true;
     if (flags & P2G_ENCODE_LUT) return false;
@@ -214,10 +215,7 @@ static bool use_tensor_encode(uint32_t flags, uint32_t S, uint32_t R, uint64_t s
         if (!strcmp(e, "tensor")) return true;
         if (!strcmp(e, "lut")) return false;
     }
-    (void)S;
-    (void)R;
-    (void)slice_size;
-    return false;
+    return prefer_mma(slice_size, S, R);
 }
 
 static bool generate_basis() {
@@ -326,6 +324,7 @@ struct DeviceJob {
     uint8_t* d_h16k = nullptr;
     uint8_t* d_hfull = nullptr;  // null: hash_full not on the device
     uint8_t* d_pkt = nullptr;    // null: skip packet MD5
+    uint32_t variant = 0;        // P2G_ENCODE_LUT / P2G_ENCODE_TENSOR, or 0: by shape
     // filled
     std::vector<Md5> h16k, file_ids;
     Md5 set_id{};
@@ -397,9 +396,10 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
         const char* e = getenv("P2G_TAIL_SPLIT");
         return !(e && !strcmp(e, "0"));
     }();
+    const bool mma = j.R && j.S && use_tensor_encode(j.variant, j.S, j.R, j.slice);
     const SingleJobPlan pl = plan_single_job(j.slice, j.S, j.R && j.S ? j.R : 0, n, j.d_checks != nullptr, sid_item,
                                              chains, (uint32_t)device_sm_count(), j.d_hfull ? max_len : 0,
-                                             split_tail);
+                                             split_tail, mma);
     const uint32_t nb = (uint32_t)pl.band_items.size();
     const uint32_t Q = (j.R + kChainRows - 1) / kChainRows;
     const uint64_t ctl_words = 1 + (chains ? nb + 2 * Q + 1 : 0) + 1;  // head, chain state, error word
@@ -422,8 +422,9 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     uint8_t* D = c.persist.as<uint8_t>();
     uint8_t* H = c.h_persist.as<uint8_t>();
     // basis (precomputed unless P2G_ENCODE_BASIS=derive) and 16-byte aligned slices
-    const bool gen = generate_basis();
+    const bool gen = generate_basis() || mma;  // the tensor-core items take trace strings instead
     if (j.R && j.S && !gen) P2G_CU(c.basis.ensure(basis_bytes(j.S, RG)));
+    if (mma) P2G_CU(c.tcoef.ensure(mma_coef_bytes(j.S, j.R)));
     const uint8_t* esrc = j.d_src;
     uint64_t estride = j.slice;
     if (j.R && j.S && j.slice % 16) {
@@ -461,6 +462,11 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     d.ts = pl.ts;
     d.first_exp = j.first_exp;
     d.vec = j.slice % 16 == 0 ? 1u : 0u;
+    if (mma) {
+        d.mma = 1;
+        d.tcoef = c.tcoef.as<uint32_t>();
+        d.Rpad = (j.R + kMmaTileRows - 1) / kMmaTileRows * kMmaTileRows;
+    }
     memcpy(H + o_items, pl.items.data(), sizeof(BatchItem) * pl.items.size());
     uint8_t* hb = H + o_ctl;  // band counts, file tables and names after the descriptor and items
     memcpy(hb + (o_bands - o_ctl), pl.band_items.data(), 4 * nb);
@@ -494,10 +500,12 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
         P2G_CU(cudaMemset2DAsync(j.d_rec + 2ull * pl.zero_from_sym, j.rec_stride, 0,
                                  np_bytes - 2ull * pl.zero_from_sym, j.R, st));
     if (d.basis) P2G_CU(launch_basis(c.basis.as<uint16_t>(), j.S, RG, j.R, j.first_exp, st));
+    if (mma)
+        P2G_CU(launch_tc_coef_batch(reinterpret_cast<const BatchJob*>(D + o_desc), 1, (uint64_t)j.S * d.Rpad, st));
     if (esrc != j.d_src) P2G_CU(launch_realign(j.d_src, j.slice, c.src_al.as<uint8_t>(), estride, j.S, j.slice, st));
     P2G_CU(launch_batch(reinterpret_cast<const BatchJob*>(D + o_desc), reinterpret_cast<const BatchItem*>(D + o_items),
                         (uint32_t)pl.items.size(), reinterpret_cast<uint32_t*>(D + o_ctl), err,
-                        (uint32_t)device_sm_count(), st));
+                        (uint32_t)device_sm_count(), st, mma));
     P2G_CU(cudaMemcpyAsync(c.h_err.p, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     if (j.progress && j.R && j.S) P2G_TRY(poll_progress(c, j, pl, reinterpret_cast<const uint32_t*>(D + o_ctl), st));
     if (!j.have_set_id) {
@@ -1290,6 +1298,7 @@ extern "C" p2g_status p2g_run_device_job(p2g_device_job* job) {
     j.d_checks = jb.checksums;
     j.d_h16k = jb.hash16k;
     j.d_hfull = (jb.flags & P2G_JOB_SKIP_HASH_FULL) ? nullptr : jb.hash_full;
+    j.variant = jb.flags & (P2G_ENCODE_LUT | P2G_ENCODE_TENSOR);
     j.d_pkt = jb.packet_md5;
     if (!j.d_h16k) return set_error(P2G_ERR_INVALID_ARGUMENT, "hash16k output is required (it derives the set id)");
     P2G_TRY(run_device_job(c, j, (cudaStream_t)jb.stream));

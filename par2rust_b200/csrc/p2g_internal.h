@@ -147,6 +147,7 @@ enum BatchItemKind : uint32_t {
     kItemPacket = 4,  // packet MD5s of recovery rows [a, a+b) (set id already written)
     kItemCrc = 5,     // slice CRC32 of slices [a, a+b)
     kItemFileHash = 6,  // whole-file MD5 (hash_full) of files [a, a+b), one lane each
+    kItemEncodeMma = 7,  // one (16-row tile, 240-symbol tile) of the accumulator on the tensor cores
 };
 constexpr uint64_t kCrcItemBytes = 4u << 20;  // source bytes per CRC item
 constexpr uint32_t kItemKindMask = 0x7Fu;
@@ -159,6 +160,14 @@ constexpr uint32_t kChainRows = 256;         // recovery rows per packet-MD5 cha
 inline uint32_t encode_kind(uint32_t rg, uint32_t fold, bool acc) {
     return kItemEncode | (acc ? kItemAccumulate : 0u) | (rg << 8) | ((fold == 4 ? 2u : fold == 2 ? 1u : 0u) << 24);
 }
+
+// Tensor-core encode item: kind_rg = kItemEncodeMma | acc | row tile << 8;
+// a = first symbol, b = band << 16 | symbols (<= 240), s0/sn as for kItemEncode.
+inline uint32_t encode_mma_kind(uint32_t rt, bool acc) {
+    return kItemEncodeMma | (acc ? kItemAccumulate : 0u) | (rt << 8);
+}
+constexpr uint32_t kMmaTileSymbols = 240;  // symbols of a tensor-core tile (its MMA N)
+constexpr uint32_t kMmaTileRows = 16;      // recovery rows of a tensor-core tile
 
 struct BatchItem {
     uint32_t job;
@@ -198,7 +207,9 @@ struct BatchJob {
     uint32_t n_bands, band_syms;
     uint32_t ts, first_exp;  // ts: tile width (sub-tile width of folded items)
     uint32_t vec;            // slices and file starts of src are 16-byte aligned
-    uint32_t pad;
+    uint32_t mma;            // encode items run on the tensor cores (kItemEncodeMma)
+    uint32_t* tcoef;         // mma: trace strings of the coefficients, [s][Rpad]
+    uint32_t Rpad, pad2;     // mma: R rounded up to whole 16-row tiles
 };
 
 // Items of one job run alone through the persistent kernel (the plain
@@ -215,8 +226,10 @@ struct SingleJobPlan {
 // file_bytes: largest file (non-zero: whole-file MD5 items, 256 files each);
 // split_tail: the caller zeroes the columns from zero_from_sym, so the last
 // bands' encode items may be cut into accumulating slice ranges.
+// mma: encode items on the tensor cores (kItemEncodeMma).
 SingleJobPlan plan_single_job(uint64_t slice, uint32_t S, uint32_t R, uint32_t n_files, bool scans, bool set_id,
-                              bool chains, uint32_t ctas, uint64_t file_bytes = 0, bool split_tail = false);
+                              bool chains, uint32_t ctas, uint64_t file_bytes = 0, bool split_tail = false,
+                              bool mma = false);
 // Shared memory of one batch CTA.
 size_t batch_smem_bytes();
 // Fills every job's basis (one launch; blockIdx.y = job).
@@ -231,6 +244,9 @@ cudaError_t launch_seeded_fill(uint8_t* base, const uint64_t* spans, const uint6
 // (milliseconds of one CTA).
 double est_md5_ms(uint64_t bytes);
 double est_encode_item_ms(uint32_t slices, uint32_t syms);
+double est_mma_item_ms(uint32_t slices);
+// Whether a job of this shape encodes faster on the tensor cores (cost model).
+bool prefer_mma(uint64_t slice, uint32_t S, uint32_t R);
 double est_scan_item_ms(uint64_t slice, uint32_t count);
 double est_crc_item_ms(uint64_t slice, uint32_t count);
 // slices per CRC item: ~kCrcItemBytes, at least 1, at most kScanSlices
@@ -242,8 +258,15 @@ double est_set_id_ms(uint32_t files);
 double est_packet_item_ms(uint64_t slice, uint32_t rows);
 // Sets the batch kernel's shared-memory attribute (call before stream capture).
 cudaError_t prepare_batch_kernel();
+// mma: the batch has tensor-core encode items (the CTAs allocate TMEM and
+// need the G^-1 tables of mma_tables_ready()).
 cudaError_t launch_batch(const BatchJob* jobs, const BatchItem* items, uint32_t n_items, uint32_t* ctl, int* err,
-                         uint32_t ctas, cudaStream_t st);
+                         uint32_t ctas, cudaStream_t st, bool mma = false);
+// Device address of the 512 G^-1 table entries (256 for the low byte, 256 for
+// the high) after a one-time set-up of the tensor-core tables on this device.
+cudaError_t mma_tables_ready(const uint16_t** ginv);
+// Fills every tensor-core job's trace strings (blockIdx.y = job).
+cudaError_t launch_tc_coef_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_words, cudaStream_t st);
 int device_sm_count();
 
 }  // namespace p2g

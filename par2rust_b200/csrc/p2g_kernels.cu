@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "p2g_internal.h"
+#include "p2g_mma_tile.cuh"
 
 namespace p2g {
 
@@ -1061,9 +1062,62 @@ constexpr int kBatchRingUnits = 6;
 constexpr int kBatchRingAhead = 4;
 constexpr int kBatchRingLane = kBatchRingUnits * 64 + 16;
 constexpr size_t kBatchRingBytes = (size_t)kHashThreads * kBatchRingLane;
-constexpr size_t kBatchSmem = kBatchEncBytes + kBatchRingBytes + 4 * 256 * 4 + 64;
+// Tensor-core items reuse the encode region and the MD5 rings for their
+// operand and input rings and the G^-1 tables; their barriers, the TMEM
+// address, an abort flag and the pipeline state live past the other regions,
+// so they persist across items.
+constexpr size_t kBatchMmaBarsOff = kBatchEncBytes + kBatchRingBytes + 4 * 256 * 4 + 64;
+constexpr size_t kBatchSmem = kBatchMmaBarsOff + mma::kBarBytes + 32;
 static_assert(kBatchEncBytes % 16 == 0, "MD5 rings must start 16-byte aligned");
+static_assert(mma::kRingBytes + mma::kGinvBytes <= kBatchEncBytes + kBatchRingBytes,
+              "tensor-core rings fit the encode region and the MD5 rings");
+static_assert(kBatchMmaBarsOff % 8 == 0 && kBatchSmem <= 227 * 1024, "batch shared memory");
 size_t batch_smem_bytes() { return kBatchSmem; }
+
+// One tensor-core item of the batch kernel, all threads: 14 operand-building
+// warps (warps 2..15).  Kept out of line, with its pipeline state in shared
+// memory (words [2..4] past the barriers: K-steps, tiles, drains), so that it
+// adds no registers to the other item kinds.
+__device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ Jp, const uint16_t* __restrict__ ginv,
+                                            uint32_t kind_rg, uint32_t a, uint32_t b, uint32_t s0, uint32_t sn) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint32_t* mm = reinterpret_cast<uint32_t*>(smem + kBatchMmaBarsOff + mma::kBarBytes);
+    uint16_t* gsm = reinterpret_cast<uint16_t*>(smem + mma::kRingBytes);  // shared with other item kinds
+    for (int i = threadIdx.x; i < 512; i += kEncThreads) gsm[i] = ginv[i];
+    __syncthreads();
+    const BatchJob& J = *Jp;
+    mma::Pipe P;
+    P.ring = smem_u32(smem);
+    P.bars = smem_u32(smem + kBatchMmaBarsOff);
+    P.tmem = mm[0];
+    P.ginv = gsm;
+    P.abort_flag = mm + 1;
+    P.g = mm[2];
+    P.tcount = mm[3];
+    P.drains = mm[4];
+    mma::Tile T;
+    T.src = J.esrc;
+    T.src_stride = J.estride;
+    T.tcoef = J.tcoef;
+    T.rec = J.rec;
+    T.rec_stride = J.rec_stride;
+    T.s0 = s0;
+    T.sn = sn ? sn : J.S - s0;
+    T.Rpad = J.Rpad;
+    T.R = J.R;
+    T.r0 = ((kind_rg >> 8) & 0xFFFFu) * kMmaTileRows;
+    T.n0 = a;
+    T.syms = b & 0xFFFFu;
+    T.accumulate = (kind_rg & kItemAccumulate) ? 1u : 0u;
+    const bool ok = mma::run_tile<14>(P, T);  // ends with a CTA barrier
+    if (threadIdx.x == 0) {
+        mm[2] = P.g;
+        mm[3] = P.tcount;
+        mm[4] = P.drains;
+    }
+    __syncthreads();
+    return ok;
+}
 
 __device__ __forceinline__ void store_digest(uint8_t* out, const uint32_t st[4]) {
     uint32_t* o = reinterpret_cast<uint32_t*>(out);  // 4-byte aligned
@@ -1321,8 +1375,8 @@ __device__ void advance_all(const BatchJob& J, uint32_t ring, uint32_t* misc) {
 
 __global__ void __launch_bounds__(kEncThreads, 1)
     batch_kernel(const BatchJob* __restrict__ jobs, const BatchItem* __restrict__ items, uint32_t n_items,
-                 uint32_t* __restrict__ ctl, int* __restrict__ err) {
-    extern __shared__ __align__(128) uint8_t smem[];
+                 uint32_t* __restrict__ ctl, int* __restrict__ err, const uint16_t* __restrict__ mma_ginv) {
+    extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* enc = smem;
     uint64_t* bars = reinterpret_cast<uint64_t*>(enc + encode_bars_offset<kEncChunks, 4, kBatchEncStages>());
     uint8_t* ring_p = smem + kBatchEncBytes;
@@ -1330,11 +1384,29 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     uint32_t* misc = reinterpret_cast<uint32_t*>(ring_p + kBatchRingBytes + 4 * 256 * 4);  // [0] item [1] last [4..7] set id
     const uint32_t ring = smem_u32(ring_p);
     const int tid = threadIdx.x;
+    // tensor-core items (mma_ginv set): TMEM for the whole launch, barriers
+    // and scale factors set up once.  mma_misc: [0] TMEM address, [1] abort
+    // flag, [2..4] pipeline state.
+    uint32_t* mma_misc = reinterpret_cast<uint32_t*>(smem + kBatchMmaBarsOff + mma::kBarBytes);
+    const uint32_t mma_bars = smem_u32(smem + kBatchMmaBarsOff);
     if (tid == 0) {
         for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
+        if (mma_ginv) {
+            mma::init_bars(mma_bars, 14);
+            mma_misc[1] = mma_misc[2] = mma_misc[3] = mma_misc[4] = 0;
+        }
         fence_mbar_init();
     }
+    if (mma_ginv && (tid >> 5) == 1) mma::tmem_alloc(smem_u32(mma_misc));
+    mma::tc_fence_before();
     crc_tables_build(T);  // ends with __syncthreads
+    if (mma_ginv) {
+        mma::tc_fence_after();
+        if ((tid >> 5) >= 4 && (tid >> 5) < 8) mma::sf_fill(mma_misc[0], (uint32_t)(tid >> 5) & 3u);
+        mma::tc_fence_before();
+        __syncthreads();
+        mma::tc_fence_after();
+    }
     uint32_t phase = 0;
     for (;;) {
         if (tid == 0) misc[0] = *reinterpret_cast<volatile int*>(err) ? n_items : atomicAdd(&ctl[0], 1u);
@@ -1389,6 +1461,30 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             batch_packets(J, ring, misc + 4, it.a, it.a + it.b);
             continue;
         }
+        if (kind == kItemEncodeMma) {
+            const bool ok = batch_mma_tile(&J, mma_ginv, it.kind_rg, it.a, it.b, it.s0, it.sn);
+            // the operand rings covered the encode region's barriers: set them up again
+            if (tid == 0) {
+                for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
+                fence_mbar_init();
+            }
+            phase = 0;
+            __syncthreads();
+            if (!ok) {
+                if (tid == 0) atomicOr(err, 1);
+                break;
+            }
+            if (!J.n_bands) continue;
+            const uint32_t band = it.b >> 16;
+            __threadfence();  // release this tile's rows before counting it
+            __syncthreads();
+            if (tid == 0) misc[1] = (atomicAdd(&J.bstate[band], 1u) + 1 == J.band_items[band]) ? 1u : 0u;
+            __syncthreads();
+            if (!misc[1]) continue;
+            __threadfence();  // acquire: the whole band is visible from here on
+            advance_all(J, ring, misc);
+            continue;
+        }
         if (kind == kItemEncode) {
             // the job's precomputed basis when it has one, else derived per slice
             const uint32_t rg = (it.kind_rg >> 8) & 0xFFFFu, sn = it.sn ? it.sn : J.S;
@@ -1413,6 +1509,20 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             if (!misc[1]) continue;
             __threadfence();  // acquire: the whole band is visible from here on
             advance_all(J, ring, misc);
+        }
+    }
+    if (mma_ginv) {  // every MMA issued has completed before TMEM is given back
+        mma::tc_fence_before();
+        __syncthreads();
+        if ((tid >> 5) == 1) {
+            if ((tid & 31) == 0) {
+                const mma::Bars B(mma_bars);
+                mma::mma_commit(B.drain);
+                mma::bar_drain(B.drain, mma_misc[4] & 1u);
+            }
+            __syncwarp();
+            mma::tc_fence_after();
+            mma::tmem_free(mma_misc[0]);
         }
     }
 }
@@ -1856,11 +1966,13 @@ cudaError_t prepare_batch_kernel() {
 }
 
 cudaError_t launch_batch(const BatchJob* jobs, const BatchItem* items, uint32_t n_items, uint32_t* ctl, int* err,
-                         uint32_t ctas, cudaStream_t st) {
+                         uint32_t ctas, cudaStream_t st, bool mma) {
     if (!n_items) return cudaSuccess;
     cudaError_t e = prepare_batch_kernel();
     if (e != cudaSuccess) return e;
-    batch_kernel<<<ctas, kEncThreads, kBatchSmem, st>>>(jobs, items, n_items, ctl, err);
+    const uint16_t* ginv = nullptr;
+    if (mma && (e = mma_tables_ready(&ginv)) != cudaSuccess) return e;
+    batch_kernel<<<ctas, kEncThreads, kBatchSmem, st>>>(jobs, items, n_items, ctl, err, ginv);
     count_launch();
     return cudaGetLastError();
 }

@@ -35,143 +35,31 @@
 #include <mutex>
 
 #include "p2g_internal.h"
+#include "p2g_mma_tile.cuh"
 
 namespace p2g {
 
 // T_c = d_trace_lo[c & 255] ^ d_trace_hi[c >> 8]; G^-1 y likewise from two
-// 256-entry tables of 16-bit columns.
+// 256-entry tables of 16-bit columns, d_ginv[0..255] for the low byte of y
+// and d_ginv[256..511] for the high byte.
 __device__ uint32_t d_trace_lo[256], d_trace_hi[256];
-__device__ uint16_t d_ginv_lo[256], d_ginv_hi[256];
+__device__ uint16_t d_ginv[512];
 
 namespace {
 
-constexpr uint32_t kN = 240;            // symbols per tile (MMA N)
-constexpr uint32_t kTileRows = 16;      // recovery rows per tile (two M=128 MMAs)
-constexpr uint32_t kKSlices = 4;        // input slices per K-step (K = 64)
-constexpr int kOpStages = 8;            // operand ring (A0, A1, B)
-constexpr int kInStages = 8;            // source ring
+using namespace mma;
 constexpr int kGenWarps = 8;
 constexpr int kThreads = 64 + 32 * kGenWarps;
-constexpr uint32_t kAccCol1 = 256;      // TMEM column of the second accumulator
-constexpr uint32_t kSfaCol = 496, kSfbCol = 504;  // scale factors (all 1.0)
 
-// shared memory layout (bytes)
-constexpr uint32_t kATileBytes = 4096;                  // 128 rows x 32 B
-constexpr uint32_t kBTileBytes = kN * 32;               // 7680
-constexpr uint32_t kOpStageBytes = 2 * kATileBytes + 8192;
-constexpr uint32_t kSrcSliceBytes = kN * 2;             // 480
-constexpr uint32_t kInCoefBytes = kKSlices * kTileRows * 4;  // T of 16 rows x 4 slices
-constexpr uint32_t kInStageBytes = 2304;                // T values, then 4 slices x 480, rounded
+// shared memory layout (bytes): the rings, G^-1 tables, barriers, misc
 constexpr uint32_t kOffOp = 0;
 constexpr uint32_t kOffIn = kOffOp + kOpStages * kOpStageBytes;
-constexpr uint32_t kOffGinv = kOffIn + kInStages * kInStageBytes;
-constexpr uint32_t kOffBars = kOffGinv + 1024;
-constexpr uint32_t kNumBars = 2 * kInStages + 2 * kOpStages + 3;
-constexpr uint32_t kOffMisc = kOffBars + kNumBars * 8;
+constexpr uint32_t kOffGinv = kRingBytes;
+constexpr uint32_t kOffBars = kOffGinv + kGinvBytes;
+constexpr uint32_t kOffMisc = kOffBars + kBarBytes;
 constexpr uint32_t kSmemBytes = kOffMisc + 16;
 static_assert(kSmemBytes > 116 * 1024, "one CTA per SM: TMEM is allocated whole");
-static_assert(kBTileBytes <= kOpStageBytes - 2 * kATileBytes, "B tile fits its stage");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void bar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void bar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void bar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait: false when it gave up or another role has (abort flag set).
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, volatile uint32_t* abort_flag) {
-    for (uint32_t it = 0; it < (1u << 22); ++it) {
-        if (bar_try_wait(bar, parity)) return true;
-        if ((it & 255u) == 255u && *abort_flag) return false;
-    }
-    *abort_flag = 1u;
-    return false;
-}
-__device__ __forceinline__ void tma_1d(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-// --- tcgen05 -------------------------------------------------------------
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8
-// rows x 16 bytes; LBO = byte distance between the two 16-byte K halves,
-// SBO = byte distance between 8-row groups; version 1 (bits 46-47).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
-}
-// Instruction descriptor of kind::mxf4 with UE8M0 block scales: A and B
-// e2m1 (format 1), K-major, N >> 3 at bit 17, scale format bit 23, M >> 4 at
-// bit 24, scale-factor ids 0, dense K = 64.
-constexpr uint32_t kIdesc = (1u << 7) | (1u << 10) | ((kN >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
-
-__device__ __forceinline__ void mma_mxf4(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t sfa,
-                                         uint32_t sfb, uint32_t accumulate) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %6, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%4], [%5], p;\n}" ::"r"(d_tmem),
-        "l"(a_desc), "l"(b_desc), "r"(kIdesc), "r"(sfa), "r"(sfb), "r"(accumulate)
-        : "memory");
-}
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, uint32_t v) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(taddr), "r"(v)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(taddr)
-        : "memory");
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// 16 bits -> 16 e2m1 values (0 or 1.0 = 0x2), 8 bytes.  Bit pairs (4q, 4q+1)
-// go to byte q of the low word, pairs (4q+2, 4q+3) to byte q of the high
-// word, each pair through a 4-entry byte table (PRMT).  A and B go through
-// the same map, so K positions pair bit j with bit j.
-__device__ __forceinline__ uint2 spread16(uint32_t x) {
-    constexpr uint32_t kPairs = 0x22200200u;  // byte g = e2m1 pair of bits (g & 1, g >> 1)
-    return make_uint2(__byte_perm(kPairs, 0u, x & 0x3333u), __byte_perm(kPairs, 0u, (x >> 2) & 0x3333u));
-}
-__device__ __forceinline__ void sts64(uint32_t addr, uint2 v) {
-    asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(addr), "r"(v.x), "r"(v.y) : "memory");
-}
-__device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
-    uint32_t v;
-    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
-    return v;
-}
-__device__ __forceinline__ uint32_t lds_u16(uint32_t addr) {
-    uint16_t v;
-    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(addr));
-    return v;
-}
 
 }  // namespace
 
@@ -231,10 +119,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         misc[1] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < 256; i += kThreads) {
-        ginv[i] = d_ginv_lo[i];
-        ginv[256 + i] = d_ginv_hi[i];
-    }
+    for (int i = tid; i < 512; i += kThreads) ginv[i] = d_ginv[i];
     if (warp == 1) {  // the whole of TMEM: two accumulators and the scale factors
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(sbase + kOffMisc)
                      : "memory");
@@ -347,7 +232,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int j = 0; j < 4; ++j) {
                     const uint32_t it = (uint32_t)gw + 8u * j, t = it >> 4, grp = it & 15u;
                     const uint32_t m = grp * 8 + m8;
-                    const uint32_t T = s < S ? lds_u32(ins + (sl * kTileRows + 8 * t + (m >> 4)) * 4) : 0u;
+                    const uint32_t T = s < S ? lds_b32(ins + (sl * kTileRows + 8 * t + (m >> 4)) * 4) : 0u;
                     sts64(a + t * kATileBytes + grp * 256 + lane_off, spread16((T >> (m & 15u)) & 0xFFFFu));
                 }
                 // B: 30 groups of 8 symbols
@@ -490,8 +375,8 @@ cudaError_t mma_prepare() {
     if (!build_trace_tables(tlo, thi, glo, ghi)) return cudaErrorInvalidValue;
     if ((e = cudaMemcpyToSymbol(d_trace_lo, tlo, sizeof tlo)) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(d_trace_hi, thi, sizeof thi)) != cudaSuccess) return e;
-    if ((e = cudaMemcpyToSymbol(d_ginv_lo, glo, sizeof glo)) != cudaSuccess) return e;
-    if ((e = cudaMemcpyToSymbol(d_ginv_hi, ghi, sizeof ghi)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(d_ginv, glo, sizeof glo)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(d_ginv, ghi, sizeof ghi, sizeof glo)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(encode_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes)) !=
         cudaSuccess)
         return e;
@@ -499,6 +384,52 @@ cudaError_t mma_prepare() {
     return cudaSuccess;
 }
 }  // namespace
+
+cudaError_t mma_tables_ready(const uint16_t** ginv) {
+    cudaError_t e = mma_prepare();
+    if (e != cudaSuccess) return e;
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, d_ginv);
+    *ginv = static_cast<const uint16_t*>(p);
+    return e;
+}
+
+// The trace strings of every tensor-core job of a batch (blockIdx.y = job),
+// as tc_coef_kernel computes them for one.
+__global__ void tc_coef_batch_kernel(const BatchJob* __restrict__ jobs, const uint16_t* __restrict__ antilog,
+                                     const uint16_t* __restrict__ logbase) {
+    const BatchJob& J = jobs[blockIdx.y];
+    if (!J.mma || !J.R || !J.tcoef) return;
+    const uint64_t total = (uint64_t)J.S * J.Rpad;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = (uint32_t)(i / J.Rpad), r = (uint32_t)(i % J.Rpad);
+        uint32_t T = 0;
+        if (r < J.R) {
+            const uint32_t e = (J.first_exp + r) % kFieldLimit;
+            uint32_t k = (uint32_t)logbase[s] * e;
+            k = (k & 0xFFFFu) + (k >> 16);
+            k = (k & 0xFFFFu) + (k >> 16);
+            if (k >= kFieldLimit) k -= kFieldLimit;
+            const uint32_t c = antilog[k];
+            T = d_trace_lo[c & 0xFFu] ^ d_trace_hi[c >> 8];
+        }
+        J.tcoef[i] = T;
+    }
+}
+
+cudaError_t launch_tc_coef_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_words, cudaStream_t st) {
+    if (!n_jobs || !max_words) return cudaSuccess;
+    const uint16_t* g = nullptr;
+    cudaError_t e = mma_tables_ready(&g);
+    if (e != cudaSuccess) return e;
+    const uint16_t *antilog = nullptr, *logbase = nullptr;
+    if ((e = gf_device_tables(&antilog, &logbase)) != cudaSuccess) return e;
+    const uint64_t want = (max_words + 255) / 256;
+    const unsigned bx = (unsigned)std::min<uint64_t>(want, (uint64_t)device_sm_count() * 4);
+    tc_coef_batch_kernel<<<dim3(bx, n_jobs), 256, 0, st>>>(jobs, antilog, logbase);
+    add_launches(1);
+    return cudaGetLastError();
+}
 
 size_t mma_coef_bytes(uint32_t S, uint32_t R) {
     const uint64_t Rpad = (uint64_t)(R + kTileRows - 1) / kTileRows * kTileRows;

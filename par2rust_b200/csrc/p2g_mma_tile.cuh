@@ -1,0 +1,361 @@
+// p2g_mma_tile.cuh -- device code of the tensor-core (tcgen05, kind::mxf4)
+// encode shared by its standalone kernel (p2g_mma.cu) and the persistent
+// batch kernel (p2g_kernels.cu).
+//
+// The arithmetic (bits(c*x) = G^-1 H_c bits(x), H_c a Hankel matrix from the
+// 31-bit trace string T_c) is explained at the top of p2g_mma.cu.  Here: the
+// shared-memory and TMEM layout of one CTA and the work of one 16-row x
+// 240-symbol tile over a range of input slices.
+//
+// Shared memory (from `ring`, 1024-aligned): kOpStages operand stages of 16
+// KiB (A rows of the two 8-row halves, 4 KiB each; B rows, 7,680 B), then
+// kInStages input stages of 2,304 B (the 16 rows' trace strings of 4 slices,
+// 256 B; then the tile's bytes of those 4 slices, 4 x 480 B).  Both operands
+// are K-major without swizzle: core matrices of 8 rows x 16 B, K halves
+// 128 B apart, 8-row groups 256 B apart.  TMEM: the two fp32 accumulators at
+// columns 0 and 256 (240 columns each), scale factors 1.0 at 496-511.
+#pragma once
+#include <stdint.h>
+
+namespace p2g {
+namespace mma {
+
+constexpr uint32_t kN = 240;        // symbols per tile (MMA N)
+constexpr uint32_t kTileRows = 16;  // recovery rows per tile (two M = 128 MMAs)
+constexpr uint32_t kKSlices = 4;    // input slices per K-step (K = 64 e2m1 values)
+constexpr int kOpStages = 8;
+constexpr int kInStages = 8;
+constexpr uint32_t kAccCol1 = 256;                // TMEM column of the second accumulator
+constexpr uint32_t kSfaCol = 496, kSfbCol = 504;  // scale factors (all 1.0)
+constexpr uint32_t kATileBytes = 4096;            // 128 rows x 32 B
+constexpr uint32_t kBTileBytes = kN * 32;         // 240 rows x 32 B
+constexpr uint32_t kOpStageBytes = 2 * kATileBytes + 8192;
+constexpr uint32_t kSrcSliceBytes = kN * 2;
+constexpr uint32_t kInCoefBytes = kKSlices * kTileRows * 4;
+constexpr uint32_t kInStageBytes = 2304;
+constexpr uint32_t kRingBytes = kOpStages * kOpStageBytes + kInStages * kInStageBytes;
+constexpr uint32_t kGinvBytes = 1024;             // G^-1 tables: 256 lo then 256 hi u16
+constexpr uint32_t kNumBars = 2 * kInStages + 2 * kOpStages + 3;
+constexpr uint32_t kBarBytes = kNumBars * 8;
+static_assert(kBTileBytes <= kOpStageBytes - 2 * kATileBytes, "B tile fits its stage");
+static_assert(kInCoefBytes + kKSlices * kSrcSliceBytes <= kInStageBytes, "input stage");
+
+// Instruction descriptor of kind::mxf4 with UE8M0 block scales: A and B
+// e2m1 (format 1 at bits 7 and 10), K-major, N >> 3 at bit 17, scale format
+// UE8M0 at bit 23, M >> 4 at bit 24, scale-factor ids 0, dense K = 64.
+constexpr uint32_t kIdesc = (1u << 7) | (1u << 10) | ((kN >> 3) << 17) | (1u << 23) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false when it gave up (it then sets the abort flag) or when
+// another role has given up.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, volatile uint32_t* abort_flag) {
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        if (bar_try_wait(bar, parity)) return true;
+        if ((it & 255u) == 255u && *abort_flag) return false;
+    }
+    *abort_flag = 1u;
+    return false;
+}
+// Waits (bounded) for a phase without looking at the abort flag: for
+// copies and MMAs in flight, which land whatever happened elsewhere.
+__device__ __forceinline__ void bar_drain(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < (1u << 22) && !bar_try_wait(bar, parity); ++it) {
+    }
+}
+__device__ __forceinline__ void tma_1d(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Shared-memory matrix descriptor, K-major, no swizzle: start >> 4, leading
+// (K-half) byte offset >> 4 at bit 16, stride (8-row group) byte offset >> 4
+// at bit 32, version 1 at bit 46.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void mma_mxf4(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t sfa,
+                                         uint32_t sfb, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %6, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%4], [%5], p;\n}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(kIdesc), "r"(sfa), "r"(sfb), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, uint32_t v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(taddr), "r"(v)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+// 16 bits -> 16 e2m1 values (0 or 1.0 = 0x2), 8 bytes.  Bit pairs (4q, 4q+1)
+// go to byte q of the low word, pairs (4q+2, 4q+3) to byte q of the high
+// word, each pair through a 4-entry byte table (PRMT).  A and B go through
+// the same map, so K positions pair bit j with bit j.
+__device__ __forceinline__ uint2 spread16(uint32_t x) {
+    constexpr uint32_t kPairs = 0x22200200u;  // byte g = e2m1 pair of bits (g & 1, g >> 1)
+    return make_uint2(__byte_perm(kPairs, 0u, x & 0x3333u), __byte_perm(kPairs, 0u, (x >> 2) & 0x3333u));
+}
+__device__ __forceinline__ void sts64(uint32_t addr, uint2 v) {
+    asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(addr), "r"(v.x), "r"(v.y) : "memory");
+}
+__device__ __forceinline__ uint32_t lds_b32(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ uint32_t lds_u16(uint32_t addr) {
+    uint16_t v;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(addr));
+    return v;
+}
+
+// Barrier block: in_full[kInStages], in_empty[kInStages], op_full[kOpStages],
+// op_empty[kOpStages], acc_full, acc_empty, drain.
+struct Bars {
+    uint32_t in_full, in_empty, op_full, op_empty, acc_full, acc_empty, drain;
+    __device__ explicit Bars(uint32_t b)
+        : in_full(b), in_empty(b + 8 * kInStages), op_full(b + 16 * kInStages),
+          op_empty(b + 16 * kInStages + 8 * kOpStages), acc_full(b + 16 * kInStages + 16 * kOpStages),
+          acc_empty(acc_full + 8), drain(acc_full + 16) {}
+};
+// One thread: counts for `ngen` operand-building warps.
+__device__ __forceinline__ void init_bars(uint32_t b, uint32_t ngen) {
+    const Bars B(b);
+    for (int i = 0; i < kInStages; ++i) {
+        bar_init(B.in_full + 8 * i, 1);
+        bar_init(B.in_empty + 8 * i, ngen);
+    }
+    for (int i = 0; i < kOpStages; ++i) {
+        bar_init(B.op_full + 8 * i, ngen);
+        bar_init(B.op_empty + 8 * i, 1);
+    }
+    bar_init(B.acc_full, 1);
+    bar_init(B.acc_empty, ngen);
+    bar_init(B.drain, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// The whole of TMEM (one warp; the slot receives the base address), and
+// given up again at the end by the same warp.
+__device__ __forceinline__ void tmem_alloc(uint32_t slot) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(slot) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_free(uint32_t tmem) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+// Scale factors 1.0 (UE8M0 127) over the 32 lanes of warp quadrant q,
+// columns 496..511 (called by four warps with distinct quadrants).
+__device__ __forceinline__ void sf_fill(uint32_t tmem, uint32_t q) {
+    const uint32_t t = tmem + ((32 * q) << 16) + kSfaCol;
+    tmem_st8(t, 0x7F7F7F7Fu);
+    tmem_st8(t + 8, 0x7F7F7F7Fu);
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// One tile: recovery rows [r0, r0+16) x symbols [n0, n0+syms) over input
+// slices [s0, s0+sn).  Slice s of the source is at src + s*src_stride; its
+// trace strings at tcoef + s*Rpad (rows past R hold 0).  accumulate: XOR the
+// tile into the rows (the caller zeroed them) instead of storing it.
+struct Tile {
+    const uint8_t* src;
+    uint64_t src_stride;
+    const uint32_t* tcoef;
+    uint8_t* rec;
+    uint64_t rec_stride;
+    uint32_t s0, sn, Rpad, R, r0, n0, syms, accumulate;
+};
+
+// Per-CTA pipeline state, the same in every thread: K-steps, tiles and
+// drains so far (ring positions and barrier parities follow from them).
+struct Pipe {
+    uint32_t ring, bars, tmem;
+    const uint16_t* ginv;  // shared memory
+    volatile uint32_t* abort_flag;
+    uint32_t g, tcount, drains;
+};
+
+// All threads of the CTA call this.  Warp 0 lane 0 streams the inputs, warp
+// 1 lane 0 issues the MMAs, warps 2 .. 2+NGEN-1 build operands and run the
+// epilogue (the first eight of them; warp w reads TMEM lanes 32*(w%4)..).
+// Other warps idle.  Returns false (uniformly, after a CTA barrier) when a
+// bounded wait gave up; copies and MMAs in flight have then landed.
+template <int NGEN>
+__device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
+    static_assert(NGEN >= 8, "eight warps cover the two accumulators' four lane quadrants");
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const Bars B(P.bars);
+    const uint32_t op0 = P.ring, in0 = P.ring + kOpStages * kOpStageBytes;
+    const uint32_t KS = (T.sn + kKSlices - 1) / kKSlices;
+    const uint32_t g0 = P.g, tc = P.tcount;
+    bool ok = true;
+    if (warp == 0) {
+        if (lane == 0) {
+            const uint32_t bytes = 2 * T.syms;
+            uint32_t g = g0;
+            for (uint32_t k = 0; k < KS; ++k, ++g) {
+                const uint32_t st = g % kInStages;
+                if (!bar_wait(B.in_empty + 8 * st, ((g / kInStages) & 1u) ^ 1u, P.abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t sa = T.s0 + k * kKSlices, ns = min(kKSlices, T.s0 + T.sn - sa);
+                const uint32_t dst = in0 + st * kInStageBytes;
+                bar_expect_tx(B.in_full + 8 * st, ns * (bytes + kTileRows * 4));
+                for (uint32_t j = 0; j < ns; ++j) {
+                    tma_1d(dst + j * kTileRows * 4, T.tcoef + (size_t)(sa + j) * T.Rpad + T.r0, kTileRows * 4,
+                           B.in_full + 8 * st);
+                    tma_1d(dst + kInCoefBytes + j * kSrcSliceBytes,
+                           T.src + (size_t)(sa + j) * T.src_stride + (size_t)T.n0 * 2, bytes, B.in_full + 8 * st);
+                }
+            }
+            if (!ok)  // copies issued but maybe not consumed land before the stages are reused
+                for (uint32_t b = g > g0 + kInStages ? g - kInStages : g0; b < g; ++b)
+                    bar_drain(B.in_full + 8 * (b % kInStages), (b / kInStages) & 1u);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const bool two = T.R - T.r0 > 8;
+            if (!bar_wait(B.acc_empty, (tc & 1u) ^ 1u, P.abort_flag)) ok = false;
+            tc_fence_after();
+            uint32_t g = g0;
+            for (uint32_t k = 0; ok && k < KS; ++k, ++g) {
+                const uint32_t so = g % kOpStages;
+                if (!bar_wait(B.op_full + 8 * so, (g / kOpStages) & 1u, P.abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t a = op0 + so * kOpStageBytes;
+                const uint64_t bdesc = smem_desc(a + 2 * kATileBytes, 128, 256);
+                mma_mxf4(P.tmem, smem_desc(a, 128, 256), bdesc, P.tmem + kSfaCol, P.tmem + kSfbCol, k > 0);
+                if (two)
+                    mma_mxf4(P.tmem + kAccCol1, smem_desc(a + kATileBytes, 128, 256), bdesc, P.tmem + kSfaCol,
+                             P.tmem + kSfbCol, k > 0);
+                mma_commit(B.op_empty + 8 * so);
+            }
+            if (ok) {
+                mma_commit(B.acc_full);
+            } else {  // every MMA issued completes before its stages or TMEM are reused
+                mma_commit(B.drain);
+                bar_drain(B.drain, P.drains & 1u);
+            }
+        }
+    } else if (warp < 2 + NGEN) {
+        const int gw = warp - 2;
+        const uint32_t m8 = (uint32_t)lane >> 2, sl = (uint32_t)lane & 3u;
+        const uint32_t lane_off = (sl >> 1) * 128 + m8 * 16 + (sl & 1u) * 8;  // canonical K-major position
+        uint32_t g = g0;
+        for (uint32_t k = 0; k < KS; ++k, ++g) {
+            const uint32_t si = g % kInStages, so = g % kOpStages;
+            if (!bar_wait(B.in_full + 8 * si, (g / kInStages) & 1u, P.abort_flag) ||
+                !bar_wait(B.op_empty + 8 * so, ((g / kOpStages) & 1u) ^ 1u, P.abort_flag)) {
+                ok = false;
+                break;
+            }
+            const uint32_t a = op0 + so * kOpStageBytes, ins = in0 + si * kInStageBytes;
+            const bool live = k * kKSlices + sl < T.sn;  // slices past the range were not loaded
+            // 32 groups of 8 A rows (row m = 16*rl + i of half t is bits i..i+15
+            // of T for recovery row r0 + 8t + rl), then 30 groups of 8 B rows
+            for (uint32_t it = (uint32_t)gw; it < 62; it += NGEN) {
+                if (it < 32) {
+                    const uint32_t t = it >> 4, grp = it & 15u, m = grp * 8 + m8;
+                    const uint32_t Tc = live ? lds_b32(ins + (sl * kTileRows + 8 * t + (m >> 4)) * 4) : 0u;
+                    sts64(a + t * kATileBytes + grp * 256 + lane_off, spread16((Tc >> (m & 15u)) & 0xFFFFu));
+                } else {
+                    const uint32_t grp = it - 32, n = grp * 8 + m8;
+                    const uint32_t x =
+                        (live && n < T.syms) ? lds_u16(ins + kInCoefBytes + sl * kSrcSliceBytes + n * 2) : 0u;
+                    sts64(a + 2 * kATileBytes + grp * 256 + lane_off, spread16(x));
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+                bar_arrive(B.op_full + 8 * so);
+                bar_arrive(B.in_empty + 8 * si);
+            }
+        }
+        if (ok && !bar_wait(B.acc_full, tc & 1u, P.abort_flag)) ok = false;
+        if (ok && gw < 8) {
+            tc_fence_after();
+            const uint32_t q = (uint32_t)warp & 3u, t = (uint32_t)gw >> 2;
+            const uint32_t ra = T.r0 + 8 * t + 2 * q, rb = ra + 1;
+            if (ra < T.R) {
+                for (uint32_t c0 = 0; c0 < kN; c0 += 32) {
+                    uint32_t v[32];
+                    tmem_ld32(P.tmem + ((32 * q) << 16) + t * kAccCol1 + c0, v);
+                    uint32_t mine = 0;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const uint32_t b = __ballot_sync(0xFFFFFFFFu, __float2uint_rz(__uint_as_float(v[j])) & 1u);
+                        if (lane == j) mine = b;
+                    }
+                    // ballot lanes 0-15: the bits of row ra, lanes 16-31: row rb
+                    const uint32_t col = c0 + (uint32_t)lane;
+                    const uint32_t ya = mine & 0xFFFFu, yb = mine >> 16;
+                    const uint32_t va = P.ginv[ya & 0xFFu] ^ P.ginv[256 + (ya >> 8)];
+                    const uint32_t vb = rb < T.R ? P.ginv[yb & 0xFFu] ^ P.ginv[256 + (yb >> 8)] : 0u;
+                    if (T.accumulate) {
+                        // pairs of columns as 32-bit words (tiles start on an even symbol)
+                        const uint32_t wa = va | (__shfl_down_sync(0xFFFFFFFFu, va, 1) << 16);
+                        const uint32_t wb = vb | (__shfl_down_sync(0xFFFFFFFFu, vb, 1) << 16);
+                        if (!(lane & 1) && col < T.syms) {
+                            uint8_t* p = T.rec + (size_t)ra * T.rec_stride + (size_t)(T.n0 + col) * 2;
+                            atomicXor(reinterpret_cast<unsigned int*>(p), wa);
+                            if (rb < T.R) atomicXor(reinterpret_cast<unsigned int*>(p + T.rec_stride), wb);
+                        }
+                    } else if (col < T.syms) {
+                        uint8_t* p = T.rec + (size_t)ra * T.rec_stride + (size_t)(T.n0 + col) * 2;
+                        *reinterpret_cast<uint16_t*>(p) = (uint16_t)va;
+                        if (rb < T.R) *reinterpret_cast<uint16_t*>(p + T.rec_stride) = (uint16_t)vb;
+                    }
+                }
+            }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (ok && lane == 0) bar_arrive(B.acc_empty);
+    }
+    const bool bad = __syncthreads_or(!ok) != 0;
+    P.g += KS;
+    P.tcount += 1;
+    if (bad) P.drains += 1;
+    return !bad;
+}
+
+}  // namespace mma
+}  // namespace p2g

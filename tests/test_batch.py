@@ -90,11 +90,14 @@ def test_device_job_plan_covers_every_slice_of_every_tile_once(p2g, slice_, S, R
     items, zero_from, bands = p2g.plan_device_job(slice_, S, R)
     Np = (slice_ + 15) // 16 * 16 // 2
     assert items and 0 <= zero_from <= Np
-    RG = (R + 31) // 32
+    tensor = items[0]["fold"] == 0  # tensor-core tiles: 16 rows, at most 240 symbols
+    assert all((it["fold"] == 0) == tensor for it in items)
+    RG = (R + 15) // 16 if tensor else (R + 31) // 32
     pieces = {}
     for it in items:
-        assert 0 <= it["row_group"] < RG and it["fold"] in (1, 2, 4)
-        assert it["fold"] == 1 or it["row_group"] == RG - 1
+        assert 0 <= it["row_group"] < RG and it["fold"] in ((0,) if tensor else (1, 2, 4))
+        assert it["fold"] <= 1 or it["row_group"] == RG - 1
+        assert not tensor or (it["symbols"] <= 240 and it["first_symbol"] % 240 == 0)
         assert 0 < it["symbols"] and it["first_symbol"] + it["symbols"] <= Np
         assert 0 <= it["first_slice"] and it["first_slice"] + it["slices"] <= S and it["slices"] > 0
         assert it["accumulate"] == (0 if it["slices"] == S else 1)
@@ -121,7 +124,7 @@ def test_device_job_plan_covers_every_slice_of_every_tile_once(p2g, slice_, S, R
             seq = sorted((n0, ps[0][4]) for (g, n0), ps in pieces.items() if g == rg)
             assert all(a[1] <= b[1] for a, b in zip(seq, seq[1:])), (rg, seq)
         for (g, n0), ps in pieces.items():
-            if ps[0][3] == 1:
+            if ps[0][3] <= 1:
                 assert band_at.setdefault(n0, ps[0][4]) == ps[0][4], (g, n0)
     # every row group covers every symbol (a folded tail item covers `fold` tiles)
     for rg in range(RG):
@@ -249,10 +252,15 @@ def batch_jobs(p2g):
 
 
 @pytest.mark.gpu
-def test_batch_matches_oracle(p2g, oracle, gpu, batch_jobs):
+@pytest.mark.parametrize("variant", ["by-shape", "tensor", "lut"])
+def test_batch_matches_oracle(p2g, oracle, gpu, batch_jobs, variant):
     import torch
 
-    b = p2g.Batch([j for j, _, _ in batch_jobs])
+    flags = {"by-shape": 0, "tensor": p2g.BATCH_TENSOR, "lut": p2g.BATCH_LUT}[variant]
+    for j, _, _ in batch_jobs:  # no stale rows from an earlier run
+        j.bufs.recovery.fill_(0xA5)
+        j.bufs.packet_md5.zero_()
+    b = p2g.Batch([j for j, _, _ in batch_jobs], flags=flags)
     b.launch()
     torch.cuda.synchronize()
     b.check()

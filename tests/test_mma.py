@@ -59,3 +59,31 @@ def test_tensor_encode_large_sums_stay_exact(p2g, gpu, oracle):
     got = p2g.encode(src, sl, R, variant=p2g.ENCODE_TENSOR).reshape(R, sl)
     want = oracle.encode_fast(src, S, sl, R).reshape(R, sl)
     assert np.array_equal(got, want)
+
+
+DEVICE_JOB_SHAPES = [  # (file lengths, slice, R): tail split, ragged slices, several files, R % 16 != 0
+    ([100 * 524288 - 777], 524288, 200), ([600 * 4100 - 3], 4100, 100), ([100 * 65540], 65540, 30),
+    ([70_001, 4096 * 9, 123], 4096, 17), ([16_777_216], 65536, 32),
+]
+
+
+@pytest.mark.parametrize("lengths,slice_,R", DEVICE_JOB_SHAPES)
+def test_device_job_on_tensor_cores_matches_oracle(p2g, gpu, oracle, lengths, slice_, R):
+    """The whole device job (persistent kernel with tensor-core encode items,
+    packet-MD5 chains per band, the tail split's accumulating pieces) against
+    the oracle: every row, checksum, hash and packet MD5."""
+    import torch
+
+    from oracle import parity
+    from par2rust_b200.workloads import file_bytes
+
+    files = [file_bytes(31 * k + R, n) for k, n in enumerate(lengths)]
+    src = torch.from_numpy(parity.padded_source(files, slice_)).cuda()
+    names = [f"f{k}.bin".encode() for k in range(len(files))]
+    S = src.numel() // slice_
+    bufs = p2g.run_device_job(src, lengths, names, slice_, R, variant=p2g.ENCODE_TENSOR)
+    torch.cuda.synchronize()
+    out = parity.device_outputs(bufs, S, len(files), slice_, R)
+    bad = parity.check_device_job(files, names, slice_, R, out["rec"], out["checks"], out["hash16k"], bufs.set_id,
+                                  out["packet_md5"], hash_full=out["hash_full"])
+    assert not bad, bad
