@@ -1373,6 +1373,10 @@ __device__ void advance_all(const BatchJob& J, uint32_t ring, uint32_t* misc) {
     for (uint32_t q = 0; q < Q; ++q) try_advance(J, q, ring, misc);
 }
 
+// MMA: the launch has tensor-core items (mma_ginv set).  The variant without
+// them keeps the other item kinds' code free of the tensor pipeline's
+// registers.
+template <bool MMA>
 __global__ void __launch_bounds__(kEncThreads, 1)
     batch_kernel(const BatchJob* __restrict__ jobs, const BatchItem* __restrict__ items, uint32_t n_items,
                  uint32_t* __restrict__ ctl, int* __restrict__ err, const uint16_t* __restrict__ mma_ginv) {
@@ -1391,16 +1395,16 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     const uint32_t mma_bars = smem_u32(smem + kBatchMmaBarsOff);
     if (tid == 0) {
         for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
-        if (mma_ginv) {
+        if (MMA) {
             mma::init_bars(mma_bars, 14);
             mma_misc[1] = mma_misc[2] = mma_misc[3] = mma_misc[4] = 0;
         }
         fence_mbar_init();
     }
-    if (mma_ginv && (tid >> 5) == 1) mma::tmem_alloc(smem_u32(mma_misc));
-    mma::tc_fence_before();
+    if (MMA && (tid >> 5) == 1) mma::tmem_alloc(smem_u32(mma_misc));
+    if (MMA) mma::tc_fence_before();
     crc_tables_build(T);  // ends with __syncthreads
-    if (mma_ginv) {
+    if (MMA) {
         mma::tc_fence_after();
         if ((tid >> 5) >= 4 && (tid >> 5) < 8) mma::sf_fill(mma_misc[0], (uint32_t)(tid >> 5) & 3u);
         mma::tc_fence_before();
@@ -1461,7 +1465,7 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             batch_packets(J, ring, misc + 4, it.a, it.a + it.b);
             continue;
         }
-        if (kind == kItemEncodeMma) {
+        if (MMA && kind == kItemEncodeMma) {
             const bool ok = batch_mma_tile(&J, mma_ginv, it.kind_rg, it.a, it.b, it.s0, it.sn);
             // the operand rings covered the encode region's barriers: set them up again
             if (tid == 0) {
@@ -1511,7 +1515,7 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             advance_all(J, ring, misc);
         }
     }
-    if (mma_ginv) {  // every MMA issued has completed before TMEM is given back
+    if (MMA) {  // every MMA issued has completed before TMEM is given back
         mma::tc_fence_before();
         __syncthreads();
         if ((tid >> 5) == 1) {
@@ -1958,7 +1962,10 @@ cudaError_t prepare_batch_kernel() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 256 || !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem);
+        cudaError_t e =
+            cudaFuncSetAttribute(batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 256) attr_set[dev] = true;
     }
@@ -1972,7 +1979,10 @@ cudaError_t launch_batch(const BatchJob* jobs, const BatchItem* items, uint32_t 
     if (e != cudaSuccess) return e;
     const uint16_t* ginv = nullptr;
     if (mma && (e = mma_tables_ready(&ginv)) != cudaSuccess) return e;
-    batch_kernel<<<ctas, kEncThreads, kBatchSmem, st>>>(jobs, items, n_items, ctl, err, ginv);
+    if (mma)
+        batch_kernel<true><<<ctas, kEncThreads, kBatchSmem, st>>>(jobs, items, n_items, ctl, err, ginv);
+    else
+        batch_kernel<false><<<ctas, kEncThreads, kBatchSmem, st>>>(jobs, items, n_items, ctl, err, nullptr);
     count_launch();
     return cudaGetLastError();
 }

@@ -26,10 +26,13 @@
 //   warp 0       TMA producer: 1-D bulk copies of 4 source slices' tile bytes
 //                and of the 16 rows' trace strings of those slices
 //   warp 1       TMEM allocation; lane 0 issues the MMAs and commits
-//   warps 2..9   operand builders (A rows from T_c, B rows from source
+//   warps 2..15  operand builders (A rows from T_c, B rows from source
 //                symbols, both spread to e2m1 in the canonical K-major
-//                layout), then the epilogue: tcgen05.ld of the sums, parity,
-//                one ballot per column (= two recovery symbols), G^-1, store.
+//                layout, 16-byte K halves), then (warps 2..9) the epilogue:
+//                tcgen05.ld of the sums, parity, one ballot per column (= two
+//                recovery symbols), G^-1, store.
+// The tile pipeline itself is p2g_mma_tile.cuh, shared with the persistent
+// batch kernel's tensor-core items.
 // Every mbarrier wait is bounded; a wait that gives up sets the error flag,
 // stops all roles, drains copies and MMAs in flight and frees TMEM.
 #include <mutex>
@@ -48,7 +51,7 @@ __device__ uint16_t d_ginv[512];
 namespace {
 
 using namespace mma;
-constexpr int kGenWarps = 8;
+constexpr int kGenWarps = 14;
 constexpr int kThreads = 64 + 32 * kGenWarps;
 
 // shared memory layout (bytes): the rings, G^-1 tables, barriers, misc
@@ -92,207 +95,56 @@ __global__ void __launch_bounds__(kThreads, 1)
                       const uint32_t* __restrict__ tcoef, uint32_t Rpad, uint32_t R, uint8_t* __restrict__ rec,
                       uint64_t rec_stride, uint32_t n_row_tiles, uint32_t n_tiles, int* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t sbase = smem_addr(smem);
-    const uint32_t op0 = sbase + kOffOp, in0 = sbase + kOffIn;
+    const int tid = threadIdx.x, warp = tid >> 5;
     uint16_t* ginv = reinterpret_cast<uint16_t*>(smem + kOffGinv);  // [0,256) lo, [256,512) hi
-    const uint32_t bars = sbase + kOffBars;
-    const uint32_t in_full = bars, in_empty = bars + 8 * kInStages;
-    const uint32_t op_full = bars + 16 * kInStages, op_empty = op_full + 8 * kOpStages;
-    const uint32_t acc_full = op_empty + 8 * kOpStages, acc_empty = acc_full + 8, drain = acc_full + 16;
     uint32_t* misc = reinterpret_cast<uint32_t*>(smem + kOffMisc);  // [0] TMEM base, [1] abort
-    volatile uint32_t* abort_flag = misc + 1;
-    const uint32_t KS = (S + kKSlices - 1) / kKSlices;
-
+    mma::Pipe P;
+    P.ring = smem_addr(smem + kOffOp);
+    P.bars = smem_addr(smem + kOffBars);
+    P.ginv = ginv;
+    P.abort_flag = misc + 1;
+    P.g = P.tcount = P.drains = 0;
     if (tid == 0) {
-        for (int i = 0; i < kInStages; ++i) {
-            bar_init(in_full + 8 * i, 1);
-            bar_init(in_empty + 8 * i, kGenWarps);
-        }
-        for (int i = 0; i < kOpStages; ++i) {
-            bar_init(op_full + 8 * i, kGenWarps);
-            bar_init(op_empty + 8 * i, 1);
-        }
-        bar_init(acc_full, 1);
-        bar_init(acc_empty, kGenWarps);
-        bar_init(drain, 1);
+        init_bars(P.bars, kGenWarps);
         misc[1] = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < 512; i += kThreads) ginv[i] = d_ginv[i];
-    if (warp == 1) {  // the whole of TMEM: two accumulators and the scale factors
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(sbase + kOffMisc)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
+    if (warp == 1) tmem_alloc(smem_addr(misc));  // the whole of TMEM: two accumulators and the scale factors
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = misc[0];
-    if (warp >= 2 && warp < 6) {  // scale factors 1.0 over all 128 lanes, columns 496..511
-        const uint32_t t = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + kSfaCol;
-        tmem_st8(t, 0x7F7F7F7Fu);
-        tmem_st8(t + 8, 0x7F7F7F7Fu);
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-    }
+    P.tmem = misc[0];
+    if (warp >= 4 && warp < 8) sf_fill(P.tmem, (uint32_t)warp & 3u);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-
-    if (warp == 0) {
-        // ---- producer: the tile's bytes of 4 source slices per K-step ----
-        if (lane == 0) {
-            uint32_t g = 0;
-            bool ok = true;
-            for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
-                const uint32_t n0 = (tile / n_row_tiles) * kN;
-                const uint32_t r0 = (tile % n_row_tiles) * kTileRows;
-                const uint32_t bytes = 2 * min(kN, Np - n0);
-                for (uint32_t k = 0; k < KS; ++k, ++g) {
-                    const uint32_t st = g % kInStages;
-                    if (!bar_wait(in_empty + 8 * st, ((g / kInStages) & 1u) ^ 1u, abort_flag)) {
-                        ok = false;
-                        break;
-                    }
-                    const uint32_t s0 = k * kKSlices, ns = min(kKSlices, S - s0);
-                    const uint32_t dst = in0 + st * kInStageBytes;
-                    bar_expect_tx(in_full + 8 * st, ns * (bytes + kTileRows * 4));
-                    for (uint32_t j = 0; j < ns; ++j) {
-                        tma_1d(dst + j * kTileRows * 4, tcoef + (size_t)(s0 + j) * Rpad + r0, kTileRows * 4,
-                               in_full + 8 * st);
-                        tma_1d(dst + kInCoefBytes + j * kSrcSliceBytes,
-                               src + (size_t)(s0 + j) * src_stride + (size_t)n0 * 2, bytes, in_full + 8 * st);
-                    }
-                }
-            }
-            // copies still in flight land before the CTA's shared memory goes away
-            for (uint32_t b = g > (uint32_t)kInStages ? g - kInStages : 0; b < g; ++b) {
-                const uint32_t st = b % kInStages;
-                for (uint32_t it = 0; it < (1u << 22) && !bar_try_wait(in_full + 8 * st, (b / kInStages) & 1u); ++it) {
-                }
-            }
-        }
-    } else if (warp == 1) {
-        // ---- MMA issuer ----
-        if (lane == 0) {
-            uint32_t g = 0, tcount = 0;
-            bool ok = true;
-            for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, ++tcount) {
-                const uint32_t r0 = (tile % n_row_tiles) * kTileRows;
-                const bool two = R - r0 > 8;
-                if (!bar_wait(acc_empty, (tcount & 1u) ^ 1u, abort_flag)) break;
-                tc_fence_after();
-                for (uint32_t k = 0; k < KS; ++k, ++g) {
-                    const uint32_t so = g % kOpStages;
-                    if (!bar_wait(op_full + 8 * so, (g / kOpStages) & 1u, abort_flag)) {
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint32_t a = op0 + so * kOpStageBytes;
-                    const uint64_t bdesc = smem_desc(a + 2 * kATileBytes, 128, 256);
-                    mma_mxf4(tmem, smem_desc(a, 128, 256), bdesc, tmem + kSfaCol, tmem + kSfbCol, k > 0);
-                    if (two)
-                        mma_mxf4(tmem + kAccCol1, smem_desc(a + kATileBytes, 128, 256), bdesc, tmem + kSfaCol,
-                                 tmem + kSfbCol, k > 0);
-                    mma_commit(op_empty + 8 * so);
-                }
-                if (ok) mma_commit(acc_full);
-            }
-            // every MMA issued has completed before TMEM is freed
-            mma_commit(drain);
-            for (uint32_t it = 0; it < (1u << 22) && !bar_try_wait(drain, 0); ++it) {
-            }
-        }
-    } else {
-        // ---- operand builders, then the epilogue of each tile ----
-        const int gw = warp - 2;
-        const uint32_t m8 = (uint32_t)lane >> 2, sl = (uint32_t)lane & 3u;
-        const uint32_t lane_off = (sl >> 1) * 128 + m8 * 16 + (sl & 1u) * 8;  // canonical K-major position
-        uint32_t g = 0, tcount = 0;
-        bool ok = true;
-        for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, ++tcount) {
-            const uint32_t r0 = (tile % n_row_tiles) * kTileRows;
-            const uint32_t n0 = (tile / n_row_tiles) * kN;
-            const uint32_t syms = min(kN, Np - n0);
-            for (uint32_t k = 0; k < KS; ++k, ++g) {
-                const uint32_t si = g % kInStages, so = g % kOpStages;
-                if (!bar_wait(in_full + 8 * si, (g / kInStages) & 1u, abort_flag) ||
-                    !bar_wait(op_empty + 8 * so, ((g / kOpStages) & 1u) ^ 1u, abort_flag)) {
-                    ok = false;
-                    break;
-                }
-                const uint32_t a = op0 + so * kOpStageBytes;
-                const uint32_t s = k * kKSlices + sl;
-                const uint32_t ins = in0 + si * kInStageBytes;
-                // A: 2 tiles x 16 groups of 8 rows; row m = 16*rl + i of tile t
-                // is bits i..i+15 of T for recovery row r0 + 8t + rl (rows past
-                // R have T = 0; slices past S were not loaded)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const uint32_t it = (uint32_t)gw + 8u * j, t = it >> 4, grp = it & 15u;
-                    const uint32_t m = grp * 8 + m8;
-                    const uint32_t T = s < S ? lds_b32(ins + (sl * kTileRows + 8 * t + (m >> 4)) * 4) : 0u;
-                    sts64(a + t * kATileBytes + grp * 256 + lane_off, spread16((T >> (m & 15u)) & 0xFFFFu));
-                }
-                // B: 30 groups of 8 symbols
-                const uint32_t srcst = ins + kInCoefBytes + sl * kSrcSliceBytes;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const uint32_t grp = (uint32_t)gw + 8u * j;
-                    if (grp < kN / 8) {
-                        const uint32_t n = grp * 8 + m8;
-                        const uint32_t x = (n < syms && s < S) ? lds_u16(srcst + n * 2) : 0u;
-                        sts64(a + 2 * kATileBytes + grp * 256 + lane_off, spread16(x));
-                    }
-                }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) {
-                    bar_arrive(op_full + 8 * so);
-                    bar_arrive(in_empty + 8 * si);
-                }
-            }
-            if (!ok) break;
-            // epilogue: warp (t, q) reads lanes 32q.. of accumulator t
-            if (!bar_wait(acc_full, tcount & 1u, abort_flag)) break;
-            tc_fence_after();
-            const uint32_t q = (uint32_t)warp & 3u, t = (uint32_t)gw >> 2;
-            const uint32_t ra = r0 + 8 * t + 2 * q, rb = ra + 1;
-            if (ra < R) {
-                for (uint32_t c0 = 0; c0 < kN; c0 += 32) {
-                    uint32_t v[32];
-                    tmem_ld32(tmem + ((32 * q) << 16) + t * kAccCol1 + c0, v);
-                    uint32_t mine = 0;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const uint32_t b = __ballot_sync(0xFFFFFFFFu, __float2uint_rz(__uint_as_float(v[j])) & 1u);
-                        if (lane == j) mine = b;
-                    }
-                    // lanes 0-15 of the ballot: bits of row ra, lanes 16-31: row rb
-                    const uint32_t col = c0 + (uint32_t)lane;
-                    if (col < syms) {
-                        const uint32_t ya = mine & 0xFFFFu, yb = mine >> 16;
-                        const uint16_t va = ginv[ya & 0xFFu] ^ ginv[256 + (ya >> 8)];
-                        const uint16_t vb = ginv[yb & 0xFFu] ^ ginv[256 + (yb >> 8)];
-                        uint8_t* p = rec + (size_t)ra * rec_stride + (size_t)(n0 + col) * 2;
-                        *reinterpret_cast<uint16_t*>(p) = va;
-                        if (rb < R) *reinterpret_cast<uint16_t*>(p + rec_stride) = vb;
-                    }
-                }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) bar_arrive(acc_empty);
-        }
+    // tiles in order of symbol tile, row tile fastest: concurrent CTAs share
+    // their source bytes in L2
+    bool ok = true;
+    for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
+        Tile T;
+        T.src = src;
+        T.src_stride = src_stride;
+        T.tcoef = tcoef;
+        T.rec = rec;
+        T.rec_stride = rec_stride;
+        T.s0 = 0;
+        T.sn = S;
+        T.Rpad = Rpad;
+        T.R = R;
+        T.r0 = (tile % n_row_tiles) * kTileRows;
+        T.n0 = (tile / n_row_tiles) * kN;
+        T.syms = min(kN, Np - T.n0);
+        T.accumulate = 0;
+        ok = run_tile<kGenWarps>(P, T);
     }
+    if (tid == 0 && !ok) atomicOr(err, 1);
     tc_fence_before();
     __syncthreads();
-    if (tid == 0 && *abort_flag) atomicOr(err, 1);
     if (warp == 1) {
         __syncwarp();
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+        tmem_free(P.tmem);
     }
 }
 

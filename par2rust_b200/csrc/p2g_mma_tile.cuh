@@ -132,6 +132,10 @@ __device__ __forceinline__ uint2 spread16(uint32_t x) {
 __device__ __forceinline__ void sts64(uint32_t addr, uint2 v) {
     asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(addr), "r"(v.x), "r"(v.y) : "memory");
 }
+__device__ __forceinline__ void sts128(uint32_t addr, uint2 lo, uint2 hi) {
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(lo.x), "r"(lo.y), "r"(hi.x), "r"(hi.y)
+                 : "memory");
+}
 __device__ __forceinline__ uint32_t lds_b32(uint32_t addr) {
     uint32_t v;
     asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
@@ -276,8 +280,11 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
         }
     } else if (warp < 2 + NGEN) {
         const int gw = warp - 2;
-        const uint32_t m8 = (uint32_t)lane >> 2, sl = (uint32_t)lane & 3u;
-        const uint32_t lane_off = (sl >> 1) * 128 + m8 * 16 + (sl & 1u) * 8;  // canonical K-major position
+        // a lane writes one 16-byte K half (2 slices) of one operand row: rows
+        // m8 of 8-row group 2u+gsub, K half kh -- each quarter warp stores 128
+        // contiguous bytes
+        const uint32_t m8 = (uint32_t)lane & 7u, kh = ((uint32_t)lane >> 3) & 1u, gsub = (uint32_t)lane >> 4;
+        const uint32_t lane_off = kh * 128 + m8 * 16;
         uint32_t g = g0;
         for (uint32_t k = 0; k < KS; ++k, ++g) {
             const uint32_t si = g % kInStages, so = g % kOpStages;
@@ -287,19 +294,28 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
                 break;
             }
             const uint32_t a = op0 + so * kOpStageBytes, ins = in0 + si * kInStageBytes;
-            const bool live = k * kKSlices + sl < T.sn;  // slices past the range were not loaded
-            // 32 groups of 8 A rows (row m = 16*rl + i of half t is bits i..i+15
-            // of T for recovery row r0 + 8t + rl), then 30 groups of 8 B rows
-            for (uint32_t it = (uint32_t)gw; it < 62; it += NGEN) {
-                if (it < 32) {
-                    const uint32_t t = it >> 4, grp = it & 15u, m = grp * 8 + m8;
-                    const uint32_t Tc = live ? lds_b32(ins + (sl * kTileRows + 8 * t + (m >> 4)) * 4) : 0u;
-                    sts64(a + t * kATileBytes + grp * 256 + lane_off, spread16((Tc >> (m & 15u)) & 0xFFFFu));
-                } else {
-                    const uint32_t grp = it - 32, n = grp * 8 + m8;
-                    const uint32_t x =
-                        (live && n < T.syms) ? lds_u16(ins + kInCoefBytes + sl * kSrcSliceBytes + n * 2) : 0u;
-                    sts64(a + 2 * kATileBytes + grp * 256 + lane_off, spread16(x));
+            // slices past the range were not loaded: their K positions get 0
+            const bool live0 = k * kKSlices + 2 * kh < T.sn, live1 = k * kKSlices + 2 * kh + 1 < T.sn;
+            // units 0..15: A, 8-row groups 2u, 2u+1 of the 32 (row m = 16*rl + i
+            // of half t is bits i..i+15 of T for recovery row r0 + 8t + rl);
+            // units 16..30: B, 8-row groups of the 240 symbols
+#pragma unroll
+            for (int j = 0; j < (31 + NGEN - 1) / NGEN; ++j) {
+                const uint32_t u = (uint32_t)gw + (uint32_t)j * NGEN;
+                if (u < 16) {
+                    const uint32_t G = 2 * u + gsub, t = G >> 4, grp = G & 15u, m = grp * 8 + m8;
+                    const uint32_t tq = ins + (2 * kh * kTileRows + 8 * t + (m >> 4)) * 4;
+                    const uint32_t T0 = live0 ? lds_b32(tq) : 0u, T1 = live1 ? lds_b32(tq + kTileRows * 4) : 0u;
+                    const uint32_t i = m & 15u;
+                    const uint2 v0 = spread16((T0 >> i) & 0xFFFFu), v1 = spread16((T1 >> i) & 0xFFFFu);
+                    sts128(a + t * kATileBytes + grp * 256 + lane_off, v0, v1);
+                } else if (u < 31) {
+                    const uint32_t grp = 2 * (u - 16) + gsub, n = grp * 8 + m8;
+                    const uint32_t sq = ins + kInCoefBytes + 2 * kh * kSrcSliceBytes + n * 2;
+                    const bool nv = n < T.syms;
+                    const uint32_t x0 = (live0 && nv) ? lds_u16(sq) : 0u;
+                    const uint32_t x1 = (live1 && nv) ? lds_u16(sq + kSrcSliceBytes) : 0u;
+                    sts128(a + 2 * kATileBytes + grp * 256 + lane_off, spread16(x0), spread16(x1));
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
