@@ -139,11 +139,18 @@ def test_device_job_plan_covers_every_slice_of_every_tile_once(p2g, slice_, S, R
     assert again == items and z2 == zero_from and b2 == bands
 
 
-def test_device_job_plan_splits_the_538mb_job(p2g):
+def test_device_job_plan_splits_the_538mb_job(p2g, monkeypatch):
+    """On the lookup kernel the 538 MB job's last bands are cut into slice
+    ranges (its 1.5 ms items would otherwise end in lockstep); the tensor-core
+    plan's 14,209 short items (1,093 symbol tiles x 13 row tiles) need no cut."""
+    monkeypatch.setenv("P2G_ENCODE_VARIANT", "lut")
     items, zero_from, bands = p2g.plan_device_job(524288, 1027, 200)
     acc = [it for it in items if it["accumulate"]]
     assert bands > 1 and acc and zero_from < 262144
     assert not any(it["accumulate"] for it in p2g.plan_device_job(524288, 1027, 200, with_chains=False)[0])
+    monkeypatch.setenv("P2G_ENCODE_VARIANT", "tensor")
+    items, zero_from, bands = p2g.plan_device_job(524288, 1027, 200)
+    assert len(items) == 1093 * 13 and all(it["fold"] == 0 for it in items) and bands > 1
 
 
 def test_staged_groups_cover_jobs_in_order(p2g):
