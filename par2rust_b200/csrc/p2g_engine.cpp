@@ -347,7 +347,8 @@ static p2g_status poll_progress(Context& c, DeviceJob& j, const SingleJobPlan& p
                                 cudaStream_t st) {
     uint64_t first_enc = 0, n_enc = 0;
     for (size_t i = 0; i < pl.items.size(); ++i)
-        if ((pl.items[i].kind_rg & kItemKindMask) == kItemEncode) {
+        if ((pl.items[i].kind_rg & kItemKindMask) == kItemEncode ||
+            (pl.items[i].kind_rg & kItemKindMask) == kItemEncodeMma) {
             if (!n_enc) first_enc = i;
             ++n_enc;
         }
