@@ -23,8 +23,8 @@ namespace mma {
 constexpr uint32_t kN = 240;        // symbols per tile (MMA N)
 constexpr uint32_t kTileRows = 16;  // recovery rows per tile (two M = 128 MMAs)
 constexpr uint32_t kKSlices = 4;    // input slices per K-step (K = 64 e2m1 values)
-constexpr int kOpStages = 8;
-constexpr int kInStages = 8;
+constexpr int kOpStages = 6;
+constexpr int kInStages = 32;  // deep: each stage waits on 8 small copies from L2 or DRAM
 constexpr uint32_t kAccCol1 = 256;                // TMEM column of the second accumulator
 constexpr uint32_t kSfaCol = 496, kSfbCol = 504;  // scale factors (all 1.0)
 constexpr uint32_t kATileBytes = 4096;            // 128 rows x 32 B
