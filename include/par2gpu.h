@@ -394,7 +394,8 @@ typedef struct p2g_batch_shape {
 #define P2G_BATCH_DERIVE_BASIS 4u       /* no basis scratch: encode items derive their bases */
 #define P2G_BATCH_TENSOR 8u             /* every job's encode on the tensor cores (tcgen05) */
 #define P2G_BATCH_LUT 16u               /* every job's encode on the shared-memory lookup kernel
-                                           (neither flag: chosen per job shape) */
+                                           (neither flag: one kernel for the whole batch, the
+                                           cheaper for its jobs by the cost model) */
 
 /* Validate the jobs (the checks of p2g_run_device_job), plan the items and
  * allocate the batch's device scratch.  The job buffers must stay valid

@@ -612,7 +612,7 @@ BATCH_NO_GRAPH = 1
 BATCH_NO_AUTOTUNE = 2
 BATCH_DERIVE_BASIS = 4
 BATCH_TENSOR = 8  # every job's encode on the tensor cores
-BATCH_LUT = 16  # every job's encode on the lookup kernel (neither: by job shape)
+BATCH_LUT = 16  # every job's encode on the lookup kernel (neither: one kernel per batch, by cost)
 
 
 @dataclass

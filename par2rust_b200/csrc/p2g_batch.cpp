@@ -374,20 +374,24 @@ Plan plan_tiles(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
 double est_md5_ms(uint64_t bytes) { return md5_ms(bytes); }
 // A tensor-core item: one K-step (4 slices) of operand building and two
 // MMAs, plus the pipeline fill and the epilogue.
-constexpr double kMmaStepMs = 1.6e-4, kMmaFixedMs = 0.004;
+constexpr double kMmaStepMs = 6.9e-4, kMmaFixedMs = 0.004;  // measured: 16.97 ms for the 538 MB / R 200 encode
 double est_mma_item_ms(uint32_t slices) { return (slices + 3) / 4 * kMmaStepMs + kMmaFixedMs + kItemMs; }
 // Whether a job's encode runs on the tensor cores: by the cost of its items
 // on a full GPU (the lookup kernel folds a short last row group; the tensor
 // tiles are 16 rows high and 240 symbols wide).
-bool prefer_mma(uint64_t slice, uint32_t S, uint32_t R) {
-    if (!R || !S) return false;
+// CTA-milliseconds of a job's encode items on either kernel.
+double encode_cost_ms(uint64_t slice, uint32_t S, uint32_t R, bool mma) {
+    if (!R || !S) return 0;
     const uint32_t Np = (uint32_t)(round_up(slice, 16) / 2);
+    if (mma)
+        return (double)((Np + kMmaTileSymbols - 1) / kMmaTileSymbols) * ((R + kMmaTileRows - 1) / kMmaTileRows) *
+               est_mma_item_ms(S);
     const uint32_t RG = (R + kRowsPerGroup - 1) / kRowsPerGroup, F = tail_fold(R);
-    const double lut = (double)((Np + kEncTileSymbols - 1) / kEncTileSymbols) * (RG - 1 + 1.0 / F) *
-                       est_encode_item_ms(S, std::min<uint32_t>(Np, kEncTileSymbols)) * (F > 1 ? kFoldCost : 1.0);
-    const double mma = (double)((Np + kMmaTileSymbols - 1) / kMmaTileSymbols) *
-                       ((R + kMmaTileRows - 1) / kMmaTileRows) * est_mma_item_ms(S);
-    return mma < lut;
+    return (double)((Np + kEncTileSymbols - 1) / kEncTileSymbols) * (RG - 1 + (F > 1 ? kFoldCost / F : 1.0)) *
+           est_encode_item_ms(S, std::min<uint32_t>(Np, kEncTileSymbols));
+}
+bool prefer_mma(uint64_t slice, uint32_t S, uint32_t R) {
+    return R && S && encode_cost_ms(slice, S, R, true) < encode_cost_ms(slice, S, R, false);
 }
 double est_encode_item_ms(uint32_t slices, uint32_t syms) {
     return (double)slices * (round_up(syms, 8) + kBuildCost) / kEncRate + kItemMs;
@@ -659,16 +663,28 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
                 shape[i].file_bytes = std::max<uint64_t>(shape[i].file_bytes, jb.file_lengths[f]);
         }
     }
-    // encode kernel per job: forced by the flags (or P2G_ENCODE_VARIANT), else by the cost model
+    // One encode kernel for the whole launch: forced by the flags (or
+    // P2G_ENCODE_VARIANT), else the one the cost model prefers for the
+    // batch's total encode work.  Lookup and tensor-core items are not mixed
+    // in one launch: batches that mixed them gave wrong recovery bytes for a
+    // few tensor-core tiles (each kind alone is bit-exact).
     const char* ev = getenv("P2G_ENCODE_VARIANT");
-    for (uint32_t i = 0; i < n; ++i) {
-        bool m = prefer_mma(shape[i].slice, shape[i].S, shape[i].R);
-        if (ev && !strcmp(ev, "tensor")) m = true;
-        if (ev && !strcmp(ev, "lut")) m = false;
-        if (flags & P2G_BATCH_TENSOR) m = true;
-        if (flags & P2G_BATCH_LUT) m = false;
-        shape[i].mma = m && shape[i].R;
+    bool use_mma;
+    if (flags & P2G_BATCH_TENSOR) {
+        use_mma = true;
+    } else if (flags & P2G_BATCH_LUT) {
+        use_mma = false;
+    } else if (ev && (!strcmp(ev, "tensor") || !strcmp(ev, "lut"))) {
+        use_mma = !strcmp(ev, "tensor");
+    } else {
+        double lut = 0, mma = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            lut += encode_cost_ms(shape[i].slice, shape[i].S, shape[i].R, false);
+            mma += encode_cost_ms(shape[i].slice, shape[i].S, shape[i].R, true);
+        }
+        use_mma = mma < lut;
     }
+    for (uint32_t i = 0; i < n; ++i) shape[i].mma = use_mma && shape[i].R;
     P2G_TRY(ensure_device_ready());
     p2g_batch* b = new p2g_batch();
     cudaGetDevice(&b->device);

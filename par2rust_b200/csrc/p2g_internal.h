@@ -245,7 +245,9 @@ cudaError_t launch_seeded_fill(uint8_t* base, const uint64_t* spans, const uint6
 double est_md5_ms(uint64_t bytes);
 double est_encode_item_ms(uint32_t slices, uint32_t syms);
 double est_mma_item_ms(uint32_t slices);
-// Whether a job of this shape encodes faster on the tensor cores (cost model).
+// CTA-milliseconds of a job's encode on the lookup or the tensor-core kernel
+// (cost model), and whether the tensor cores are the cheaper.
+double encode_cost_ms(uint64_t slice, uint32_t S, uint32_t R, bool mma);
 bool prefer_mma(uint64_t slice, uint32_t S, uint32_t R);
 double est_scan_item_ms(uint64_t slice, uint32_t count);
 double est_crc_item_ms(uint64_t slice, uint32_t count);
