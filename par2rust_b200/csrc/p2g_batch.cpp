@@ -785,12 +785,6 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         d.first_exp = 0;
         d.vec = jb.slice_size % 16 == 0 ? 1u : 0u;
         d.basis = load_basis && d.R && !shape[i].mma ? reinterpret_cast<uint16_t*>(A + o_basis[i]) : nullptr;
-        if (shape[i].mma) {
-            d.mma = 1;
-            d.Rpad = (d.R + kMmaTileRows - 1) / kMmaTileRows * kMmaTileRows;
-            d.tcoef = reinterpret_cast<uint32_t*>(A + o_tcoef[i]);
-            b->max_tcoef_words = std::max<uint64_t>(b->max_tcoef_words, (uint64_t)d.S * d.Rpad);
-        }
         if (d.R && jb.slice_size % 16) {
             d.esrc = A + o_real[i];
             d.estride = round_up(jb.slice_size, 16);
@@ -798,6 +792,14 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         } else {
             d.esrc = jb.src;
             d.estride = jb.slice_size;
+        }
+        if (shape[i].mma) {
+            d.mma = 1;
+            d.Rpad = (d.R + kMmaTileRows - 1) / kMmaTileRows * kMmaTileRows;
+            d.Spad = mma_tcoef_spad(d.S);
+            d.tcoef = reinterpret_cast<uint32_t*>(A + o_tcoef[i]);
+            b->max_tcoef_words = std::max<uint64_t>(b->max_tcoef_words, mma_coef_words(d.S, d.R));
+            if (e == cudaSuccess) e = make_src_map(&d.src_map, d.esrc, d.estride, d.S, (uint32_t)(d.estride / 2));
         }
         if (d.basis) b->max_basis_words = std::max<uint64_t>(b->max_basis_words, (uint64_t)d.S * d.RG * 512);
         uint64_t first = 0;

@@ -467,6 +467,8 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
         d.mma = 1;
         d.tcoef = c.tcoef.as<uint32_t>();
         d.Rpad = (j.R + kMmaTileRows - 1) / kMmaTileRows * kMmaTileRows;
+        d.Spad = mma_tcoef_spad(j.S);
+        P2G_CU(make_src_map(&d.src_map, esrc, estride, j.S, (uint32_t)(estride / 2)));
     }
     memcpy(H + o_items, pl.items.data(), sizeof(BatchItem) * pl.items.size());
     uint8_t* hb = H + o_ctl;  // band counts, file tables and names after the descriptor and items
@@ -502,7 +504,7 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
                                  np_bytes - 2ull * pl.zero_from_sym, j.R, st));
     if (d.basis) P2G_CU(launch_basis(c.basis.as<uint16_t>(), j.S, RG, j.R, j.first_exp, st));
     if (mma)
-        P2G_CU(launch_tc_coef_batch(reinterpret_cast<const BatchJob*>(D + o_desc), 1, (uint64_t)j.S * d.Rpad, st));
+        P2G_CU(launch_tc_coef_batch(reinterpret_cast<const BatchJob*>(D + o_desc), 1, mma_coef_words(j.S, j.R), st));
     if (esrc != j.d_src) P2G_CU(launch_realign(j.d_src, j.slice, c.src_al.as<uint8_t>(), estride, j.S, j.slice, st));
     P2G_CU(launch_batch(reinterpret_cast<const BatchJob*>(D + o_desc), reinterpret_cast<const BatchItem*>(D + o_items),
                         (uint32_t)pl.items.size(), reinterpret_cast<uint32_t*>(D + o_ctl), err,

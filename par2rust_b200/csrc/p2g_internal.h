@@ -1,6 +1,7 @@
 // p2g_internal.h -- launch wrappers shared between the kernel file and the
 // host pipeline of libpar2gpu.so.  Not part of the public ABI.
 #pragma once
+#include <cuda.h>  // CUtensorMap and its enums (the encode function is looked up at run time)
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -127,8 +128,16 @@ cudaError_t gf_device_tables(const uint16_t** antilog, const uint16_t** logbase)
 // `tcoef` (mma_coef_bytes(S, R) of scratch) with the coefficients' trace
 // strings, then the persistent tcgen05 kernel accumulates 16-row x
 // 240-symbol tiles over all S slices.  src rows are read in whole 16-byte
-// units, as by launch_encode.
+// units, as by launch_encode, through a 2-D tensor map (16-byte aligned src
+// and src_stride).
 size_t mma_coef_bytes(uint32_t S, uint32_t R);
+uint64_t mma_coef_words(uint32_t S, uint32_t R);
+// Input slices per 16-row tile in that scratch: S rounded up to 16, plus 16
+// (room for a whole 16-slice copy from any first slice).
+constexpr uint32_t mma_tcoef_spad(uint32_t S) { return (S + 15) / 16 * 16 + 16; }
+// The source as a 2-D tensor map of Np u16 symbols x S slices for the
+// tensor-core tiles (cuTensorMapEncodeTiled, found through the runtime).
+cudaError_t make_src_map(CUtensorMap* map, const void* src, uint64_t stride, uint32_t S, uint32_t Np);
 cudaError_t launch_encode_mma(const uint8_t* src, uint64_t src_stride, uint32_t S, uint64_t slice_size, uint32_t R,
                               uint32_t first_exp, uint32_t* tcoef, uint8_t* rec, uint64_t rec_stride, int* err,
                               cudaStream_t st);
@@ -208,8 +217,9 @@ struct BatchJob {
     uint32_t ts, first_exp;  // ts: tile width (sub-tile width of folded items)
     uint32_t vec;            // slices and file starts of src are 16-byte aligned
     uint32_t mma;            // encode items run on the tensor cores (kItemEncodeMma)
-    uint32_t* tcoef;         // mma: trace strings of the coefficients, [s][Rpad]
-    uint32_t Rpad, pad2;     // mma: R rounded up to whole 16-row tiles
+    uint32_t* tcoef;         // mma: trace strings of the coefficients, per 16-row tile (mma_coef_words)
+    uint32_t Rpad, Spad;     // mma: R rounded up to whole 16-row tiles; tcoef's slices per tile
+    CUtensorMap src_map;     // mma: esrc as a 2-D tensor (make_src_map); 64-byte aligned
 };
 
 // Items of one job run alone through the persistent kernel (the plain

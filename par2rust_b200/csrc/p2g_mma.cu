@@ -63,36 +63,50 @@ constexpr uint32_t kOffMisc = kOffBars + kBarBytes;
 constexpr uint32_t kSmemBytes = kOffMisc + 16;
 static_assert(kSmemBytes > 116 * 1024, "one CTA per SM: TMEM is allocated whole");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
+static_assert(mma_tcoef_spad(1027) == tcoef_spad(1027) && mma_tcoef_spad(32) == tcoef_spad(32),
+              "host and device agree on the trace-string layout");
 
 }  // namespace
 
-// Coefficient trace strings: tcoef[s * Rpad + r] = T_c(r,s) for c(r,s) =
-// base_s ^ (first_exp + r) = 2^(logbase_s * (first_exp + r) mod 65535)
-// (RsEncoder::coefficient, src/reedsolomon.rs:56-60; gf_pow src/galois.rs:
-// 74-87); rows r >= R get 0.
-__global__ void tc_coef_kernel(uint32_t* __restrict__ tcoef, const uint16_t* __restrict__ antilog,
-                               const uint16_t* __restrict__ logbase, uint32_t S, uint32_t R, uint32_t Rpad,
-                               uint32_t first_exp) {
-    const uint64_t total = (uint64_t)S * Rpad;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t s = (uint32_t)(i / Rpad), r = (uint32_t)(i % Rpad);
-        uint32_t T = 0;
-        if (r < R) {
-            const uint32_t e = (first_exp + r) % kFieldLimit;
-            uint32_t k = (uint32_t)logbase[s] * e;  // < 2^32
-            k = (k & 0xFFFFu) + (k >> 16);
-            k = (k & 0xFFFFu) + (k >> 16);
-            if (k >= kFieldLimit) k -= kFieldLimit;
-            const uint32_t c = antilog[k];
-            T = d_trace_lo[c & 0xFFu] ^ d_trace_hi[c >> 8];
-        }
-        tcoef[i] = T;
+// Trace string of the coefficient c(r,s) = base_s ^ (first_exp + r) =
+// 2^(logbase_s * (first_exp + r) mod 65535) (RsEncoder::coefficient,
+// src/reedsolomon.rs:56-60; gf_pow src/galois.rs:74-87).
+__device__ __forceinline__ uint32_t coef_trace(uint32_t s, uint32_t r, uint32_t first_exp,
+                                               const uint16_t* __restrict__ antilog,
+                                               const uint16_t* __restrict__ logbase) {
+    const uint32_t e = (first_exp + r) % kFieldLimit;
+    uint32_t k = (uint32_t)logbase[s] * e;  // < 2^32
+    k = (k & 0xFFFFu) + (k >> 16);
+    k = (k & 0xFFFFu) + (k >> 16);
+    if (k >= kFieldLimit) k -= kFieldLimit;
+    const uint32_t c = antilog[k];
+    return d_trace_lo[c & 0xFFu] ^ d_trace_hi[c >> 8];
+}
+
+// All trace strings of one job in the per-tile layout of p2g_mma_tile.cuh:
+// tcoef[(rt * Spad + s) * 16 + i] for row 16 rt + i, 0 past R or S.
+__device__ __forceinline__ void fill_tcoef(uint32_t* __restrict__ tcoef, uint32_t S, uint32_t R, uint32_t first_exp,
+                                           const uint16_t* __restrict__ antilog, const uint16_t* __restrict__ logbase,
+                                           uint64_t i0, uint64_t step) {
+    const uint32_t Spad = tcoef_spad(S), n_row = (R + kTileRows - 1) / kTileRows;
+    const uint64_t total = (uint64_t)n_row * Spad * kTileRows;
+    for (uint64_t i = i0; i < total; i += step) {
+        const uint32_t ri = (uint32_t)(i % kTileRows);
+        const uint64_t q = i / kTileRows;
+        const uint32_t s = (uint32_t)(q % Spad), r = (uint32_t)(q / Spad) * kTileRows + ri;
+        tcoef[i] = (r < R && s < S) ? coef_trace(s, r, first_exp, antilog, logbase) : 0u;
     }
 }
 
+__global__ void tc_coef_kernel(uint32_t* __restrict__ tcoef, const uint16_t* __restrict__ antilog,
+                               const uint16_t* __restrict__ logbase, uint32_t S, uint32_t R, uint32_t first_exp) {
+    fill_tcoef(tcoef, S, R, first_exp, antilog, logbase, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
+               (uint64_t)gridDim.x * blockDim.x);
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
-    encode_mma_kernel(const uint8_t* __restrict__ src, uint64_t src_stride, uint32_t S, uint32_t Np,
-                      const uint32_t* __restrict__ tcoef, uint32_t Rpad, uint32_t R, uint8_t* __restrict__ rec,
+    encode_mma_kernel(const __grid_constant__ CUtensorMap src_map, uint32_t S, uint32_t Np,
+                      const uint32_t* __restrict__ tcoef, uint32_t R, uint8_t* __restrict__ rec,
                       uint64_t rec_stride, uint32_t n_row_tiles, uint32_t n_tiles, int* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -103,7 +117,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     P.bars = smem_addr(smem + kOffBars);
     P.ginv = ginv;
     P.abort_flag = misc + 1;
-    P.g = P.tcount = P.drains = 0;
+    P.g = P.gi = P.tcount = P.drains = 0;
     if (tid == 0) {
         init_bars(P.bars, kGenWarps);
         misc[1] = 0;
@@ -123,14 +137,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     bool ok = true;
     for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
         Tile T;
-        T.src = src;
-        T.src_stride = src_stride;
+        T.src_map = &src_map;
         T.tcoef = tcoef;
         T.rec = rec;
         T.rec_stride = rec_stride;
         T.s0 = 0;
         T.sn = S;
-        T.Rpad = Rpad;
+        T.Spad = tcoef_spad(S);
         T.R = R;
         T.r0 = (tile % n_row_tiles) * kTileRows;
         T.n0 = (tile / n_row_tiles) * kN;
@@ -252,21 +265,8 @@ __global__ void tc_coef_batch_kernel(const BatchJob* __restrict__ jobs, const ui
                                      const uint16_t* __restrict__ logbase) {
     const BatchJob& J = jobs[blockIdx.y];
     if (!J.mma || !J.R || !J.tcoef) return;
-    const uint64_t total = (uint64_t)J.S * J.Rpad;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t s = (uint32_t)(i / J.Rpad), r = (uint32_t)(i % J.Rpad);
-        uint32_t T = 0;
-        if (r < J.R) {
-            const uint32_t e = (J.first_exp + r) % kFieldLimit;
-            uint32_t k = (uint32_t)logbase[s] * e;
-            k = (k & 0xFFFFu) + (k >> 16);
-            k = (k & 0xFFFFu) + (k >> 16);
-            if (k >= kFieldLimit) k -= kFieldLimit;
-            const uint32_t c = antilog[k];
-            T = d_trace_lo[c & 0xFFu] ^ d_trace_hi[c >> 8];
-        }
-        J.tcoef[i] = T;
-    }
+    fill_tcoef(J.tcoef, J.S, J.R, J.first_exp, antilog, logbase, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
+               (uint64_t)gridDim.x * blockDim.x);
 }
 
 cudaError_t launch_tc_coef_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_words, cudaStream_t st) {
@@ -283,9 +283,38 @@ cudaError_t launch_tc_coef_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t
     return cudaGetLastError();
 }
 
-size_t mma_coef_bytes(uint32_t S, uint32_t R) {
-    const uint64_t Rpad = (uint64_t)(R + kTileRows - 1) / kTileRows * kTileRows;
-    return (size_t)S * Rpad * sizeof(uint32_t);
+size_t mma_coef_bytes(uint32_t S, uint32_t R) { return mma_coef_words(S, R) * sizeof(uint32_t); }
+uint64_t mma_coef_words(uint32_t S, uint32_t R) {
+    return (uint64_t)((R + kTileRows - 1) / kTileRows) * tcoef_spad(S) * kTileRows;
+}
+
+// The source as a 2-D tensor of u16 symbols: Np symbols per input slice, S
+// slices `stride` bytes apart (16-byte aligned base and stride), read in
+// boxes of 240 symbols x 16 slices, zeros past either extent.
+cudaError_t make_src_map(CUtensorMap* map, const void* src, uint64_t stride, uint32_t S, uint32_t Np) {
+    using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                     const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                     CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static EncodeTiled encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<EncodeTiled>(fn);
+    });
+    if (!encode) return cudaErrorNotSupported;
+    if ((uintptr_t)src % 16 || stride % 16 || !S || !Np) return cudaErrorInvalidValue;
+    const cuuint64_t dims[2] = {Np, S};
+    const cuuint64_t strides[1] = {stride};
+    const cuuint32_t box[2] = {kN, kInSlices};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(src), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 cudaError_t launch_encode_mma(const uint8_t* src, uint64_t src_stride, uint32_t S, uint64_t slice_size, uint32_t R,
@@ -297,17 +326,19 @@ cudaError_t launch_encode_mma(const uint8_t* src, uint64_t src_stride, uint32_t 
     const uint16_t *antilog = nullptr, *logbase = nullptr;
     if ((e = gf_device_tables(&antilog, &logbase)) != cudaSuccess) return e;
     const uint32_t Np = (uint32_t)(((slice_size + 15) & ~15ull) / 2);
-    const uint32_t n_row = (R + kTileRows - 1) / kTileRows, Rpad = n_row * kTileRows;
+    CUtensorMap map;
+    if ((e = make_src_map(&map, src, src_stride, S, Np)) != cudaSuccess) return e;
+    const uint32_t n_row = (R + kTileRows - 1) / kTileRows;
     const uint32_t n_sym = (Np + kN - 1) / kN;
-    const uint64_t total = (uint64_t)S * Rpad;
+    const uint64_t total = mma_coef_words(S, R);
     const int sms = device_sm_count();
     const unsigned cb = (unsigned)std::min<uint64_t>((total + 255) / 256, (uint64_t)sms * 8);
-    tc_coef_kernel<<<cb, 256, 0, st>>>(tcoef, antilog, logbase, S, R, Rpad, first_exp);
+    tc_coef_kernel<<<cb, 256, 0, st>>>(tcoef, antilog, logbase, S, R, first_exp);
     add_launches(1);
     const uint64_t tiles = (uint64_t)n_sym * n_row;
     const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms);
-    encode_mma_kernel<<<grid, kThreads, kSmemBytes, st>>>(src, src_stride, S, Np, tcoef, Rpad, R, rec, rec_stride,
-                                                          n_row, (uint32_t)tiles, err);
+    encode_mma_kernel<<<grid, kThreads, kSmemBytes, st>>>(map, S, Np, tcoef, R, rec, rec_stride, n_row,
+                                                          (uint32_t)tiles, err);
     add_launches(1);
     return cudaGetLastError();
 }

@@ -7,13 +7,18 @@
 // shared-memory and TMEM layout of one CTA and the work of one 16-row x
 // 240-symbol tile over a range of input slices.
 //
-// Shared memory (from `ring`, 1024-aligned): kOpStages operand stages of 16
-// KiB (A rows of the two 8-row halves, 4 KiB each; B rows, 7,680 B), then
-// kInStages input stages of 2,304 B (the 16 rows' trace strings of 4 slices,
-// 256 B; then the tile's bytes of those 4 slices, 4 x 480 B).  Both operands
-// are K-major without swizzle: core matrices of 8 rows x 16 B, K halves
-// 128 B apart, 8-row groups 256 B apart.  TMEM: the two fp32 accumulators at
-// columns 0 and 256 (240 columns each), scale factors 1.0 at 496-511.
+// Shared memory (from `ring`, 1024-aligned): kOpStages operand stages of
+// two K-steps, 16 KiB each (A rows of the two 8-row halves, 4 KiB each; B
+// rows, 7,680 B), then kInStages input stages of 8,704 B, each covering
+// kInSteps K-steps (16 input slices): the 16 rows' trace strings of those
+// slices ([slice][row], 1 KiB, one bulk copy) and the tile's symbols of those
+// slices ([slice][240 symbols], 7,680 B, one 2-D tensor copy).  Two copies
+// per four K-steps: a copy costs the issuing thread more than a K-step of
+// MMAs, so small copies per slice would starve the tensor core.  Both
+// operands are K-major without swizzle: core matrices of 8 rows x 16 B, K
+// halves 128 B apart, 8-row groups 256 B apart.  TMEM: the two fp32
+// accumulators at columns 0 and 256 (240 columns each), scale factors 1.0 at
+// 496-511.
 #pragma once
 #include <stdint.h>
 
@@ -23,22 +28,33 @@ namespace mma {
 constexpr uint32_t kN = 240;        // symbols per tile (MMA N)
 constexpr uint32_t kTileRows = 16;  // recovery rows per tile (two M = 128 MMAs)
 constexpr uint32_t kKSlices = 4;    // input slices per K-step (K = 64 e2m1 values)
-constexpr int kOpStages = 6;
-constexpr int kInStages = 32;  // deep: each stage waits on 8 small copies from L2 or DRAM
+constexpr uint32_t kOpSteps = 2;    // K-steps per operand stage
+constexpr int kOpStages = 3;
+constexpr uint32_t kInSteps = 4;                   // K-steps per input stage
+constexpr uint32_t kInSlices = kInSteps * kKSlices;  // 16 input slices per input stage
+constexpr int kInStages = 8;
 constexpr uint32_t kAccCol1 = 256;                // TMEM column of the second accumulator
 constexpr uint32_t kSfaCol = 496, kSfbCol = 504;  // scale factors (all 1.0)
 constexpr uint32_t kATileBytes = 4096;            // 128 rows x 32 B
 constexpr uint32_t kBTileBytes = kN * 32;         // 240 rows x 32 B
-constexpr uint32_t kOpStageBytes = 2 * kATileBytes + 8192;
+constexpr uint32_t kOpStepBytes = 2 * kATileBytes + 8192;
+constexpr uint32_t kOpStageBytes = kOpSteps * kOpStepBytes;
 constexpr uint32_t kSrcSliceBytes = kN * 2;
-constexpr uint32_t kInCoefBytes = kKSlices * kTileRows * 4;
-constexpr uint32_t kInStageBytes = 2304;
+constexpr uint32_t kInCoefBytes = kInSlices * kTileRows * 4;               // 1 KiB
+constexpr uint32_t kInSrcBytes = kInSlices * kSrcSliceBytes;               // 7,680 B
+constexpr uint32_t kInStageBytes = kInCoefBytes + kInSrcBytes;             // 8,704 B
 constexpr uint32_t kRingBytes = kOpStages * kOpStageBytes + kInStages * kInStageBytes;
 constexpr uint32_t kGinvBytes = 1024;             // G^-1 tables: 256 lo then 256 hi u16
 constexpr uint32_t kNumBars = 2 * kInStages + 2 * kOpStages + 3;
 constexpr uint32_t kBarBytes = kNumBars * 8;
-static_assert(kBTileBytes <= kOpStageBytes - 2 * kATileBytes, "B tile fits its stage");
-static_assert(kInCoefBytes + kKSlices * kSrcSliceBytes <= kInStageBytes, "input stage");
+static_assert(kInStageBytes % 128 == 0 && kInCoefBytes % 128 == 0, "tensor copies land 128-byte aligned");
+
+// Trace strings in global memory, per 16-row tile: tcoef[(rt * Spad + s) *
+// 16 + i] = T_c for recovery row 16 rt + i and input slice s (0 past R or S).
+// Spad leaves room for a whole stage's copy from any first slice.
+__host__ __device__ constexpr uint32_t tcoef_spad(uint32_t S) { return (S + 15) / 16 * 16 + kInSlices; }
+static_assert(kBTileBytes <= kOpStepBytes - 2 * kATileBytes, "B tile fits its K-step");
+static_assert(kInSteps == 2 * kOpSteps, "an input stage feeds two operand stages");
 
 // Instruction descriptor of kind::mxf4 with UE8M0 block scales: A and B
 // e2m1 (format 1 at bits 7 and 10), K-major, N >> 3 at bit 17, scale format
@@ -84,6 +100,21 @@ __device__ __forceinline__ void tma_1d(uint32_t dst, const void* src, uint32_t b
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                  "l"(src), "r"(bytes), "r"(bar)
                  : "memory");
+}
+// 2-D tiled tensor copy: the box at (x, y) of the tensor map `map` (a generic
+// address of a CUtensorMap in kernel-parameter or global memory).  x times
+// the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_2d(uint32_t dst, const void* map, int32_t x, int32_t y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+// Before the first copy through a tensor map that ordinary stores wrote to
+// global memory (the batch job descriptors).
+__device__ __forceinline__ void tensormap_acquire(const void* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -191,25 +222,27 @@ __device__ __forceinline__ void sf_fill(uint32_t tmem, uint32_t q) {
 }
 
 // One tile: recovery rows [r0, r0+16) x symbols [n0, n0+syms) over input
-// slices [s0, s0+sn).  Slice s of the source is at src + s*src_stride; its
-// trace strings at tcoef + s*Rpad (rows past R hold 0).  accumulate: XOR the
-// tile into the rows (the caller zeroed them) instead of storing it.
+// slices [s0, s0+sn).  src_map: 2-D tensor map over the source (u16 symbols
+// x input slices, the slice stride a multiple of 16 bytes; symbols and slices
+// past its extent read 0); n0 is a multiple of 8.  The trace strings are at
+// tcoef in the per-tile layout above, Spad = tcoef_spad(S).  accumulate: XOR
+// the tile into the rows (the caller zeroed them) instead of storing it.
 struct Tile {
-    const uint8_t* src;
-    uint64_t src_stride;
+    const void* src_map;
     const uint32_t* tcoef;
     uint8_t* rec;
     uint64_t rec_stride;
-    uint32_t s0, sn, Rpad, R, r0, n0, syms, accumulate;
+    uint32_t s0, sn, Spad, R, r0, n0, syms, accumulate;
 };
 
-// Per-CTA pipeline state, the same in every thread: K-steps, tiles and
-// drains so far (ring positions and barrier parities follow from them).
+// Per-CTA pipeline state, the same in every thread: operand stages, input
+// stages, tiles and drains so far (ring positions and barrier
+// parities follow from them).
 struct Pipe {
     uint32_t ring, bars, tmem;
     const uint16_t* ginv;  // shared memory
     volatile uint32_t* abort_flag;
-    uint32_t g, tcount, drains;
+    uint32_t g, gi, tcount, drains;
 };
 
 // All threads of the CTA call this.  Warp 0 lane 0 streams the inputs, warp
@@ -223,32 +256,32 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const Bars B(P.bars);
     const uint32_t op0 = P.ring, in0 = P.ring + kOpStages * kOpStageBytes;
-    const uint32_t KS = (T.sn + kKSlices - 1) / kKSlices;
-    const uint32_t g0 = P.g, tc = P.tcount;
+    const uint32_t KS = (T.sn + kKSlices - 1) / kKSlices, NI = (KS + kInSteps - 1) / kInSteps;
+    const uint32_t NS = (KS + kOpSteps - 1) / kOpSteps;  // operand stages
+    const uint32_t g0 = P.g, gi0 = P.gi, tc = P.tcount, rt = T.r0 / kTileRows;
+    // a tensor copy's x offset must be 16-byte aligned (the same in every thread)
+    if (T.n0 & 7u) return false;
     bool ok = true;
     if (warp == 0) {
         if (lane == 0) {
-            const uint32_t bytes = 2 * T.syms;
-            uint32_t g = g0;
-            for (uint32_t k = 0; k < KS; ++k, ++g) {
-                const uint32_t st = g % kInStages;
-                if (!bar_wait(B.in_empty + 8 * st, ((g / kInStages) & 1u) ^ 1u, P.abort_flag)) {
+            uint32_t gi = gi0;
+            for (uint32_t k = 0; k < NI; ++k, ++gi) {
+                const uint32_t st = gi % kInStages;
+                if (!bar_wait(B.in_empty + 8 * st, ((gi / kInStages) & 1u) ^ 1u, P.abort_flag)) {
                     ok = false;
                     break;
                 }
-                const uint32_t sa = T.s0 + k * kKSlices, ns = min(kKSlices, T.s0 + T.sn - sa);
+                const uint32_t sa = T.s0 + k * kInSlices;
                 const uint32_t dst = in0 + st * kInStageBytes;
-                bar_expect_tx(B.in_full + 8 * st, ns * (bytes + kTileRows * 4));
-                for (uint32_t j = 0; j < ns; ++j) {
-                    tma_1d(dst + j * kTileRows * 4, T.tcoef + (size_t)(sa + j) * T.Rpad + T.r0, kTileRows * 4,
-                           B.in_full + 8 * st);
-                    tma_1d(dst + kInCoefBytes + j * kSrcSliceBytes,
-                           T.src + (size_t)(sa + j) * T.src_stride + (size_t)T.n0 * 2, bytes, B.in_full + 8 * st);
-                }
+                // slices past the tile's range (up to 15) are copied too and
+                // masked by the builders; past S the tensor map reads 0
+                bar_expect_tx(B.in_full + 8 * st, kInStageBytes);
+                tma_1d(dst, T.tcoef + ((size_t)rt * T.Spad + sa) * kTileRows, kInCoefBytes, B.in_full + 8 * st);
+                tma_2d(dst + kInCoefBytes, T.src_map, (int32_t)T.n0, (int32_t)sa, B.in_full + 8 * st);
             }
             if (!ok)  // copies issued but maybe not consumed land before the stages are reused
-                for (uint32_t b = g > g0 + kInStages ? g - kInStages : g0; b < g; ++b)
-                    bar_drain(B.in_full + 8 * (b % kInStages), (b / kInStages) & 1u);
+                for (uint32_t q = gi > gi0 + kInStages ? gi - kInStages : gi0; q < gi; ++q)
+                    bar_drain(B.in_full + 8 * (q % kInStages), (q / kInStages) & 1u);
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -256,19 +289,24 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
             if (!bar_wait(B.acc_empty, (tc & 1u) ^ 1u, P.abort_flag)) ok = false;
             tc_fence_after();
             uint32_t g = g0;
-            for (uint32_t k = 0; ok && k < KS; ++k, ++g) {
+            for (uint32_t p = 0; ok && p < NS; ++p, ++g) {
                 const uint32_t so = g % kOpStages;
                 if (!bar_wait(B.op_full + 8 * so, (g / kOpStages) & 1u, P.abort_flag)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t a = op0 + so * kOpStageBytes;
-                const uint64_t bdesc = smem_desc(a + 2 * kATileBytes, 128, 256);
-                mma_mxf4(P.tmem, smem_desc(a, 128, 256), bdesc, P.tmem + kSfaCol, P.tmem + kSfbCol, k > 0);
-                if (two)
-                    mma_mxf4(P.tmem + kAccCol1, smem_desc(a + kATileBytes, 128, 256), bdesc, P.tmem + kSfaCol,
-                             P.tmem + kSfbCol, k > 0);
+#pragma unroll
+                for (uint32_t ks = 0; ks < kOpSteps; ++ks) {
+                    const uint32_t k = p * kOpSteps + ks;
+                    if (k >= KS) break;
+                    const uint32_t a = op0 + so * kOpStageBytes + ks * kOpStepBytes;
+                    const uint64_t bdesc = smem_desc(a + 2 * kATileBytes, 128, 256);
+                    mma_mxf4(P.tmem, smem_desc(a, 128, 256), bdesc, P.tmem + kSfaCol, P.tmem + kSfbCol, k > 0);
+                    if (two)
+                        mma_mxf4(P.tmem + kAccCol1, smem_desc(a + kATileBytes, 128, 256), bdesc, P.tmem + kSfaCol,
+                                 P.tmem + kSfbCol, k > 0);
+                }
                 mma_commit(B.op_empty + 8 * so);
             }
             if (ok) {
@@ -280,49 +318,87 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
         }
     } else if (warp < 2 + NGEN) {
         const int gw = warp - 2;
-        // a lane writes one 16-byte K half (2 slices) of one operand row: rows
-        // m8 of 8-row group 2u+gsub, K half kh -- each quarter warp stores 128
-        // contiguous bytes
+        // A lane writes one 16-byte K half (2 slices) of one operand row:
+        // rows m8 of 8-row group 2v+gsub, K half kh -- each quarter warp
+        // stores 128 contiguous bytes.  Per operand stage the builders share
+        // 31 warp units per K-step (v 0..15: A, the 32 8-row groups of the
+        // two accumulators; v 16..30: B, the 30 8-row groups of the 240
+        // symbols), dealt round-robin over the warps.  Both kinds take the
+        // same steps: two 32-bit loads from the input stage (A: trace strings
+        // of slices 2kh, 2kh+1; B: the words holding symbol n of them), a
+        // shift and mask to 16 bits (A: bits i..i+15 of T for row bit i; B:
+        // the symbol's half), spread16, one 16-byte store.
         const uint32_t m8 = (uint32_t)lane & 7u, kh = ((uint32_t)lane >> 3) & 1u, gsub = (uint32_t)lane >> 4;
         const uint32_t lane_off = kh * 128 + m8 * 16;
+        constexpr int kUnits = 31 * (int)kOpSteps;
+        constexpr int kTasks = (kUnits + NGEN - 1) / NGEN;
+        // fixed for the tile, per task: input offsets (from the input stage)
+        // for the first and the second operand stage of the pair, operand
+        // offset (from the operand stage), shift | distance to the second
+        // slice << 8 | slice within the stage << 20, and the 2-bit-pair mask
+        // (0 for symbols past the tile).  Tasks past the units load from
+        // offset 0 and store nothing.
+        uint32_t t_in0[kTasks], t_in1[kTasks], t_op[kTasks], t_fl[kTasks], t_m[kTasks];
+#pragma unroll
+        for (int j = 0; j < kTasks; ++j) {
+            const uint32_t u = (uint32_t)gw + (uint32_t)j * NGEN;
+            const uint32_t ks = u / 31u, v = u % 31u;
+            const uint32_t sl = ks * kKSlices + 2 * kh;
+            if (u >= (uint32_t)kUnits) {
+                t_in0[j] = t_in1[j] = t_op[j] = t_fl[j] = t_m[j] = 0;
+            } else if (v < 16) {
+                const uint32_t G = 2 * v + gsub, t = G >> 4, grp = G & 15u, m = grp * 8 + m8;
+                t_in0[j] = ks * kKSlices * kTileRows * 4 + (2 * kh * kTileRows + 8 * t + (m >> 4)) * 4;
+                t_in1[j] = t_in0[j] + kOpSteps * kKSlices * kTileRows * 4;
+                t_op[j] = ks * kOpStepBytes + t * kATileBytes + grp * 256 + lane_off;
+                t_fl[j] = (m & 15u) | ((kTileRows * 4) << 8) | (sl << 20);
+                t_m[j] = 0x3333u;
+            } else {
+                const uint32_t grp = 2 * (v - 16) + gsub, n = grp * 8 + m8;
+                t_in0[j] = kInCoefBytes + ks * kKSlices * kSrcSliceBytes + 2 * kh * kSrcSliceBytes + ((n * 2) & ~3u);
+                t_in1[j] = t_in0[j] + kOpSteps * kKSlices * kSrcSliceBytes;
+                t_op[j] = ks * kOpStepBytes + 2 * kATileBytes + grp * 256 + lane_off;
+                t_fl[j] = ((n & 1u) * 16) | (kSrcSliceBytes << 8) | (sl << 20);
+                t_m[j] = n < T.syms ? 0x3333u : 0u;
+            }
+        }
         uint32_t g = g0;
-        for (uint32_t k = 0; k < KS; ++k, ++g) {
-            const uint32_t si = g % kInStages, so = g % kOpStages;
-            if (!bar_wait(B.in_full + 8 * si, (g / kInStages) & 1u, P.abort_flag) ||
+        for (uint32_t p = 0; p < NS; ++p, ++g) {
+            const uint32_t half = p & 1u, gi = gi0 + p / 2, si = gi % kInStages, so = g % kOpStages;
+            if ((half == 0 && !bar_wait(B.in_full + 8 * si, (gi / kInStages) & 1u, P.abort_flag)) ||
                 !bar_wait(B.op_empty + 8 * so, ((g / kOpStages) & 1u) ^ 1u, P.abort_flag)) {
                 ok = false;
                 break;
             }
-            const uint32_t a = op0 + so * kOpStageBytes, ins = in0 + si * kInStageBytes;
-            // slices past the range were not loaded: their K positions get 0
-            const bool live0 = k * kKSlices + 2 * kh < T.sn, live1 = k * kKSlices + 2 * kh + 1 < T.sn;
-            // units 0..15: A, 8-row groups 2u, 2u+1 of the 32 (row m = 16*rl + i
-            // of half t is bits i..i+15 of T for recovery row r0 + 8t + rl);
-            // units 16..30: B, 8-row groups of the 240 symbols
+            const uint32_t ins = in0 + si * kInStageBytes, ops = op0 + so * kOpStageBytes;
+            // slices of this operand stage: [first, first + 8); past sn the K positions get 0
+            const int32_t klim = (int32_t)T.sn - (int32_t)(p * kOpSteps * kKSlices);
+            const bool full = klim >= (int32_t)(kOpSteps * kKSlices);
 #pragma unroll
-            for (int j = 0; j < (31 + NGEN - 1) / NGEN; ++j) {
-                const uint32_t u = (uint32_t)gw + (uint32_t)j * NGEN;
-                if (u < 16) {
-                    const uint32_t G = 2 * u + gsub, t = G >> 4, grp = G & 15u, m = grp * 8 + m8;
-                    const uint32_t tq = ins + (2 * kh * kTileRows + 8 * t + (m >> 4)) * 4;
-                    const uint32_t T0 = live0 ? lds_b32(tq) : 0u, T1 = live1 ? lds_b32(tq + kTileRows * 4) : 0u;
-                    const uint32_t i = m & 15u;
-                    const uint2 v0 = spread16((T0 >> i) & 0xFFFFu), v1 = spread16((T1 >> i) & 0xFFFFu);
-                    sts128(a + t * kATileBytes + grp * 256 + lane_off, v0, v1);
-                } else if (u < 31) {
-                    const uint32_t grp = 2 * (u - 16) + gsub, n = grp * 8 + m8;
-                    const uint32_t sq = ins + kInCoefBytes + 2 * kh * kSrcSliceBytes + n * 2;
-                    const bool nv = n < T.syms;
-                    const uint32_t x0 = (live0 && nv) ? lds_u16(sq) : 0u;
-                    const uint32_t x1 = (live1 && nv) ? lds_u16(sq + kSrcSliceBytes) : 0u;
-                    sts128(a + 2 * kATileBytes + grp * 256 + lane_off, spread16(x0), spread16(x1));
+            for (int j = 0; j < kTasks; ++j) {
+                const uint32_t fl = t_fl[j];
+                const uint32_t a0 = ins + (half ? t_in1[j] : t_in0[j]), a1 = a0 + ((fl >> 8) & 0xFFFu);
+                const uint32_t x0 = lds_b32(a0), x1 = lds_b32(a1);
+                uint32_t m0 = t_m[j], m1 = t_m[j];
+                if (!full) {
+                    const int32_t sl = (int32_t)(fl >> 20);
+                    if (sl >= klim) m0 = 0;
+                    if (sl + 1 >= klim) m1 = 0;
                 }
+                const uint32_t sh = fl & 31u;
+                // spread16 of 16 bits y: pairs (4q, 4q+1) from y & 0x3333, pairs (4q+2, 4q+3) from (y >> 2) & 0x3333
+                constexpr uint32_t kPairs = 0x22200200u;
+                const uint2 w0 = make_uint2(__byte_perm(kPairs, 0u, (x0 >> sh) & m0),
+                                            __byte_perm(kPairs, 0u, (x0 >> (sh + 2)) & m0));
+                const uint2 w1 = make_uint2(__byte_perm(kPairs, 0u, (x1 >> sh) & m1),
+                                            __byte_perm(kPairs, 0u, (x1 >> (sh + 2)) & m1));
+                if ((uint32_t)gw + (uint32_t)j * NGEN < (uint32_t)kUnits) sts128(ops + t_op[j], w0, w1);
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) {
                 bar_arrive(B.op_full + 8 * so);
-                bar_arrive(B.in_empty + 8 * si);
+                if (half == 1 || p == NS - 1) bar_arrive(B.in_empty + 8 * si);
             }
         }
         if (ok && !bar_wait(B.acc_full, tc & 1u, P.abort_flag)) ok = false;
@@ -367,7 +443,8 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
         if (ok && lane == 0) bar_arrive(B.acc_empty);
     }
     const bool bad = __syncthreads_or(!ok) != 0;
-    P.g += KS;
+    P.g += NS;
+    P.gi += NI;
     P.tcount += 1;
     if (bad) P.drains += 1;
     return !bad;
