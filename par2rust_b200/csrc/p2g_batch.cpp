@@ -160,7 +160,8 @@ Plan build_items(const std::vector<PlanJob>& jobs) {
         for (uint32_t b = 0; b < nb; ++b) {
             const uint32_t t0 = b * bt, t1 = std::min(j.tiles, t0 + bt);
             const uint32_t C = b >= first_split ? j.split_chunks : 1;
-            const uint32_t cs = (j.S + C - 1) / C;
+            // tensor-core ranges start on whole 16-slice stages of the A image
+            const uint32_t cs = j.mma ? ((j.S + C - 1) / C + 15) / 16 * 16 : (j.S + C - 1) / C;
             auto push = [&](uint32_t rg, uint32_t fold, uint32_t n0, uint32_t syms) {
                 for (uint32_t s0 = 0; s0 < j.S; s0 += cs) {
                     const uint32_t sn = C > 1 ? std::min(cs, j.S - s0) : 0;
@@ -502,7 +503,7 @@ struct p2g_batch {
     uint64_t err_word = 0;      // index of the error word in d_ctl
     size_t ctl_bytes = 0;
     uint64_t max_basis_words = 0;
-    uint64_t max_tcoef_words = 0;  // tensor-core jobs: trace strings to fill per run
+    uint64_t max_aimg_bytes = 0;  // tensor-core jobs: largest A image to fill per run
     struct Realign {
         const uint8_t* src;
         uint8_t* dst;
@@ -523,9 +524,9 @@ p2g_status enqueue_run(p2g_batch* b, cudaStream_t st) {
     int* err = reinterpret_cast<int*>(b->d_ctl + b->err_word);
     P2G_CU(cudaMemsetAsync(b->d_ctl, 0, b->ctl_bytes, st));
     if (b->max_basis_words) P2G_CU(launch_basis_batch(b->d_jobs, b->n_jobs, b->max_basis_words, st));
-    if (b->max_tcoef_words) P2G_CU(launch_tc_coef_batch(b->d_jobs, b->n_jobs, b->max_tcoef_words, st));
+    if (b->max_aimg_bytes) P2G_CU(launch_a_image_batch(b->d_jobs, b->n_jobs, b->max_aimg_bytes, st));
     for (const auto& r : b->realigns) P2G_CU(launch_realign(r.src, r.slice, r.dst, r.estride, r.S, r.slice, st));
-    P2G_CU(launch_batch(b->d_jobs, b->d_items, b->n_items, b->d_ctl, err, b->ctas, st, b->max_tcoef_words != 0));
+    P2G_CU(launch_batch(b->d_jobs, b->d_items, b->n_items, b->d_ctl, err, b->ctas, st, b->max_aimg_bytes != 0));
     return P2G_OK;
 }
 
@@ -731,10 +732,10 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
     for (uint32_t i = 0; i < n; ++i)
         if (shape[i].R && !shape[i].mma) basis_total += basis_bytes(shape[i].S, shape[i].RG);
     const bool load_basis = !(flags & P2G_BATCH_DERIVE_BASIS) && basis_total <= basis_budget();
-    std::vector<size_t> o_scratch(n), o_basis(n, 0), o_real(n, 0), o_tcoef(n, 0);
+    std::vector<size_t> o_scratch(n), o_basis(n, 0), o_real(n, 0), o_aimg(n, 0);
     for (uint32_t i = 0; i < n; ++i) {
         o_scratch[i] = take(32ull * shape[i].n + 12);
-        if (shape[i].mma) o_tcoef[i] = take(mma_coef_bytes(shape[i].S, shape[i].R));
+        if (shape[i].mma) o_aimg[i] = take(mma_aimg_bytes(shape[i].S, shape[i].R));
         if (load_basis && shape[i].R && !shape[i].mma) o_basis[i] = take(basis_bytes(shape[i].S, shape[i].RG));
         if (shape[i].R && jobs[i].slice_size % 16) o_real[i] = take(round_up(jobs[i].slice_size, 16) * shape[i].S);
     }
@@ -796,9 +797,9 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         if (shape[i].mma) {
             d.mma = 1;
             d.Rpad = (d.R + kMmaTileRows - 1) / kMmaTileRows * kMmaTileRows;
-            d.Spad = mma_tcoef_spad(d.S);
-            d.tcoef = reinterpret_cast<uint32_t*>(A + o_tcoef[i]);
-            b->max_tcoef_words = std::max<uint64_t>(b->max_tcoef_words, mma_coef_words(d.S, d.R));
+            d.ksteps = mma_image_steps(d.S);
+            d.aimg = A + o_aimg[i];
+            b->max_aimg_bytes = std::max<uint64_t>(b->max_aimg_bytes, mma_aimg_bytes(d.S, d.R));
             if (e == cudaSuccess) e = make_src_map(&d.src_map, d.esrc, d.estride, d.S, (uint32_t)(d.estride / 2));
         }
         if (d.basis) b->max_basis_words = std::max<uint64_t>(b->max_basis_words, (uint64_t)d.S * d.RG * 512);
@@ -828,7 +829,7 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
         release(b);
         return cuda_fail(e, "batch tables upload");
     }
-    b->kernels_per_run = 1 + (b->max_basis_words ? 1 : 0) + (b->max_tcoef_words ? 1 : 0) + (uint32_t)b->realigns.size();
+    b->kernels_per_run = 1 + (b->max_basis_words ? 1 : 0) + (b->max_aimg_bytes ? 1 : 0) + (uint32_t)b->realigns.size();
 
     // ---- capture the run into a CUDA graph ----
     if (!(flags & P2G_BATCH_NO_GRAPH)) {

@@ -90,7 +90,7 @@ struct Context {
     cudaStream_t st[kStreams] = {};
     cudaEvent_t ev_fork = nullptr, ev_h16k = nullptr, ev_join[kStreams] = {}, ev_band[kBandEvents] = {};
     DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out, md5_state;
-    DevBuf tcoef;      // coefficient trace strings of the tensor-core encode
+    DevBuf aimg;       // A operand image of the tensor-core encode
     DevBuf persist;    // single-job persistent run: descriptor, items, chain state, tables
     PinBuf h_spans, h_h16k, h_err, h_stage, h_persist;
     PinBuf h_rec;   // host copy of the recovery rows (create calls)
@@ -425,7 +425,7 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     // basis (precomputed unless P2G_ENCODE_BASIS=derive) and 16-byte aligned slices
     const bool gen = generate_basis() || mma;  // the tensor-core items take trace strings instead
     if (j.R && j.S && !gen) P2G_CU(c.basis.ensure(basis_bytes(j.S, RG)));
-    if (mma) P2G_CU(c.tcoef.ensure(mma_coef_bytes(j.S, j.R)));
+    if (mma) P2G_CU(c.aimg.ensure(mma_aimg_bytes(j.S, j.R)));
     const uint8_t* esrc = j.d_src;
     uint64_t estride = j.slice;
     if (j.R && j.S && j.slice % 16) {
@@ -465,9 +465,9 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     d.vec = j.slice % 16 == 0 ? 1u : 0u;
     if (mma) {
         d.mma = 1;
-        d.tcoef = c.tcoef.as<uint32_t>();
+        d.aimg = c.aimg.as<uint8_t>();
         d.Rpad = (j.R + kMmaTileRows - 1) / kMmaTileRows * kMmaTileRows;
-        d.Spad = mma_tcoef_spad(j.S);
+        d.ksteps = mma_image_steps(j.S);
         P2G_CU(make_src_map(&d.src_map, esrc, estride, j.S, (uint32_t)(estride / 2)));
     }
     memcpy(H + o_items, pl.items.data(), sizeof(BatchItem) * pl.items.size());
@@ -504,7 +504,7 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
                                  np_bytes - 2ull * pl.zero_from_sym, j.R, st));
     if (d.basis) P2G_CU(launch_basis(c.basis.as<uint16_t>(), j.S, RG, j.R, j.first_exp, st));
     if (mma)
-        P2G_CU(launch_tc_coef_batch(reinterpret_cast<const BatchJob*>(D + o_desc), 1, mma_coef_words(j.S, j.R), st));
+        P2G_CU(launch_a_image_batch(reinterpret_cast<const BatchJob*>(D + o_desc), 1, mma_aimg_bytes(j.S, j.R), st));
     if (esrc != j.d_src) P2G_CU(launch_realign(j.d_src, j.slice, c.src_al.as<uint8_t>(), estride, j.S, j.slice, st));
     P2G_CU(launch_batch(reinterpret_cast<const BatchJob*>(D + o_desc), reinterpret_cast<const BatchItem*>(D + o_items),
                         (uint32_t)pl.items.size(), reinterpret_cast<uint32_t*>(D + o_ctl), err,
@@ -1107,9 +1107,9 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
         }
         P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s));
         if (use_tensor_encode(jb.flags, S, R, jb.slice_size)) {
-            P2G_CU(c.tcoef.ensure(mma_coef_bytes(S, R)));
+            P2G_CU(c.aimg.ensure(mma_aimg_bytes(S, R)));
             P2G_CU(launch_encode_mma(jb.src, jb.src_stride, S, jb.slice_size, R, jb.first_exponent,
-                                     c.tcoef.as<uint32_t>(), jb.recovery, jb.recovery_stride, c.err.as<int>(), s));
+                                     c.aimg.as<uint8_t>(), jb.recovery, jb.recovery_stride, c.err.as<int>(), s));
         } else {
             const bool gen = generate_basis();
             if (!gen) {
@@ -1137,9 +1137,9 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
         if (stride != jb.slice_size)  // the 16-byte padding of each row is read: zero it
             P2G_CU(cudaMemset2DAsync(c.src.as<uint8_t>() + jb.slice_size, stride, 0, stride - jb.slice_size, S, s));
         if (use_tensor_encode(jb.flags, S, R, jb.slice_size)) {
-            P2G_CU(c.tcoef.ensure(mma_coef_bytes(S, R)));
+            P2G_CU(c.aimg.ensure(mma_aimg_bytes(S, R)));
             P2G_CU(launch_encode_mma(c.src.as<uint8_t>(), stride, S, jb.slice_size, R, jb.first_exponent,
-                                     c.tcoef.as<uint32_t>(), c.rec.as<uint8_t>(), stride, c.err.as<int>(), s));
+                                     c.aimg.as<uint8_t>(), c.rec.as<uint8_t>(), stride, c.err.as<int>(), s));
         } else {
             const bool gen = generate_basis();
             if (!gen) {

@@ -124,22 +124,20 @@ cudaError_t launch_encode_noheap(const uint8_t* src, uint64_t src_stride, uint32
 // Device addresses of the GF antilog and input-logbase tables (after upload_tables).
 cudaError_t gf_device_tables(const uint16_t** antilog, const uint16_t** logbase);
 
-// The encode on the tensor cores (p2g_mma.cu): tc_coef_kernel fills
-// `tcoef` (mma_coef_bytes(S, R) of scratch) with the coefficients' trace
-// strings, then the persistent tcgen05 kernel accumulates 16-row x
+// The encode on the tensor cores (p2g_mma.cu): a_image_kernel fills `aimg`
+// (mma_aimg_bytes(S, R) of scratch) with the A operand of every 16-row tile
+// and K-step, then the persistent tcgen05 kernel accumulates 16-row x
 // 240-symbol tiles over all S slices.  src rows are read in whole 16-byte
 // units, as by launch_encode, through a 2-D tensor map (16-byte aligned src
 // and src_stride).
-size_t mma_coef_bytes(uint32_t S, uint32_t R);
-uint64_t mma_coef_words(uint32_t S, uint32_t R);
-// Input slices per 16-row tile in that scratch: S rounded up to 16, plus 16
-// (room for a whole 16-slice copy from any first slice).
-constexpr uint32_t mma_tcoef_spad(uint32_t S) { return (S + 15) / 16 * 16 + 16; }
+size_t mma_aimg_bytes(uint32_t S, uint32_t R);
+// K-steps (4 slices) per 16-row tile in that image: whole 16-slice stages.
+constexpr uint32_t mma_image_steps(uint32_t S) { return (S + 15) / 16 * 4; }
 // The source as a 2-D tensor map of Np u16 symbols x S slices for the
 // tensor-core tiles (cuTensorMapEncodeTiled, found through the runtime).
 cudaError_t make_src_map(CUtensorMap* map, const void* src, uint64_t stride, uint32_t S, uint32_t Np);
 cudaError_t launch_encode_mma(const uint8_t* src, uint64_t src_stride, uint32_t S, uint64_t slice_size, uint32_t R,
-                              uint32_t first_exp, uint32_t* tcoef, uint8_t* rec, uint64_t rec_stride, int* err,
+                              uint32_t first_exp, uint8_t* aimg, uint8_t* rec, uint64_t rec_stride, int* err,
                               cudaStream_t st);
 
 // Size in bytes of the coefficient-basis scratch for S slices and RG groups.
@@ -217,8 +215,8 @@ struct BatchJob {
     uint32_t ts, first_exp;  // ts: tile width (sub-tile width of folded items)
     uint32_t vec;            // slices and file starts of src are 16-byte aligned
     uint32_t mma;            // encode items run on the tensor cores (kItemEncodeMma)
-    uint32_t* tcoef;         // mma: trace strings of the coefficients, per 16-row tile (mma_coef_words)
-    uint32_t Rpad, Spad;     // mma: R rounded up to whole 16-row tiles; tcoef's slices per tile
+    uint8_t* aimg;           // mma: the A operand image (mma_aimg_bytes)
+    uint32_t Rpad, ksteps;   // mma: R rounded up to whole 16-row tiles; the image's K-steps per tile
     CUtensorMap src_map;     // mma: esrc as a 2-D tensor (make_src_map); 64-byte aligned
 };
 
@@ -277,8 +275,9 @@ cudaError_t launch_batch(const BatchJob* jobs, const BatchItem* items, uint32_t 
 // Device address of the 512 G^-1 table entries (256 for the low byte, 256 for
 // the high) after a one-time set-up of the tensor-core tables on this device.
 cudaError_t mma_tables_ready(const uint16_t** ginv);
-// Fills every tensor-core job's trace strings (blockIdx.y = job).
-cudaError_t launch_tc_coef_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_words, cudaStream_t st);
+// Fills every tensor-core job's A image (blockIdx.y = job); max_bytes: the
+// largest image.
+cudaError_t launch_a_image_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_bytes, cudaStream_t st);
 int device_sm_count();
 
 }  // namespace p2g

@@ -1099,12 +1099,12 @@ __device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ Jp, con
     if (threadIdx.x == 0) mma::tensormap_acquire(&J.src_map);  // written by the host's upload of the jobs
     mma::Tile T;
     T.src_map = &J.src_map;
-    T.tcoef = J.tcoef;
+    T.aimg = J.aimg;
     T.rec = J.rec;
     T.rec_stride = J.rec_stride;
     T.s0 = s0;
     T.sn = sn ? sn : J.S - s0;
-    T.Spad = J.Spad;
+    T.ksteps = J.ksteps;
     T.R = J.R;
     T.r0 = ((kind_rg >> 8) & 0xFFFFu) * kMmaTileRows;
     T.n0 = a;

@@ -22,15 +22,16 @@
 //
 // Tile: 16 recovery rows (two M = 128 MMAs, 8 rows x 16 bits each) x 240
 // symbols (N), accumulated in TMEM over all input slices, K-step = 4 slices
-// (K = 64 e2m1 values = 32 bytes per operand row).  Warp roles:
-//   warp 0       TMA producer: 1-D bulk copies of 4 source slices' tile bytes
-//                and of the 16 rows' trace strings of those slices
+// (K = 64 e2m1 values = 32 bytes per operand row).  a_image_kernel first
+// writes the A operand of the whole job to global memory (R x S x 128 bytes,
+// built once instead of once per symbol tile).  Warp roles:
+//   warp 0       TMA producer: per 16 input slices, one bulk copy of their A
+//                rows and one 2-D tensor copy of the tile's source symbols
 //   warp 1       TMEM allocation; lane 0 issues the MMAs and commits
-//   warps 2..15  operand builders (A rows from T_c, B rows from source
-//                symbols, both spread to e2m1 in the canonical K-major
-//                layout, 16-byte K halves), then (warps 2..9) the epilogue:
-//                tcgen05.ld of the sums, parity, one ballot per column (= two
-//                recovery symbols), G^-1, store.
+//   warps 2..15  B operand builders (source symbols spread to e2m1 in the
+//                canonical K-major layout, 16-byte K halves), then (warps
+//                2..9) the epilogue: tcgen05.ld of the sums, parity, one
+//                ballot per column (= two recovery symbols), G^-1, store.
 // The tile pipeline itself is p2g_mma_tile.cuh, shared with the persistent
 // batch kernel's tensor-core items.
 // Every mbarrier wait is bounded; a wait that gives up sets the error flag,
@@ -51,7 +52,7 @@ __device__ uint16_t d_ginv[512];
 namespace {
 
 using namespace mma;
-constexpr int kGenWarps = 14;
+constexpr int kGenWarps = 15;  // 30 B units per operand stage: two each
 constexpr int kThreads = 64 + 32 * kGenWarps;
 
 // shared memory layout (bytes): the rings, G^-1 tables, barriers, misc
@@ -63,8 +64,8 @@ constexpr uint32_t kOffMisc = kOffBars + kBarBytes;
 constexpr uint32_t kSmemBytes = kOffMisc + 16;
 static_assert(kSmemBytes > 116 * 1024, "one CTA per SM: TMEM is allocated whole");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
-static_assert(mma_tcoef_spad(1027) == tcoef_spad(1027) && mma_tcoef_spad(32) == tcoef_spad(32),
-              "host and device agree on the trace-string layout");
+static_assert(mma_image_steps(1027) == a_image_steps(1027) && mma_image_steps(32) == a_image_steps(32),
+              "host and device agree on the A image layout");
 
 }  // namespace
 
@@ -83,30 +84,37 @@ __device__ __forceinline__ uint32_t coef_trace(uint32_t s, uint32_t r, uint32_t 
     return d_trace_lo[c & 0xFFu] ^ d_trace_hi[c >> 8];
 }
 
-// All trace strings of one job in the per-tile layout of p2g_mma_tile.cuh:
-// tcoef[(rt * Spad + s) * 16 + i] for row 16 rt + i, 0 past R or S.
-__device__ __forceinline__ void fill_tcoef(uint32_t* __restrict__ tcoef, uint32_t S, uint32_t R, uint32_t first_exp,
-                                           const uint16_t* __restrict__ antilog, const uint16_t* __restrict__ logbase,
-                                           uint64_t i0, uint64_t step) {
-    const uint32_t Spad = tcoef_spad(S), n_row = (R + kTileRows - 1) / kTileRows;
-    const uint64_t total = (uint64_t)n_row * Spad * kTileRows;
+// The A image of one job (layout: a_image_steps in p2g_mma_tile.cuh), one
+// 16-byte K half of an operand row per step of the loop: rows of recovery
+// row r >= R and slices s >= S are 0.
+__device__ __forceinline__ void fill_a_image(uint8_t* __restrict__ aimg, uint32_t S, uint32_t R, uint32_t first_exp,
+                                             const uint16_t* __restrict__ antilog,
+                                             const uint16_t* __restrict__ logbase, uint64_t i0, uint64_t step) {
+    const uint32_t ksteps = a_image_steps(S), n_row = (R + kTileRows - 1) / kTileRows;
+    const uint64_t total = (uint64_t)n_row * ksteps * (kAStepBytes / 16);
     for (uint64_t i = i0; i < total; i += step) {
-        const uint32_t ri = (uint32_t)(i % kTileRows);
-        const uint64_t q = i / kTileRows;
-        const uint32_t s = (uint32_t)(q % Spad), r = (uint32_t)(q / Spad) * kTileRows + ri;
-        tcoef[i] = (r < R && s < S) ? coef_trace(s, r, first_exp, antilog, logbase) : 0u;
+        const uint32_t c = (uint32_t)(i % (kAStepBytes / 16));  // byte c*16 = t*4096 + grp*256 + kh*128 + m8*16
+        const uint64_t q = i / (kAStepBytes / 16);
+        const uint32_t k = (uint32_t)(q % ksteps), rt = (uint32_t)(q / ksteps);
+        const uint32_t t = c >> 8, grp = (c >> 4) & 15u, kh = (c >> 3) & 1u, m8 = c & 7u;
+        const uint32_t m = grp * 8 + m8, r = rt * kTileRows + 8 * t + (m >> 4), bit = m & 15u;
+        const uint32_t s0 = k * kKSlices + 2 * kh;
+        const uint32_t T0 = (r < R && s0 < S) ? coef_trace(s0, r, first_exp, antilog, logbase) : 0u;
+        const uint32_t T1 = (r < R && s0 + 1 < S) ? coef_trace(s0 + 1, r, first_exp, antilog, logbase) : 0u;
+        const uint2 v0 = spread16((T0 >> bit) & 0xFFFFu), v1 = spread16((T1 >> bit) & 0xFFFFu);
+        reinterpret_cast<uint4*>(aimg)[i] = make_uint4(v0.x, v0.y, v1.x, v1.y);
     }
 }
 
-__global__ void tc_coef_kernel(uint32_t* __restrict__ tcoef, const uint16_t* __restrict__ antilog,
+__global__ void a_image_kernel(uint8_t* __restrict__ aimg, const uint16_t* __restrict__ antilog,
                                const uint16_t* __restrict__ logbase, uint32_t S, uint32_t R, uint32_t first_exp) {
-    fill_tcoef(tcoef, S, R, first_exp, antilog, logbase, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
-               (uint64_t)gridDim.x * blockDim.x);
+    fill_a_image(aimg, S, R, first_exp, antilog, logbase, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                 (uint64_t)gridDim.x * blockDim.x);
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
     encode_mma_kernel(const __grid_constant__ CUtensorMap src_map, uint32_t S, uint32_t Np,
-                      const uint32_t* __restrict__ tcoef, uint32_t R, uint8_t* __restrict__ rec,
+                      const uint8_t* __restrict__ aimg, uint32_t R, uint8_t* __restrict__ rec,
                       uint64_t rec_stride, uint32_t n_row_tiles, uint32_t n_tiles, int* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -138,12 +146,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
         Tile T;
         T.src_map = &src_map;
-        T.tcoef = tcoef;
+        T.aimg = aimg;
         T.rec = rec;
         T.rec_stride = rec_stride;
         T.s0 = 0;
         T.sn = S;
-        T.Spad = tcoef_spad(S);
+        T.ksteps = a_image_steps(S);
         T.R = R;
         T.r0 = (tile % n_row_tiles) * kTileRows;
         T.n0 = (tile / n_row_tiles) * kN;
@@ -259,33 +267,31 @@ cudaError_t mma_tables_ready(const uint16_t** ginv) {
     return e;
 }
 
-// The trace strings of every tensor-core job of a batch (blockIdx.y = job),
-// as tc_coef_kernel computes them for one.
-__global__ void tc_coef_batch_kernel(const BatchJob* __restrict__ jobs, const uint16_t* __restrict__ antilog,
+// The A images of every tensor-core job of a batch (blockIdx.y = job).
+__global__ void a_image_batch_kernel(const BatchJob* __restrict__ jobs, const uint16_t* __restrict__ antilog,
                                      const uint16_t* __restrict__ logbase) {
     const BatchJob& J = jobs[blockIdx.y];
-    if (!J.mma || !J.R || !J.tcoef) return;
-    fill_tcoef(J.tcoef, J.S, J.R, J.first_exp, antilog, logbase, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
-               (uint64_t)gridDim.x * blockDim.x);
+    if (!J.mma || !J.R || !J.aimg) return;
+    fill_a_image(J.aimg, J.S, J.R, J.first_exp, antilog, logbase, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                 (uint64_t)gridDim.x * blockDim.x);
 }
 
-cudaError_t launch_tc_coef_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_words, cudaStream_t st) {
-    if (!n_jobs || !max_words) return cudaSuccess;
+cudaError_t launch_a_image_batch(const BatchJob* jobs, uint32_t n_jobs, uint64_t max_bytes, cudaStream_t st) {
+    if (!n_jobs || !max_bytes) return cudaSuccess;
     const uint16_t* g = nullptr;
     cudaError_t e = mma_tables_ready(&g);
     if (e != cudaSuccess) return e;
     const uint16_t *antilog = nullptr, *logbase = nullptr;
     if ((e = gf_device_tables(&antilog, &logbase)) != cudaSuccess) return e;
-    const uint64_t want = (max_words + 255) / 256;
-    const unsigned bx = (unsigned)std::min<uint64_t>(want, (uint64_t)device_sm_count() * 4);
-    tc_coef_batch_kernel<<<dim3(bx, n_jobs), 256, 0, st>>>(jobs, antilog, logbase);
+    const uint64_t want = (max_bytes / 16 + 255) / 256;
+    const unsigned bx = (unsigned)std::min<uint64_t>(want, (uint64_t)device_sm_count() * 8);
+    a_image_batch_kernel<<<dim3(bx, n_jobs), 256, 0, st>>>(jobs, antilog, logbase);
     add_launches(1);
     return cudaGetLastError();
 }
 
-size_t mma_coef_bytes(uint32_t S, uint32_t R) { return mma_coef_words(S, R) * sizeof(uint32_t); }
-uint64_t mma_coef_words(uint32_t S, uint32_t R) {
-    return (uint64_t)((R + kTileRows - 1) / kTileRows) * tcoef_spad(S) * kTileRows;
+size_t mma_aimg_bytes(uint32_t S, uint32_t R) {
+    return (size_t)((R + kTileRows - 1) / kTileRows) * a_image_steps(S) * kAStepBytes;
 }
 
 // The source as a 2-D tensor of u16 symbols: Np symbols per input slice, S
@@ -318,7 +324,7 @@ cudaError_t make_src_map(CUtensorMap* map, const void* src, uint64_t stride, uin
 }
 
 cudaError_t launch_encode_mma(const uint8_t* src, uint64_t src_stride, uint32_t S, uint64_t slice_size, uint32_t R,
-                              uint32_t first_exp, uint32_t* tcoef, uint8_t* rec, uint64_t rec_stride, int* err,
+                              uint32_t first_exp, uint8_t* aimg, uint8_t* rec, uint64_t rec_stride, int* err,
                               cudaStream_t st) {
     if (!S || !R) return cudaSuccess;
     cudaError_t e = mma_prepare();
@@ -330,14 +336,14 @@ cudaError_t launch_encode_mma(const uint8_t* src, uint64_t src_stride, uint32_t 
     if ((e = make_src_map(&map, src, src_stride, S, Np)) != cudaSuccess) return e;
     const uint32_t n_row = (R + kTileRows - 1) / kTileRows;
     const uint32_t n_sym = (Np + kN - 1) / kN;
-    const uint64_t total = mma_coef_words(S, R);
+    const uint64_t chunks = mma_aimg_bytes(S, R) / 16;
     const int sms = device_sm_count();
-    const unsigned cb = (unsigned)std::min<uint64_t>((total + 255) / 256, (uint64_t)sms * 8);
-    tc_coef_kernel<<<cb, 256, 0, st>>>(tcoef, antilog, logbase, S, R, first_exp);
+    const unsigned cb = (unsigned)std::min<uint64_t>((chunks + 255) / 256, (uint64_t)sms * 8);
+    a_image_kernel<<<cb, 256, 0, st>>>(aimg, antilog, logbase, S, R, first_exp);
     add_launches(1);
     const uint64_t tiles = (uint64_t)n_sym * n_row;
     const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms);
-    encode_mma_kernel<<<grid, kThreads, kSmemBytes, st>>>(map, S, Np, tcoef, R, rec, rec_stride, n_row,
+    encode_mma_kernel<<<grid, kThreads, kSmemBytes, st>>>(map, S, Np, aimg, R, rec, rec_stride, n_row,
                                                           (uint32_t)tiles, err);
     add_launches(1);
     return cudaGetLastError();

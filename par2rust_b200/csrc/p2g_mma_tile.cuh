@@ -7,18 +7,22 @@
 // shared-memory and TMEM layout of one CTA and the work of one 16-row x
 // 240-symbol tile over a range of input slices.
 //
-// Shared memory (from `ring`, 1024-aligned): kOpStages operand stages of
-// two K-steps, 16 KiB each (A rows of the two 8-row halves, 4 KiB each; B
-// rows, 7,680 B), then kInStages input stages of 8,704 B, each covering
-// kInSteps K-steps (16 input slices): the 16 rows' trace strings of those
-// slices ([slice][row], 1 KiB, one bulk copy) and the tile's symbols of those
-// slices ([slice][240 symbols], 7,680 B, one 2-D tensor copy).  Two copies
-// per four K-steps: a copy costs the issuing thread more than a K-step of
-// MMAs, so small copies per slice would starve the tensor core.  Both
-// operands are K-major without swizzle: core matrices of 8 rows x 16 B, K
-// halves 128 B apart, 8-row groups 256 B apart.  TMEM: the two fp32
-// accumulators at columns 0 and 256 (240 columns each), scale factors 1.0 at
-// 496-511.
+// The A operand (the coefficients' bit matrices) depends only on the 16-row
+// tile and the K-step, so it is built once per job in global memory (the A
+// image, a_image_index below) and every tile copies it in.  The B operand
+// (the source symbols' bit planes) is built per tile in shared memory.
+//
+// Shared memory (from `ring`, 1024-aligned): kInStages input stages of
+// 40,448 B, each covering kInSteps K-steps (16 input slices): the A image of
+// those 4 K-steps (4 x 8 KiB: the two 8-row halves' 128 operand rows of 32
+// B, one bulk copy) and the tile's symbols of those slices ([slice][240
+// symbols], 7,680 B, one 2-D tensor copy); then kOpStages operand stages of
+// kOpSteps K-steps of B rows (8 KiB slots of 7,680 B).  The MMAs read A from
+// the input stage, so an input stage is free again when the MMAs of its last
+// K-step have completed.  Both operands are K-major without swizzle: core
+// matrices of 8 rows x 16 B, K halves 128 B apart, 8-row groups 256 B apart.
+// TMEM: the two fp32 accumulators at columns 0 and 256 (240 columns each),
+// scale factors 1.0 at 496-511.
 #pragma once
 #include <stdint.h>
 
@@ -29,32 +33,39 @@ constexpr uint32_t kN = 240;        // symbols per tile (MMA N)
 constexpr uint32_t kTileRows = 16;  // recovery rows per tile (two M = 128 MMAs)
 constexpr uint32_t kKSlices = 4;    // input slices per K-step (K = 64 e2m1 values)
 constexpr uint32_t kOpSteps = 2;    // K-steps per operand stage
-constexpr int kOpStages = 3;
-constexpr uint32_t kInSteps = 4;                   // K-steps per input stage
+constexpr int kOpStages = 4;
+constexpr uint32_t kInSteps = 4;                     // K-steps per input stage
 constexpr uint32_t kInSlices = kInSteps * kKSlices;  // 16 input slices per input stage
-constexpr int kInStages = 8;
+constexpr int kInStages = 3;
 constexpr uint32_t kAccCol1 = 256;                // TMEM column of the second accumulator
 constexpr uint32_t kSfaCol = 496, kSfbCol = 504;  // scale factors (all 1.0)
 constexpr uint32_t kATileBytes = 4096;            // 128 rows x 32 B
+constexpr uint32_t kAStepBytes = 2 * kATileBytes;  // both halves of one K-step
 constexpr uint32_t kBTileBytes = kN * 32;         // 240 rows x 32 B
-constexpr uint32_t kOpStepBytes = 2 * kATileBytes + 8192;
-constexpr uint32_t kOpStageBytes = kOpSteps * kOpStepBytes;
+constexpr uint32_t kBSlotBytes = 8192;
+constexpr uint32_t kOpStageBytes = kOpSteps * kBSlotBytes;
 constexpr uint32_t kSrcSliceBytes = kN * 2;
-constexpr uint32_t kInCoefBytes = kInSlices * kTileRows * 4;               // 1 KiB
-constexpr uint32_t kInSrcBytes = kInSlices * kSrcSliceBytes;               // 7,680 B
-constexpr uint32_t kInStageBytes = kInCoefBytes + kInSrcBytes;             // 8,704 B
-constexpr uint32_t kRingBytes = kOpStages * kOpStageBytes + kInStages * kInStageBytes;
+constexpr uint32_t kInABytes = kInSteps * kAStepBytes;         // 32 KiB
+constexpr uint32_t kInSrcBytes = kInSlices * kSrcSliceBytes;   // 7,680 B
+constexpr uint32_t kInStageBytes = kInABytes + kInSrcBytes;    // 40,448 B
+constexpr uint32_t kRingBytes = kInStages * kInStageBytes + kOpStages * kOpStageBytes;
 constexpr uint32_t kGinvBytes = 1024;             // G^-1 tables: 256 lo then 256 hi u16
 constexpr uint32_t kNumBars = 2 * kInStages + 2 * kOpStages + 3;
 constexpr uint32_t kBarBytes = kNumBars * 8;
-static_assert(kInStageBytes % 128 == 0 && kInCoefBytes % 128 == 0, "tensor copies land 128-byte aligned");
-
-// Trace strings in global memory, per 16-row tile: tcoef[(rt * Spad + s) *
-// 16 + i] = T_c for recovery row 16 rt + i and input slice s (0 past R or S).
-// Spad leaves room for a whole stage's copy from any first slice.
-__host__ __device__ constexpr uint32_t tcoef_spad(uint32_t S) { return (S + 15) / 16 * 16 + kInSlices; }
-static_assert(kBTileBytes <= kOpStepBytes - 2 * kATileBytes, "B tile fits its K-step");
+static_assert(kInStageBytes % 128 == 0 && kInABytes % 128 == 0, "tensor copies land 128-byte aligned");
+static_assert(kBTileBytes <= kBSlotBytes, "B tile fits its slot");
 static_assert(kInSteps == 2 * kOpSteps, "an input stage feeds two operand stages");
+
+// The A image in global memory: for 16-row tile rt and K-step k (slices 4k ..
+// 4k+3), 8 KiB laid out as in shared memory -- byte
+//   ((rt * ksteps + k) * 2 + t) * 4096 + grp * 256 + kh * 128 + m8 * 16
+// holds operand row m = 8 grp + m8 of half t (recovery row 16 rt + 8 t + m /
+// 16, bit i = m % 16), K half kh (slices 4k + 2kh, 4k + 2kh + 1): 8 e2m1
+// bytes per slice, the spread of bits i..i+15 of T_c.  ksteps = a_image_steps
+// (S): whole input stages, zero past S and R.
+__host__ __device__ constexpr uint32_t a_image_steps(uint32_t S) {
+    return (S + kInSlices - 1) / kInSlices * kInSteps;
+}
 
 // Instruction descriptor of kind::mxf4 with UE8M0 block scales: A and B
 // e2m1 (format 1 at bits 7 and 10), K-major, N >> 3 at bit 17, scale format
@@ -187,12 +198,14 @@ struct Bars {
           op_empty(b + 16 * kInStages + 8 * kOpStages), acc_full(b + 16 * kInStages + 16 * kOpStages),
           acc_empty(acc_full + 8), drain(acc_full + 16) {}
 };
-// One thread: counts for `ngen` operand-building warps.
+// One thread: counts for `ngen` operand-building warps.  An input stage is
+// released by the MMA warp's commit after its last K-step (the builders have
+// read it by then: the MMAs waited for their operands).
 __device__ __forceinline__ void init_bars(uint32_t b, uint32_t ngen) {
     const Bars B(b);
     for (int i = 0; i < kInStages; ++i) {
         bar_init(B.in_full + 8 * i, 1);
-        bar_init(B.in_empty + 8 * i, ngen);
+        bar_init(B.in_empty + 8 * i, 1);
     }
     for (int i = 0; i < kOpStages; ++i) {
         bar_init(B.op_full + 8 * i, ngen);
@@ -222,22 +235,23 @@ __device__ __forceinline__ void sf_fill(uint32_t tmem, uint32_t q) {
 }
 
 // One tile: recovery rows [r0, r0+16) x symbols [n0, n0+syms) over input
-// slices [s0, s0+sn).  src_map: 2-D tensor map over the source (u16 symbols
-// x input slices, the slice stride a multiple of 16 bytes; symbols and slices
-// past its extent read 0); n0 is a multiple of 8.  The trace strings are at
-// tcoef in the per-tile layout above, Spad = tcoef_spad(S).  accumulate: XOR
-// the tile into the rows (the caller zeroed them) instead of storing it.
+// slices [s0, s0+sn), s0 a multiple of 16 and s0+sn a multiple of 4 or S.
+// src_map: 2-D tensor map over the source (u16 symbols x input slices, the
+// slice stride a multiple of 16 bytes; symbols and slices past its extent
+// read 0); n0 is a multiple of 8.  aimg: the job's A image (ksteps =
+// a_image_steps(S)).  accumulate: XOR the tile into the rows (the caller
+// zeroed them) instead of storing it.
 struct Tile {
     const void* src_map;
-    const uint32_t* tcoef;
+    const uint8_t* aimg;
     uint8_t* rec;
     uint64_t rec_stride;
-    uint32_t s0, sn, Spad, R, r0, n0, syms, accumulate;
+    uint32_t s0, sn, ksteps, R, r0, n0, syms, accumulate;
 };
 
 // Per-CTA pipeline state, the same in every thread: operand stages, input
-// stages, tiles and drains so far (ring positions and barrier
-// parities follow from them).
+// stages, tiles and drains so far (ring positions and barrier parities follow
+// from them).
 struct Pipe {
     uint32_t ring, bars, tmem;
     const uint16_t* ginv;  // shared memory
@@ -246,21 +260,23 @@ struct Pipe {
 };
 
 // All threads of the CTA call this.  Warp 0 lane 0 streams the inputs, warp
-// 1 lane 0 issues the MMAs, warps 2 .. 2+NGEN-1 build operands and run the
-// epilogue (the first eight of them; warp w reads TMEM lanes 32*(w%4)..).
-// Other warps idle.  Returns false (uniformly, after a CTA barrier) when a
-// bounded wait gave up; copies and MMAs in flight have then landed.
+// 1 lane 0 issues the MMAs, warps 2 .. 2+NGEN-1 build the B operand and run
+// the epilogue (the first eight of them; warp w reads TMEM lanes
+// 32*(w%4)..).  Other warps idle.  Returns false (uniformly, after a CTA
+// barrier) when a bounded wait gave up; copies and MMAs in flight have then
+// landed.
 template <int NGEN>
 __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
     static_assert(NGEN >= 8, "eight warps cover the two accumulators' four lane quadrants");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const Bars B(P.bars);
-    const uint32_t op0 = P.ring, in0 = P.ring + kOpStages * kOpStageBytes;
+    const uint32_t in0 = P.ring, op0 = P.ring + kInStages * kInStageBytes;
     const uint32_t KS = (T.sn + kKSlices - 1) / kKSlices, NI = (KS + kInSteps - 1) / kInSteps;
     const uint32_t NS = (KS + kOpSteps - 1) / kOpSteps;  // operand stages
     const uint32_t g0 = P.g, gi0 = P.gi, tc = P.tcount, rt = T.r0 / kTileRows;
-    // a tensor copy's x offset must be 16-byte aligned (the same in every thread)
-    if (T.n0 & 7u) return false;
+    // a tensor copy's x offset must be 16-byte aligned, the A image is cut in
+    // whole input stages (the same in every thread)
+    if ((T.n0 & 7u) || (T.s0 % kInSlices)) return false;
     bool ok = true;
     if (warp == 0) {
         if (lane == 0) {
@@ -273,11 +289,12 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
                 }
                 const uint32_t sa = T.s0 + k * kInSlices;
                 const uint32_t dst = in0 + st * kInStageBytes;
-                // slices past the tile's range (up to 15) are copied too and
-                // masked by the builders; past S the tensor map reads 0
+                // slices past the tile's range (up to 15) are copied too: the
+                // builders mask their B rows
                 bar_expect_tx(B.in_full + 8 * st, kInStageBytes);
-                tma_1d(dst, T.tcoef + ((size_t)rt * T.Spad + sa) * kTileRows, kInCoefBytes, B.in_full + 8 * st);
-                tma_2d(dst + kInCoefBytes, T.src_map, (int32_t)T.n0, (int32_t)sa, B.in_full + 8 * st);
+                tma_1d(dst, T.aimg + ((size_t)rt * T.ksteps + sa / kKSlices) * kAStepBytes, kInABytes,
+                       B.in_full + 8 * st);
+                tma_2d(dst + kInABytes, T.src_map, (int32_t)T.n0, (int32_t)sa, B.in_full + 8 * st);
             }
             if (!ok)  // copies issued but maybe not consumed land before the stages are reused
                 for (uint32_t q = gi > gi0 + kInStages ? gi - kInStages : gi0; q < gi; ++q)
@@ -290,7 +307,8 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
             tc_fence_after();
             uint32_t g = g0;
             for (uint32_t p = 0; ok && p < NS; ++p, ++g) {
-                const uint32_t so = g % kOpStages;
+                const uint32_t so = g % kOpStages, gi = gi0 + p / 2, si = gi % kInStages;
+                // the A rows were copied with the input stage, which the builders waited for
                 if (!bar_wait(B.op_full + 8 * so, (g / kOpStages) & 1u, P.abort_flag)) {
                     ok = false;
                     break;
@@ -300,14 +318,15 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
                 for (uint32_t ks = 0; ks < kOpSteps; ++ks) {
                     const uint32_t k = p * kOpSteps + ks;
                     if (k >= KS) break;
-                    const uint32_t a = op0 + so * kOpStageBytes + ks * kOpStepBytes;
-                    const uint64_t bdesc = smem_desc(a + 2 * kATileBytes, 128, 256);
+                    const uint32_t a = in0 + si * kInStageBytes + ((p & 1u) * kOpSteps + ks) * kAStepBytes;
+                    const uint64_t bdesc = smem_desc(op0 + so * kOpStageBytes + ks * kBSlotBytes, 128, 256);
                     mma_mxf4(P.tmem, smem_desc(a, 128, 256), bdesc, P.tmem + kSfaCol, P.tmem + kSfbCol, k > 0);
                     if (two)
                         mma_mxf4(P.tmem + kAccCol1, smem_desc(a + kATileBytes, 128, 256), bdesc, P.tmem + kSfaCol,
                                  P.tmem + kSfbCol, k > 0);
                 }
                 mma_commit(B.op_empty + 8 * so);
+                if ((p & 1u) || p == NS - 1) mma_commit(B.in_empty + 8 * si);
             }
             if (ok) {
                 mma_commit(B.acc_full);
@@ -318,47 +337,34 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
         }
     } else if (warp < 2 + NGEN) {
         const int gw = warp - 2;
-        // A lane writes one 16-byte K half (2 slices) of one operand row:
-        // rows m8 of 8-row group 2v+gsub, K half kh -- each quarter warp
-        // stores 128 contiguous bytes.  Per operand stage the builders share
-        // 31 warp units per K-step (v 0..15: A, the 32 8-row groups of the
-        // two accumulators; v 16..30: B, the 30 8-row groups of the 240
-        // symbols), dealt round-robin over the warps.  Both kinds take the
-        // same steps: two 32-bit loads from the input stage (A: trace strings
-        // of slices 2kh, 2kh+1; B: the words holding symbol n of them), a
-        // shift and mask to 16 bits (A: bits i..i+15 of T for row bit i; B:
-        // the symbol's half), spread16, one 16-byte store.
+        // A lane writes one 16-byte K half (2 slices) of one B row: symbols
+        // m8 of 8-row group 2v+gsub, K half kh -- each quarter warp stores 128
+        // contiguous bytes.  Per operand stage the builders share 15 warp
+        // units per K-step (v = 0..14: the 30 8-row groups of the 240
+        // symbols), dealt round-robin over the warps.  A unit: two 32-bit
+        // loads from the input stage (the words holding symbol n of slices
+        // 2kh and 2kh+1), the symbol's half, spread16, one 16-byte store.
         const uint32_t m8 = (uint32_t)lane & 7u, kh = ((uint32_t)lane >> 3) & 1u, gsub = (uint32_t)lane >> 4;
         const uint32_t lane_off = kh * 128 + m8 * 16;
-        constexpr int kUnits = 31 * (int)kOpSteps;
+        constexpr int kUnits = 15 * (int)kOpSteps;
         constexpr int kTasks = (kUnits + NGEN - 1) / NGEN;
-        // fixed for the tile, per task: input offsets (from the input stage)
-        // for the first and the second operand stage of the pair, operand
-        // offset (from the operand stage), shift | distance to the second
-        // slice << 8 | slice within the stage << 20, and the 2-bit-pair mask
-        // (0 for symbols past the tile).  Tasks past the units load from
-        // offset 0 and store nothing.
-        uint32_t t_in0[kTasks], t_in1[kTasks], t_op[kTasks], t_fl[kTasks], t_m[kTasks];
+        // fixed for the tile, per task: input offset (from the input stage,
+        // first operand stage of the pair), operand offset (from the operand
+        // stage), shift | slice within the operand stage << 8, and the
+        // 2-bit-pair mask (0 for symbols past the tile).  Tasks past the units
+        // load from offset 0 and store nothing.
+        uint32_t t_in[kTasks], t_op[kTasks], t_fl[kTasks], t_m[kTasks];
 #pragma unroll
         for (int j = 0; j < kTasks; ++j) {
             const uint32_t u = (uint32_t)gw + (uint32_t)j * NGEN;
-            const uint32_t ks = u / 31u, v = u % 31u;
-            const uint32_t sl = ks * kKSlices + 2 * kh;
+            const uint32_t ks = u / 15u, v = u % 15u;
+            const uint32_t grp = 2 * v + gsub, n = grp * 8 + m8;
             if (u >= (uint32_t)kUnits) {
-                t_in0[j] = t_in1[j] = t_op[j] = t_fl[j] = t_m[j] = 0;
-            } else if (v < 16) {
-                const uint32_t G = 2 * v + gsub, t = G >> 4, grp = G & 15u, m = grp * 8 + m8;
-                t_in0[j] = ks * kKSlices * kTileRows * 4 + (2 * kh * kTileRows + 8 * t + (m >> 4)) * 4;
-                t_in1[j] = t_in0[j] + kOpSteps * kKSlices * kTileRows * 4;
-                t_op[j] = ks * kOpStepBytes + t * kATileBytes + grp * 256 + lane_off;
-                t_fl[j] = (m & 15u) | ((kTileRows * 4) << 8) | (sl << 20);
-                t_m[j] = 0x3333u;
+                t_in[j] = t_op[j] = t_fl[j] = t_m[j] = 0;
             } else {
-                const uint32_t grp = 2 * (v - 16) + gsub, n = grp * 8 + m8;
-                t_in0[j] = kInCoefBytes + ks * kKSlices * kSrcSliceBytes + 2 * kh * kSrcSliceBytes + ((n * 2) & ~3u);
-                t_in1[j] = t_in0[j] + kOpSteps * kKSlices * kSrcSliceBytes;
-                t_op[j] = ks * kOpStepBytes + 2 * kATileBytes + grp * 256 + lane_off;
-                t_fl[j] = ((n & 1u) * 16) | (kSrcSliceBytes << 8) | (sl << 20);
+                t_in[j] = kInABytes + (ks * kKSlices + 2 * kh) * kSrcSliceBytes + ((n * 2) & ~3u);
+                t_op[j] = ks * kBSlotBytes + grp * 256 + lane_off;
+                t_fl[j] = ((n & 1u) * 16) | ((ks * kKSlices + 2 * kh) << 8);
                 t_m[j] = n < T.syms ? 0x3333u : 0u;
             }
         }
@@ -370,18 +376,20 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
                 ok = false;
                 break;
             }
-            const uint32_t ins = in0 + si * kInStageBytes, ops = op0 + so * kOpStageBytes;
+            // this operand stage's symbols: K-steps 2*half, 2*half+1 of the input stage
+            const uint32_t ins = in0 + si * kInStageBytes + half * kOpSteps * kKSlices * kSrcSliceBytes;
+            const uint32_t ops = op0 + so * kOpStageBytes;
             // slices of this operand stage: [first, first + 8); past sn the K positions get 0
             const int32_t klim = (int32_t)T.sn - (int32_t)(p * kOpSteps * kKSlices);
             const bool full = klim >= (int32_t)(kOpSteps * kKSlices);
 #pragma unroll
             for (int j = 0; j < kTasks; ++j) {
                 const uint32_t fl = t_fl[j];
-                const uint32_t a0 = ins + (half ? t_in1[j] : t_in0[j]), a1 = a0 + ((fl >> 8) & 0xFFFu);
-                const uint32_t x0 = lds_b32(a0), x1 = lds_b32(a1);
+                const uint32_t a0 = ins + t_in[j];
+                const uint32_t x0 = lds_b32(a0), x1 = lds_b32(a0 + kSrcSliceBytes);
                 uint32_t m0 = t_m[j], m1 = t_m[j];
                 if (!full) {
-                    const int32_t sl = (int32_t)(fl >> 20);
+                    const int32_t sl = (int32_t)(fl >> 8);
                     if (sl >= klim) m0 = 0;
                     if (sl + 1 >= klim) m1 = 0;
                 }
@@ -396,10 +404,7 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) {
-                bar_arrive(B.op_full + 8 * so);
-                if (half == 1 || p == NS - 1) bar_arrive(B.in_empty + 8 * si);
-            }
+            if (lane == 0) bar_arrive(B.op_full + 8 * so);
         }
         if (ok && !bar_wait(B.acc_full, tc & 1u, P.abort_flag)) ok = false;
         if (ok && gw < 8) {
