@@ -375,7 +375,10 @@ Plan plan_tiles(std::vector<PlanJob>& jobs, uint32_t ctas, uint32_t flags) {
 double est_md5_ms(uint64_t bytes) { return md5_ms(bytes); }
 // A tensor-core item: one K-step (4 slices) of operand building and two
 // MMAs, plus the pipeline fill and the epilogue.
-constexpr double kMmaStepMs = 6.9e-4, kMmaFixedMs = 0.004;  // measured: 16.97 ms for the 538 MB / R 200 encode
+// Per 4-slice K-step and per tile on one SM, from the standalone kernel on
+// 14,209 tiles of 16 rows x 240 symbols (96 per SM): 1.93 ms at 256 slices,
+// 5.38 ms at 1,024.
+constexpr double kMmaStepMs = 1.87e-4, kMmaFixedMs = 0.005;
 double est_mma_item_ms(uint32_t slices) { return (slices + 3) / 4 * kMmaStepMs + kMmaFixedMs + kItemMs; }
 // Whether a job's encode runs on the tensor cores: by the cost of its items
 // on a full GPU (the lookup kernel folds a short last row group; the tensor

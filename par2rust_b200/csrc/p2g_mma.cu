@@ -52,7 +52,7 @@ __device__ uint16_t d_ginv[512];
 namespace {
 
 using namespace mma;
-constexpr int kGenWarps = 15;  // 30 B units per operand stage: two each
+constexpr int kGenWarps = 15;  // 60 B units per operand stage: four each
 constexpr int kThreads = 64 + 32 * kGenWarps;
 
 // shared memory layout (bytes): the rings, G^-1 tables, barriers, misc

@@ -32,8 +32,8 @@ namespace mma {
 constexpr uint32_t kN = 240;        // symbols per tile (MMA N)
 constexpr uint32_t kTileRows = 16;  // recovery rows per tile (two M = 128 MMAs)
 constexpr uint32_t kKSlices = 4;    // input slices per K-step (K = 64 e2m1 values)
-constexpr uint32_t kOpSteps = 2;    // K-steps per operand stage
-constexpr int kOpStages = 4;
+constexpr uint32_t kOpSteps = 4;    // K-steps per operand stage
+constexpr int kOpStages = 2;
 constexpr uint32_t kInSteps = 4;                     // K-steps per input stage
 constexpr uint32_t kInSlices = kInSteps * kKSlices;  // 16 input slices per input stage
 constexpr int kInStages = 3;
@@ -54,7 +54,8 @@ constexpr uint32_t kNumBars = 2 * kInStages + 2 * kOpStages + 3;
 constexpr uint32_t kBarBytes = kNumBars * 8;
 static_assert(kInStageBytes % 128 == 0 && kInABytes % 128 == 0, "tensor copies land 128-byte aligned");
 static_assert(kBTileBytes <= kBSlotBytes, "B tile fits its slot");
-static_assert(kInSteps == 2 * kOpSteps, "an input stage feeds two operand stages");
+constexpr uint32_t kOpPerIn = kInSteps / kOpSteps;  // operand stages per input stage
+static_assert(kInSteps % kOpSteps == 0, "an input stage feeds whole operand stages");
 
 // The A image in global memory: for 16-row tile rt and K-step k (slices 4k ..
 // 4k+3), 8 KiB laid out as in shared memory -- byte
@@ -307,7 +308,7 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
             tc_fence_after();
             uint32_t g = g0;
             for (uint32_t p = 0; ok && p < NS; ++p, ++g) {
-                const uint32_t so = g % kOpStages, gi = gi0 + p / 2, si = gi % kInStages;
+                const uint32_t so = g % kOpStages, gi = gi0 + p / kOpPerIn, si = gi % kInStages;
                 // the A rows were copied with the input stage, which the builders waited for
                 if (!bar_wait(B.op_full + 8 * so, (g / kOpStages) & 1u, P.abort_flag)) {
                     ok = false;
@@ -318,7 +319,7 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
                 for (uint32_t ks = 0; ks < kOpSteps; ++ks) {
                     const uint32_t k = p * kOpSteps + ks;
                     if (k >= KS) break;
-                    const uint32_t a = in0 + si * kInStageBytes + ((p & 1u) * kOpSteps + ks) * kAStepBytes;
+                    const uint32_t a = in0 + si * kInStageBytes + ((p % kOpPerIn) * kOpSteps + ks) * kAStepBytes;
                     const uint64_t bdesc = smem_desc(op0 + so * kOpStageBytes + ks * kBSlotBytes, 128, 256);
                     mma_mxf4(P.tmem, smem_desc(a, 128, 256), bdesc, P.tmem + kSfaCol, P.tmem + kSfbCol, k > 0);
                     if (two)
@@ -326,7 +327,7 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
                                  P.tmem + kSfbCol, k > 0);
                 }
                 mma_commit(B.op_empty + 8 * so);
-                if ((p & 1u) || p == NS - 1) mma_commit(B.in_empty + 8 * si);
+                if (p % kOpPerIn == kOpPerIn - 1 || p == NS - 1) mma_commit(B.in_empty + 8 * si);
             }
             if (ok) {
                 mma_commit(B.acc_full);
@@ -370,16 +371,16 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
         }
         uint32_t g = g0;
         for (uint32_t p = 0; p < NS; ++p, ++g) {
-            const uint32_t half = p & 1u, gi = gi0 + p / 2, si = gi % kInStages, so = g % kOpStages;
+            const uint32_t half = p % kOpPerIn, gi = gi0 + p / kOpPerIn, si = gi % kInStages, so = g % kOpStages;
             if ((half == 0 && !bar_wait(B.in_full + 8 * si, (gi / kInStages) & 1u, P.abort_flag)) ||
                 !bar_wait(B.op_empty + 8 * so, ((g / kOpStages) & 1u) ^ 1u, P.abort_flag)) {
                 ok = false;
                 break;
             }
-            // this operand stage's symbols: K-steps 2*half, 2*half+1 of the input stage
+            // this operand stage's symbols: K-steps kOpSteps*half .. of the input stage
             const uint32_t ins = in0 + si * kInStageBytes + half * kOpSteps * kKSlices * kSrcSliceBytes;
             const uint32_t ops = op0 + so * kOpStageBytes;
-            // slices of this operand stage: [first, first + 8); past sn the K positions get 0
+            // slices of this operand stage: [first, first + 4 kOpSteps); past sn the K positions get 0
             const int32_t klim = (int32_t)T.sn - (int32_t)(p * kOpSteps * kKSlices);
             const bool full = klim >= (int32_t)(kOpSteps * kKSlices);
 #pragma unroll
