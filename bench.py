@@ -14,9 +14,11 @@ Exponential volume split.
   e2e        the same metric through the public API (p2g_create_in_memory):
              pinned host source -> H2D -> device job -> whole-file MD5 ->
              D2H of recovery rows + checksums -> index/volume bytes in memory.
-  roofline   the encode kernel alone (CUDA events per launch) against the
-             measured HBM copy peak; `lut_roofline` against the shared-memory
-             lookup bound the LUT kernel is designed to.
+  roofline   the timed step's encode against the unit it is bound by: the
+             tensor pipe (nominal dense FP4, 2 x 256 e2m1 FLOP per GF MAC) when
+             the planner runs tensor-core items, else the shared-memory lookup
+             bound of the LUT kernel; `lookup_roofline` and `hbm_roofline`
+             beside it, and `encode_only` times each encode kernel alone.
   cpu_baseline  the reference's CPU create path (C port with the GFNI/AVX-512
              kernel, all host threads) on a bounded sample of the same file.
 
@@ -138,6 +140,14 @@ class ClockSampler:
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
                 "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+FP4_DENSE_TFLOPS = 9000.0  # nominal dense FP4 (block-scaled e2m1) tensor rate of one B200
+
+
+def measured_bf16():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    return json.load(open(p)).get("bf16_tflops") if os.path.exists(p) else None
 
 
 def measured_peaks():
@@ -640,6 +650,7 @@ def bench_many(dev, steps, warmup, e2e_steps, cpu_seconds, no_cpu_baseline=False
         "value": total / (ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": ms, "steps": steps,
         "encode_only_ms": enc, "encode_gf_mac_per_s": {k: macs / (v * 1e-3) for k, v in enc.items()},
         "lut_frac_of_lookup_bound": macs / (enc["lut"] * 1e-3) / lut_peak,
+        "tensor_frac_of_nominal_fp4": 2 * 256 * macs / (enc["tensor"] * 1e-3) / 1e12 / FP4_DENSE_TFLOPS,
         "e2e": e2e, "parity": par, "cpu_baseline": cb, "clocks": clk, "gpu_launches": launches,
     }
 
@@ -919,6 +930,9 @@ def main():
     alg_bytes = S * slice_ + R * slice_  # padded source read once + recovery written once
     macs = S * R * (slice_ // 2)
     lut_peak = 32 * 148 * 1965e6  # 2 shared-memory u16 lookups per MAC at 128 B/clk/SM, max clock
+    # which encode the step's plan runs: the planner reports tensor-core items with fold 0
+    plan_items, _, _ = p2g.plan_device_job(slice_, S, R)
+    step_tensor = bool(plan_items) and all(it["fold"] == 0 for it in plan_items)
     traffic = None  # DRAM bytes per batch_kernel launch (ncu, profiles/)
     tp = os.path.join(ROOT, "profiles", "batch_kernel_traffic.json")
     if os.path.exists(tp):
@@ -1017,6 +1031,24 @@ def main():
     if rank != 0:
         return 0
     step_macs = macs / (ms_max * 1e-3)
+    lookup_roofline = {"bound": "smem", "achieved": step_macs, "peak": lut_peak, "unit": "GF(2^16) MAC/s",
+                       "frac": step_macs / lut_peak,
+                       "peak_source": "computed: 2 shared-memory u16 lookups per GF MAC at 128 B/clk/SM, 148 SMs, "
+                                      "1965 MHz (the lookup kernel's design bound)"}
+    kernel_note = ("batch_kernel (one launch per step: encode items, slice MD5/CRC32, packet-MD5 chains) + "
+                   + ("a_image_kernel" if step_tensor else "basis_kernel")
+                   + "; timed per step with events on the launching stream")
+    if step_tensor:
+        # 16 x 16 e2m1 products (mul + add) per GF MAC on the tensor pipe
+        step_tflops = 2 * 256 * macs / (ms_max * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "achieved": step_tflops, "peak": FP4_DENSE_TFLOPS, "unit": "TFLOP/s",
+                    "frac": step_tflops / FP4_DENSE_TFLOPS, "traffic": traffic,
+                    "peak_source": "nominal dense FP4 (kind::mxf4) rate of B200; MEASURED_PEAKS.json holds no FP4 "
+                                   "figure (its bf16 GEMM: %s TFLOP/s)" % measured_bf16(),
+                    "kernel": kernel_note + "; encode items on tcgen05 kind::mxf4", "kernel_ms": ms_max,
+                    "macs_per_launch": macs, "e2m1_flop_per_launch": 2 * 256 * macs}
+    else:
+        roofline = dict(lookup_roofline, traffic=traffic, kernel=kernel_note, kernel_ms=ms_max, macs_per_launch=macs)
     line = {
         "metric": "encode source GB/s", "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
@@ -1029,14 +1061,11 @@ def main():
                 "the library's buffers, copy=False)",
                 "output_files": len(files)},
         "e2e_files": e2e_files,
-        # the binding unit of the timed step: the encode items' shared-memory lookups
-        "roofline": {"bound": "smem", "achieved": step_macs, "peak": lut_peak, "unit": "GF(2^16) MAC/s",
-                     "frac": step_macs / lut_peak, "traffic": traffic,
-                     "peak_source": "computed: 2 shared-memory u16 lookups per GF MAC at 128 B/clk/SM, 148 SMs, "
-                                    "1965 MHz (the lookup kernel's design bound)",
-                     "kernel": "batch_kernel (one launch per step: encode items, slice MD5/CRC32, packet-MD5 chains) "
-                               "+ basis_kernel; timed per step with events on the launching stream",
-                     "kernel_ms": ms_max, "macs_per_launch": macs},
+        # the binding unit of the timed step's encode: the tensor pipe (tcgen05
+        # items) or the shared-memory lookups (lookup-table items)
+        "roofline": roofline,
+        "step_encode": "tensor" if step_tensor else "lut",
+        "lookup_roofline": lookup_roofline,
         "hbm_roofline": {"bound": "hbm", "achieved": alg_bytes / (ms_max * 1e-3) / 1e9, "peak": hbm_peak,
                          "unit": "GB/s", "frac": alg_bytes / (ms_max * 1e-3) / 1e9 / hbm_peak, "traffic": traffic,
                          "peak_source": peak_kind, "algorithmic_bytes": alg_bytes},
@@ -1044,9 +1073,10 @@ def main():
             "lut": {"kernel": "basis_kernel + encode_lut_kernel (p2g_encode, one launch)", "kernel_ms": enc_lut,
                     "gf_mac_per_s": macs / (enc_lut * 1e-3), "frac_of_lookup_bound": macs / (enc_lut * 1e-3) / lut_peak,
                     "kernel_ms_basis_derived": enc_derive},
-            "tensor": {"kernel": "tc_coef_kernel + encode_mma_kernel (tcgen05 kind::mxf4, p2g_encode)",
+            "tensor": {"kernel": "a_image_kernel + encode_mma_kernel (tcgen05 kind::mxf4, p2g_encode)",
                        "kernel_ms": enc_tensor, "gf_mac_per_s": macs / (enc_tensor * 1e-3),
-                       "e2m1_tflops": 2 * 256 * macs / (enc_tensor * 1e-3) / 1e12}},
+                       "e2m1_tflops": 2 * 256 * macs / (enc_tensor * 1e-3) / 1e12,
+                       "frac_of_nominal_fp4": 2 * 256 * macs / (enc_tensor * 1e-3) / 1e12 / FP4_DENSE_TFLOPS}},
         "cpu_baseline": cb,
         "clocks": clk,
         "gpu_launches": launches,
