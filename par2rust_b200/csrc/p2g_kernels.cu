@@ -1143,11 +1143,15 @@ __device__ __forceinline__ bool id_eq(const uint4& a, const uint4& b) {
     return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w;
 }
 
+// The MD5 items (scan, file hash, packets, chain segments) are kept out of
+// line: their chain loops then get registers of their own rather than a
+// share of the persistent kernel's 128, which spills.
+//
 // Slice MD5 of slices [first, first+count) of job J on the kHashThreads
 // lanes (one slice each, staged through the lane's ring).  The other warps
 // idle: the lanes are bound by their chains, and the SM is the item's alone.
 template <bool VEC>
-__device__ __forceinline__ void batch_scan(const BatchJob& J, uint32_t first, uint32_t count, uint32_t ring) {
+__device__ __noinline__ void batch_scan(const BatchJob& J, uint32_t first, uint32_t count, uint32_t ring) {
     const int tid = threadIdx.x;
     if (tid < kHashThreads && (uint32_t)tid < count) {
         const uint32_t s = first + tid;
@@ -1162,7 +1166,7 @@ __device__ __forceinline__ void batch_scan(const BatchJob& J, uint32_t first, ui
 // Whole-file MD5 (hash_full, src/source.rs:222-228) of files [first,
 // first+count) of job J, one file per MD5 lane: a serial chain each.
 template <bool VEC>
-__device__ __forceinline__ void batch_file_hash(const BatchJob& J, uint32_t first, uint32_t count, uint32_t ring) {
+__device__ __noinline__ void batch_file_hash(const BatchJob& J, uint32_t first, uint32_t count, uint32_t ring) {
     const int tid = threadIdx.x;
     if (tid < kHashThreads && (uint32_t)tid < count) {
         const uint32_t f = first + tid;
@@ -1259,7 +1263,7 @@ __device__ void batch_set_id(const BatchJob& J, uint32_t ring, uint32_t* sid) {
 // Packet MD5 of recovery rows [r0, r1) of job J (all threads of the CTA):
 // MD5(set_id ‖ "PAR 2.0\0RecvSlic" ‖ exponent le32 ‖ row)
 // (src/packet/recovery.rs:15, src/format.rs:33-54).
-__device__ void batch_packets(const BatchJob& J, uint32_t ring, const uint32_t* sid, uint32_t r0, uint32_t r1) {
+__device__ __noinline__ void batch_packets(const BatchJob& J, uint32_t ring, const uint32_t* sid, uint32_t r0, uint32_t r1) {
     const int tid = threadIdx.x;
     if (tid < kHashThreads) {
         for (uint32_t r = r0 + tid; r < r1; r += kHashThreads) {
@@ -1279,7 +1283,7 @@ __device__ void batch_packets(const BatchJob& J, uint32_t ring, const uint32_t* 
 // Chain segment: rows of block q advance over the message blocks that band b
 // completed (set id ‖ type ‖ exponent ‖ row bytes; the last band also pads
 // and writes the digests).  State between bands lives in J.chain.
-__device__ void advance_rows(const BatchJob& J, uint32_t q, uint32_t b, uint32_t ring, const uint32_t* sid) {
+__device__ __noinline__ void advance_rows(const BatchJob& J, uint32_t q, uint32_t b, uint32_t ring, const uint32_t* sid) {
     const int tid = threadIdx.x;
     const uint64_t total = 36 + J.slice;
     const uint64_t nblocks = (total + 8) / 64 + 1;
