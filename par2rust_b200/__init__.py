@@ -393,9 +393,12 @@ class _OutputSetOwner:
 
     def __init__(self, os_):
         self.os_ = os_
+        # bound now: at interpreter exit the module globals may be gone first
+        self._free = lib().p2g_output_set_free
+        self._byref = C.byref
 
     def __del__(self):
-        lib().p2g_output_set_free(C.byref(self.os_))
+        self._free(self._byref(self.os_))
 
 
 def create_in_memory(opts: CreateOptions, inputs: Sequence[Tuple[bytes, object]],
