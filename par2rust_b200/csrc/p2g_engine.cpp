@@ -43,6 +43,11 @@ p2g_status cuda_fail(cudaError_t e, const char* what) {
 }
 
 static inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+// One-launch upload of page-locked inputs: from this many files on, in
+// segments of at most 4 MiB (a segment's zero pad, the tail of a file's last
+// slice, is encoded in 24 bits; larger tails are memset apart).
+constexpr uint32_t kGatherMinFiles = 8;
+constexpr uint64_t kGatherSegBytes = 4ull << 20;
 
 // Grow-only device buffer.
 struct DevBuf {
@@ -91,8 +96,9 @@ struct Context {
     cudaEvent_t ev_fork = nullptr, ev_h16k = nullptr, ev_join[kStreams] = {}, ev_band[kBandEvents] = {};
     DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out, md5_state;
     DevBuf aimg;       // A operand image of the tensor-core encode
+    DevBuf gseg;       // segment table of the one-launch upload of page-locked inputs
     DevBuf persist;    // single-job persistent run: descriptor, items, chain state, tables
-    PinBuf h_spans, h_h16k, h_err, h_stage, h_persist;
+    PinBuf h_spans, h_h16k, h_err, h_stage, h_persist, h_gseg;
     PinBuf h_rec;   // host copy of the recovery rows (create calls)
     PinBuf h_prog;  // encode progress: the device queue head, read while a job runs
 };
@@ -850,13 +856,49 @@ static p2g_status device_create(Context& c, const CreateInput* in, uint32_t n, u
     if (!src_known && fmode == FileHashMode::Host) hh.start(ptrs, lens, host_full);
 
     // Upload: each file to its first slice, zero the tail of its last slice.
+    // Many page-locked inputs go in one launch that reads them over the bus
+    // (thousands of small copies and memsets cost more in calls than in
+    // bytes); the rest, and a few large files, by cudaMemcpyAsync.
     cudaStream_t up = c.st[0];
+    std::vector<uint8_t> pinned(n, 0);
+    uint32_t n_pinned = 0;
+    for (uint32_t f = 0; f < n && n >= kGatherMinFiles; ++f) {
+        cudaPointerAttributes pa;
+        if (in[f].length && cudaPointerGetAttributes(&pa, in[f].data) == cudaSuccess &&
+            pa.type == cudaMemoryTypeHost && pa.devicePointer == in[f].data) {
+            pinned[f] = 1;
+            ++n_pinned;
+        }
+        cudaGetLastError();  // an unregistered pointer is not an error here
+    }
+    std::vector<uint64_t> seg;
+    if (n_pinned >= kGatherMinFiles) seg.reserve(3 * (size_t)(n_pinned + src_bytes / kGatherSegBytes + 1));
     for (uint32_t f = 0; f < n; ++f) {
         uint8_t* dst = c.src.as<uint8_t>() + files[f].first_slice * slice;
         const uint64_t cap = files[f].slices * slice;
         const uint64_t cp = std::min(in[f].length, cap);
+        if (n_pinned >= kGatherMinFiles && pinned[f]) {
+            const bool pad_in_seg = cap - cp < (1ull << 24);
+            if (!pad_in_seg) P2G_CU(cudaMemsetAsync(dst + cp, 0, cap - cp, up));
+            for (uint64_t o = 0; o < cp; o += kGatherSegBytes) {
+                const uint64_t len = std::min<uint64_t>(kGatherSegBytes, cp - o);
+                const uint64_t pad = o + len == cp && pad_in_seg ? cap - cp : 0;
+                seg.push_back((uint64_t)(uintptr_t)(in[f].data + o));
+                seg.push_back((uint64_t)(uintptr_t)(dst + o));
+                seg.push_back(len | (pad << 40));
+            }
+            continue;
+        }
         if (cp) P2G_CU(cudaMemcpyAsync(dst, in[f].data, cp, cudaMemcpyHostToDevice, up));
         if (cap > cp) P2G_CU(cudaMemsetAsync(dst + cp, 0, cap - cp, up));
+    }
+    if (!seg.empty()) {
+        const size_t bytes = 8 * seg.size();
+        P2G_CU(c.h_gseg.ensure(bytes));
+        P2G_CU(c.gseg.ensure(bytes));
+        memcpy(c.h_gseg.p, seg.data(), bytes);
+        P2G_CU(cudaMemcpyAsync(c.gseg.p, c.h_gseg.p, bytes, cudaMemcpyHostToDevice, up));
+        P2G_CU(launch_gather_host(c.gseg.as<uint64_t>(), (uint32_t)(seg.size() / 3), up));
     }
     P2G_CU(cudaStreamSynchronize(up));
 

@@ -87,6 +87,10 @@ cudaError_t launch_md5_recovery_range(const uint8_t* rec, uint64_t stride, uint3
 cudaError_t launch_realign(const uint8_t* src, uint64_t src_stride, uint8_t* dst,
                            uint64_t dst_stride, uint32_t count, uint64_t slice_size,
                            cudaStream_t st);
+// Copies n_seg segments from page-locked host memory to the device in one
+// launch: seg (device memory) holds 3 words per segment -- host source,
+// device destination, length | zero padding after it << 40.
+cudaError_t launch_gather_host(const uint64_t* seg, uint32_t n_seg, cudaStream_t st);
 
 // Banded encode: band b covers symbol positions [begin, end) of every row in
 // tiles of ts symbols; bands are launched in order on one stream.

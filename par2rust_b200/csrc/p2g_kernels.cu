@@ -1042,6 +1042,28 @@ __global__ void realign_kernel(const uint8_t* __restrict__ src, uint64_t src_str
     }
 }
 
+// Upload of page-locked host inputs in one launch: segment k copies len
+// bytes from seg[3k] (a host address the device reads directly, over the
+// bus) to seg[3k+1] and then zeroes pad bytes after them (the tail of a
+// file's last slice).  One CTA per segment at a time; 16-byte accesses when
+// both ends are 16-byte aligned, else bytes.  seg[3k+2] = len | pad << 40.
+__global__ void gather_host_kernel(const uint64_t* __restrict__ seg, uint32_t n_seg) {
+    for (uint32_t k = blockIdx.x; k < n_seg; k += gridDim.x) {
+        const uint8_t* s = reinterpret_cast<const uint8_t*>(seg[3 * k]);
+        uint8_t* d = reinterpret_cast<uint8_t*>(seg[3 * k + 1]);
+        const uint64_t len = seg[3 * k + 2] & ((1ull << 40) - 1), pad = seg[3 * k + 2] >> 40;
+        uint64_t done = 0;
+        if ((((uintptr_t)s | (uintptr_t)d) & 15) == 0) {
+            const uint64_t n16 = len / 16;
+            for (uint64_t i = threadIdx.x; i < n16; i += blockDim.x)
+                reinterpret_cast<uint4*>(d)[i] = reinterpret_cast<const uint4*>(s)[i];
+            done = n16 * 16;
+        }
+        for (uint64_t i = done + threadIdx.x; i < len; i += blockDim.x) d[i] = s[i];
+        for (uint64_t i = threadIdx.x; i < pad; i += blockDim.x) d[len + i] = 0;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Batched create.  One CTA per SM pops work items off a device queue until
 // it is empty.  Items of one job never wait for one another: the CTA whose
@@ -1938,6 +1960,14 @@ cudaError_t launch_realign(const uint8_t* src, uint64_t src_stride, uint8_t* dst
     const uint64_t want = (total + 255) / 256;
     const unsigned blocks = (unsigned)(want < (uint64_t)sm_count() * 16 ? want : (uint64_t)sm_count() * 16);
     realign_kernel<<<blocks, 256, 0, st>>>(src, src_stride, dst, dst_stride, count, slice_size);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_host(const uint64_t* seg, uint32_t n_seg, cudaStream_t st) {
+    if (!n_seg) return cudaSuccess;
+    const unsigned blocks = n_seg < (uint32_t)sm_count() * 4 ? n_seg : (unsigned)sm_count() * 4;
+    gather_host_kernel<<<blocks, 512, 0, st>>>(seg, n_seg);
     count_launch();
     return cudaGetLastError();
 }

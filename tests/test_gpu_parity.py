@@ -473,3 +473,35 @@ def test_device_job_persistent_equals_banded(p2g, gpu, monkeypatch, lens, slice_
         assert persistent[5][16 * i:16 * i + 16].tobytes() == hashlib.md5(host[off:off + n].tobytes()).digest(), i
         off += (n + slice_ - 1) // slice_ * slice_
 
+
+
+def test_create_in_memory_pinned_inputs_equal_pageable(p2g, oracle, gpu):
+    """Many page-locked inputs are uploaded by one kernel that reads them
+    over the bus: odd lengths, slice tails to zero, pointers at odd offsets
+    inside a pinned allocation, and files of several 4 MiB segments give the
+    same bytes as the same inputs from pageable memory, and as the oracle."""
+    import torch
+
+    rng = np.random.default_rng(21)
+    lens = [int(x) for x in rng.integers(1, 300_000, size=30)] + [9 * 1024 * 1024 + 13, 65536, 1]
+    pool = torch.empty(sum(lens) + 64 * len(lens), dtype=torch.uint8, pin_memory=True)
+    pinned, pageable, off = [], [], 0
+    for i, n in enumerate(lens):
+        off += 1 + (i % 7)  # odd offsets: the copy takes its byte path there
+        data = rnd(500 + i, n)
+        view = pool[off:off + n]
+        view.numpy()[:] = data
+        pinned.append((f"p{i:02d}.bin".encode(), view))
+        pageable.append((f"p{i:02d}.bin".encode(), data.tobytes()))
+        off += n
+    opts = p2g.CreateOptions(output="pin.par2", slice_size=65536, recovery_block_count=12,
+                             volume_scheme=p2g.VolumeScheme.Uniform(3))
+    a = p2g.create_in_memory(opts, pinned)
+    b = p2g.create_in_memory(opts, pageable)
+    assert [n for n, _ in a] == [n for n, _ in b]
+    for (n, x), (_, y) in zip(a, b):
+        assert x == y, n
+    want = oracle.create([(n, d) for n, d in pageable], 65536, 12, kind=oracle.SCHEME_UNIFORM, count=3,
+                         index_path="pin.par2")
+    for (n, x), (m, y) in zip(a, want):
+        assert n == m and x == y, n
