@@ -788,6 +788,29 @@ static Md5 critical_packets(uint64_t slice, const p2g_source_file* src, uint32_t
     return set_id;
 }
 
+// Byte length of the critical packet block of n inputs, before any of them
+// is hashed: the packets' sizes depend on names, lengths and slice counts
+// only, so zero hashes and checksums stand in.
+static size_t critical_len_of(uint64_t slice, const CreateInput* in, uint32_t n, const char* const* comments,
+                              uint32_t n_comments) {
+    std::vector<p2g_source_file> src(n);
+    uint64_t max_slices = 0;
+    for (uint32_t f = 0; f < n; ++f) max_slices = std::max<uint64_t>(max_slices, (in[f].length + slice - 1) / slice);
+    std::vector<p2g_slice_checksum> zero(std::max<uint64_t>(max_slices, 1));
+    memset(zero.data(), 0, sizeof(p2g_slice_checksum) * zero.size());
+    for (uint32_t f = 0; f < n; ++f) {
+        memset(&src[f], 0, sizeof src[f]);
+        src[f].name = const_cast<uint8_t*>(in[f].name);
+        src[f].name_len = in[f].name_len;
+        src[f].length = in[f].length;
+        src[f].slice_count = (in[f].length + slice - 1) / slice;
+        src[f].slice_checksums = zero.data();
+    }
+    std::vector<uint8_t> out;
+    critical_packets(slice, src.data(), n, comments, n_comments, out);
+    return out.size();
+}
+
 // Pinned host copy of a create call's recovery rows.  The context keeps the
 // buffer for the next call (pinning ~100 MB takes tens of milliseconds)
 // unless it grew past kRetainPinnedRec.
@@ -1794,6 +1817,24 @@ extern "C" p2g_status p2g_create_in_memory(const p2g_create_options* opts, const
     std::vector<p2g_output_file> vols(vs.size());
     size_t crit_len = 0;
     bool vols_ok = true;
+    // The volume buffers are allocated, and their pages touched, on a host
+    // thread while the device works: with hundreds of MB of recovery
+    // packets the first-touch page faults would otherwise fall between the
+    // download and the return.
+    std::vector<uint8_t*> pre(vs.size(), nullptr);
+    size_t pre_clen = 0;
+    std::thread prefault([&]() {
+        pre_clen = critical_len_of(slice, ins.data(), n, opts->comments, opts->comment_count);
+        for (size_t v = 0; v < vs.size(); ++v) {
+            const size_t len = 2 * pre_clen + (size_t)vs[v] * (68 + slice);
+            pre[v] = (uint8_t*)malloc(std::max<size_t>(len, 1));
+            if (pre[v])
+                for (size_t o = 0; o < len; o += 4096) pre[v][o] = 0;
+        }
+    });
+    auto take_pre = [&]() {  // joins the thread; buffers not handed out are freed by the caller below
+        if (prefault.joinable()) prefault.join();
+    };
     auto free_vols = [&]() {
         for (auto& of : vols) {
             free(of.name);
@@ -1803,6 +1844,7 @@ extern "C" p2g_status p2g_create_in_memory(const p2g_create_options* opts, const
     };
     const WhileHashing lay_out = [&](const CreateOutput& o, size_t clen) {
         crit_len = clen;
+        take_pre();
         uint32_t first = 0;
         std::vector<std::vector<uint8_t>> headers(vs.size());
         std::vector<std::pair<const uint8_t*, size_t>> pieces;
@@ -1820,7 +1862,12 @@ extern "C" p2g_status p2g_create_in_memory(const p2g_create_options* opts, const
             p2g_output_file& of = vols[v];
             of.name = dupstr(volume_filename(index, (uint16_t)first, vs[v]));
             of.length = tot;
-            of.data = (uint8_t*)malloc(std::max<size_t>(tot, 1));
+            if (pre[v] && clen == pre_clen) {
+                of.data = pre[v];  // prefaulted, the same size
+                pre[v] = nullptr;
+            } else {
+                of.data = (uint8_t*)malloc(std::max<size_t>(tot, 1));
+            }
             if (!of.name || !of.data) {
                 vols_ok = false;
                 break;
@@ -1851,6 +1898,8 @@ extern "C" p2g_status p2g_create_in_memory(const p2g_create_options* opts, const
     };
     const p2g_status st = device_create(c, ins.data(), n, slice, R, nullptr, opts->comments, opts->comment_count, co,
                                         rec, &lay_out);
+    take_pre();
+    for (uint8_t* b : pre) free(b);  // unused (a failed call, or a size that changed)
     if (st != P2G_OK || !vols_ok || co.critical.size() != crit_len) {
         free_vols();
         if (st != P2G_OK) return st;
