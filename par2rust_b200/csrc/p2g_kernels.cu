@@ -770,10 +770,10 @@ __device__ void md5_range_ring(uint32_t st[4], const uint32_t* pre, const uint8_
     for (; b < b_to && (b < rb0 || b >= rb1); ++b) generic(b);
     const uint64_t fast_end = rb1 < b_to ? rb1 : b_to;
     if (b < fast_end) {
-        auto fetch = [&](uint64_t u) {  // one unit = one commit group (possibly empty)
+        auto fetch = [&](uint64_t u, uint32_t slot) {  // one unit = one commit group (possibly empty)
             if (u < n_units) {
                 const uint8_t* g = data + 64 * u;
-                const uint32_t d = ring + (uint32_t)(u % UNITS) * 64;
+                const uint32_t d = ring + slot * 64;
                 if (VEC) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) cp_async16(d + 16 * q, g + 16 * q);
@@ -788,22 +788,32 @@ __device__ void md5_range_ring(uint32_t st[4], const uint32_t* pre, const uint8_
         const uint64_t first_w = 16 * b - PW;
         const uint64_t u_lo = first_w / 16;
         const uint64_t u_hi0 = (first_w + 15) / 16;
-        for (uint64_t u = u_lo; u < u_hi0 + AHEAD; ++u) fetch(u);
+        for (uint64_t u = u_lo; u < u_hi0 + AHEAD; ++u) fetch(u, (uint32_t)(u % UNITS));
+        // Each block moves the ring by one unit (16 words): the next unit to
+        // fetch, its slot and the slot of the block's first aligned quad are
+        // stepped as 32-bit counters, so no 64-bit remainder (the ring need
+        // not be a power of two) sits between one compress and the next.
+        constexpr uint32_t RW = 16 * UNITS;  // ring size in words
+        uint64_t u_next = u_hi0 + AHEAD;
+        uint32_t f_slot = (uint32_t)(u_next % UNITS);
+        uint32_t w_slot = (uint32_t)(((16 * b - PW) & ~3ull) % RW);
         for (; b < fast_end; ++b) {
-            const uint64_t u_hi = (16 * b + 15 - PW) / 16;
-            fetch(u_hi + AHEAD);
+            fetch(u_next, f_slot);
+            ++u_next;
+            f_slot = f_slot + 1 == (uint32_t)UNITS ? 0u : f_slot + 1;
             cp_async_wait<AHEAD>();
-            const uint64_t w0 = (16 * b - PW) & ~3ull;  // aligned quad holding the first word
             uint32_t q[NQ * 4];
 #pragma unroll
             for (int i = 0; i < NQ; ++i) {
-                const uint32_t widx = (uint32_t)((w0 + 4 * i) % (16 * UNITS));
+                uint32_t widx = w_slot + 4 * i;
+                if (widx >= RW) widx -= RW;
                 const uint4 v = lds128(ring + widx * 4);
                 q[4 * i] = v.x;
                 q[4 * i + 1] = v.y;
                 q[4 * i + 2] = v.z;
                 q[4 * i + 3] = v.w;
             }
+            w_slot = w_slot + 16 >= RW ? w_slot + 16 - RW : w_slot + 16;
 #pragma unroll
             for (int i = 0; i < 16; ++i) m[i] = q[SH + i];
             md5_compress(st, m);
