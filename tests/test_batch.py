@@ -98,6 +98,8 @@ def test_device_job_plan_covers_every_slice_of_every_tile_once(p2g, slice_, S, R
         assert 0 <= it["row_group"] < RG and it["fold"] in ((0,) if tensor else (1, 2, 4))
         assert it["fold"] <= 1 or it["row_group"] == RG - 1
         assert not tensor or (it["symbols"] <= 240 and it["first_symbol"] % 240 == 0)
+        # tensor-core pieces start on whole 16-slice stages of the A image
+        assert not tensor or it["first_slice"] % 16 == 0
         assert 0 < it["symbols"] and it["first_symbol"] + it["symbols"] <= Np
         assert 0 <= it["first_slice"] and it["first_slice"] + it["slices"] <= S and it["slices"] > 0
         assert it["accumulate"] == (0 if it["slices"] == S else 1)
