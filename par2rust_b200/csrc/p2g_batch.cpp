@@ -670,8 +670,10 @@ extern "C" p2g_status p2g_batch_create(const p2g_batch_job* jobs, uint32_t n, ui
     // One encode kernel for the whole launch: forced by the flags (or
     // P2G_ENCODE_VARIANT), else the one the cost model prefers for the
     // batch's total encode work.  Lookup and tensor-core items are not mixed
-    // in one launch: batches that mixed them gave wrong recovery bytes for a
-    // few tensor-core tiles (each kind alone is bit-exact).
+    // in one launch: mixed launches gave wrong recovery bytes for a few
+    // tensor-core tiles, and with the proxy fences between item kinds a
+    // 256-job mixed launch still ran into a bounded wait (each kind alone is
+    // bit-exact).
     const char* ev = getenv("P2G_ENCODE_VARIANT");
     bool use_mma;
     if (flags & P2G_BATCH_TENSOR) {

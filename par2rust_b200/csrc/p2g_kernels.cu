@@ -1116,6 +1116,10 @@ __device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ Jp, con
     uint32_t* mm = reinterpret_cast<uint32_t*>(smem + kBatchMmaBarsOff + mma::kBarBytes);
     uint16_t* gsm = reinterpret_cast<uint16_t*>(smem + mma::kRingBytes);  // shared with other item kinds
     for (int i = threadIdx.x; i < 512; i += kEncThreads) gsm[i] = ginv[i];
+    // Earlier items stored to this shared memory through the generic proxy;
+    // the tile's bulk and tensor copies write it through the async proxy.
+    // Order the two before any copy is issued.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     const BatchJob& J = *Jp;
     mma::Pipe P;
@@ -1505,7 +1509,10 @@ __global__ void __launch_bounds__(kEncThreads, 1)
         }
         if (MMA && kind == kItemEncodeMma) {
             const bool ok = batch_mma_tile(&J, mma_ginv, it.kind_rg, it.a, it.b, it.s0, it.sn);
-            // the operand rings covered the encode region's barriers: set them up again
+            // the operand rings covered the encode region's barriers: set them up
+            // again; and the builders' generic stores there come before any
+            // later item's bulk copies (async proxy) into the same bytes
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             if (tid == 0) {
                 for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
                 fence_mbar_init();

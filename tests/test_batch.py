@@ -263,6 +263,8 @@ def batch_jobs(p2g):
 @pytest.mark.gpu
 @pytest.mark.parametrize("variant", ["by-shape", "tensor", "lut"])
 def test_batch_matches_oracle(p2g, oracle, gpu, batch_jobs, variant):
+    """Every job of a heterogeneous batch against the oracle, with the encode
+    on the kernel the cost model picks for the batch, or forced to either."""
     import torch
 
     flags = {"by-shape": 0, "tensor": p2g.BATCH_TENSOR, "lut": p2g.BATCH_LUT}[variant]
