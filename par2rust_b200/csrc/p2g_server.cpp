@@ -56,6 +56,10 @@ struct SJob {
     uint32_t source_kind = 0;
     const uint8_t* host_src = nullptr;
     uint64_t source_bytes = 0, footprint = 0;
+    // encode on the tensor cores (items of kind kItemEncodeMma); the job's A
+    // image then lives in its device allocation (aimg_bytes)
+    bool mma = false;
+    uint64_t aimg_bytes = 0;
     // device memory (one allocation) and the tables uploaded with it
     void* mem = nullptr;
     BatchJob desc{};
@@ -163,7 +167,27 @@ void plan_job(p2g_server* s, SJob& j) {
     }
     j.todo.push_back({j.slot, kItemSetId, 0, 0, 0, 0});
     j.todo_ms.push_back(est_set_id_ms(j.n));
-    if (j.R) {
+    if (j.R && j.mma) {
+        // tensor-core items: 16-row tiles x 240 symbols, slice chunks on whole
+        // 16-slice stages of the A image, again at most ~wave_ms/4 each
+        const double per_stage = est_mma_item_ms(16) - est_mma_item_ms(0);
+        uint32_t mchunk = (uint32_t)std::max(1.0, floor(s->wave_ms / 4.0 / per_stage)) * 16;
+        if (mchunk >= j.S) mchunk = j.S;
+        const uint32_t mchunks = (j.S + mchunk - 1) / mchunk;
+        const uint32_t mtiles = (j.Np + kMmaTileSymbols - 1) / kMmaTileSymbols;
+        const uint32_t RT = (j.R + kMmaTileRows - 1) / kMmaTileRows;
+        for (uint32_t t = 0; t < mtiles; ++t) {
+            const uint32_t n0 = t * kMmaTileSymbols, syms = std::min(kMmaTileSymbols, j.Np - n0);
+            for (uint32_t c = 0; c < mchunks; ++c) {
+                const uint32_t s0 = c * mchunk, sn = std::min(mchunk, j.S - s0);
+                for (uint32_t rt = 0; rt < RT; ++rt) {
+                    j.todo.push_back({j.slot, encode_mma_kind(rt, mchunks > 1), n0, syms, s0, sn});
+                    j.todo_ms.push_back(est_mma_item_ms(sn));
+                    j.enc_total++;
+                }
+            }
+        }
+    } else if (j.R) {
         const bool acc = chunks > 1;
         const uint32_t F = tail_fold(j.R);  // the last row group covers F tiles per item
         for (uint32_t t = 0; t < tiles; ++t) {
@@ -200,7 +224,8 @@ p2g_status admit(p2g_server* s) {
                                  round_up(32ull * j.n + 12, 256) + round_up(j.h_names.size() + 4, 256) +
                                  round_up(8ull * j.n, 256) + round_up(24ull * j.n, 256) + round_up(8ull * j.n, 256);
         const uint64_t realign_b = j.slice % 16 ? round_up((uint64_t)j.S * rec_stride, 256) : 0;
-        const uint64_t total = src_b + rec_b + chk_b + small_b + realign_b;
+        const uint64_t aimg_b = j.mma ? round_up(j.aimg_bytes, 256) : 0;
+        const uint64_t total = src_b + rec_b + chk_b + small_b + realign_b + aimg_b;
         cudaError_t e = cudaMallocAsync(&j.mem, total, s->copy);
         if (e == cudaErrorMemoryAllocation) {
             cudaGetLastError();
@@ -263,6 +288,14 @@ p2g_status admit(p2g_server* s) {
             d.esrc = src;
             d.estride = j.slice;
         }
+        if (j.mma) {
+            d.mma = 1;
+            d.aimg = take(aimg_b);
+            d.Rpad = (j.R + kMmaTileRows - 1) / kMmaTileRows * kMmaTileRows;
+            d.ksteps = mma_image_steps(j.S);
+            const cudaError_t me = make_src_map(&d.src_map, d.esrc, d.estride, j.S, (uint32_t)(d.estride / 2));
+            if (me != cudaSuccess) return fail_cuda(s, me, "tensor map");
+        }
         const uint32_t slot = s->free_slots.back();
         s->free_slots.pop_back();
         j.slot = slot;
@@ -282,6 +315,7 @@ p2g_status admit(p2g_server* s) {
         if (realign_b) SRV_CU(s, launch_realign(src, j.slice, const_cast<uint8_t*>(d.esrc), rec_stride, j.S, j.slice, c));
         if (j.R) SRV_CU(s, cudaMemsetAsync(d.rec, 0, (uint64_t)j.R * rec_stride, c));
         SRV_CU(s, cudaMemcpyAsync(s->d_jobs + slot, &j.desc, sizeof(BatchJob), cudaMemcpyHostToDevice, c));
+        if (j.mma) SRV_CU(s, launch_a_image_batch(s->d_jobs + slot, 1, j.aimg_bytes, c));
         SRV_CU(s, cudaEventCreateWithFlags(&j.ready, cudaEventDisableTiming));
         SRV_CU(s, cudaEventRecord(j.ready, c));
         plan_job(s, j);
@@ -328,7 +362,8 @@ p2g_status retire(p2g_server* s, bool block) {
             case kItemScan:
             case kItemCrc: j->scan_done++; break;
             case kItemSetId: j->setid_done = true; break;
-            case kItemEncode: j->enc_done++; break;
+            case kItemEncode:
+            case kItemEncodeMma: j->enc_done++; break;
             case kItemPacket: j->pkt_done += it.b; break;
             }
         }
@@ -370,11 +405,21 @@ p2g_status launch_wave(p2g_server* s, bool* launched) {
     Wave w;
     w.buf = buf;
     double used = 0;
+    // A launch runs one kind of encode item: the first encode item taken
+    // sets it, and a job whose next item is of the other kind waits for a
+    // later wave (its scan, set-id and packet items run in either kind).
+    int wave_mma = -1;
     auto take_from = [&](SJob& j, double quota) {
         double got = 0;
         while (got < quota && w.items.size() < kWaveItems) {
             if (!j.todo.empty()) {
                 const BatchItem it = j.todo.front();
+                const uint32_t kd = it.kind_rg & kItemKindMask;
+                if (kd == kItemEncode || kd == kItemEncodeMma) {
+                    const int km = kd == kItemEncodeMma ? 1 : 0;
+                    if (wave_mma < 0) wave_mma = km;
+                    if (wave_mma != km) break;
+                }
                 const double ms = j.todo_ms.front();
                 j.todo.pop_front();
                 j.todo_ms.pop_front();
@@ -403,7 +448,8 @@ p2g_status launch_wave(p2g_server* s, bool* launched) {
     order.reserve(w.items.size());
     for (auto& [j, it] : w.items) {
         const uint32_t k = it.kind_rg & kItemKindMask;
-        const double ms = k == kItemEncode ? est_encode_item_ms(it.sn, std::min(it.b & 0xFFFFu, j->desc.ts))
+        const double ms = k == kItemEncode      ? est_encode_item_ms(it.sn, std::min(it.b & 0xFFFFu, j->desc.ts))
+                          : k == kItemEncodeMma ? est_mma_item_ms(it.sn)
                           : k == kItemScan ? est_scan_item_ms(j->slice, it.b)
                           : k == kItemCrc ? est_crc_item_ms(j->slice, it.b)
                           : k == kItemSetId ? est_set_id_ms(j->n)
@@ -416,7 +462,7 @@ p2g_status launch_wave(p2g_server* s, bool* launched) {
     cudaStream_t e = s->exec;
     SRV_CU(s, cudaMemcpyAsync(s->d_items[buf], s->h_items[buf], sizeof(BatchItem) * n, cudaMemcpyHostToDevice, e));
     SRV_CU(s, cudaMemsetAsync(s->d_ctl[buf], 0, sizeof(uint32_t) * (1 + s->max_jobs), e));
-    SRV_CU(s, launch_batch(s->d_jobs, s->d_items[buf], n, s->d_ctl[buf], s->d_err, s->ctas, e));
+    SRV_CU(s, launch_batch(s->d_jobs, s->d_items[buf], n, s->d_ctl[buf], s->d_err, s->ctas, e, wave_mma == 1));
     SRV_CU(s, cudaMemcpyAsync(s->h_err + buf, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, e));
     SRV_CU(s, cudaEventCreateWithFlags(&w.ev, cudaEventDisableTiming));
     SRV_CU(s, cudaEventRecord(w.ev, e));
@@ -553,6 +599,17 @@ extern "C" p2g_status p2g_server_submit(p2g_server* s, const p2g_server_job* rq,
     j->RG = (j->R + kRowsPerGroup - 1) / kRowsPerGroup;
     j->Np = (uint32_t)(round_up(j->slice, 16) / 2);
     j->footprint = S * j->slice + (uint64_t)j->R * round_up(j->slice, 16);
+    // tensor-core encode when the cost model prefers it and the A image
+    // (R x S x 128 B) stays within a quarter of the source bytes
+    const char* ev = getenv("P2G_ENCODE_VARIANT");  // "lut" / "tensor" force a kind (tensor: if the image fits)
+    const bool want_mma = ev && !strcmp(ev, "lut") ? false
+                          : ev && !strcmp(ev, "tensor") ? true
+                                                        : prefer_mma(j->slice, j->S, j->R);
+    if (j->R && want_mma && 4 * mma_aimg_bytes(j->S, j->R) <= S * j->slice) {
+        j->mma = true;
+        j->aimg_bytes = mma_aimg_bytes(j->S, j->R);
+        j->footprint += j->aimg_bytes;
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->fatal != P2G_OK) return set_error(s->fatal, "server stopped: %s", s->fatal_msg.c_str());
     if (j->footprint > s->budget)

@@ -92,7 +92,13 @@ def _serve(p2g, jobs, budget, wave_ms=2.0):
     return outs, done, stats
 
 
-def test_serve_mix_matches_oracle_and_respects_budget(p2g, oracle, gpu):
+@pytest.mark.parametrize("variant", ["by-shape", "tensor"])
+def test_serve_mix_matches_oracle_and_respects_budget(p2g, oracle, gpu, variant, monkeypatch):
+    """The mix against the oracle.  With the tensor-core encode forced, the
+    jobs whose A image fits (R 10 on 64 KiB slices, R 7 on realigned 4,100-byte
+    slices) run tensor-core items, and waves alternate the two kinds."""
+    if variant == "tensor":
+        monkeypatch.setenv("P2G_ENCODE_VARIANT", "tensor")
     jobs = list(enumerate(MIX))
     assert sum(_footprint(*j) for _, j in jobs) > BUDGET  # admission must queue
     outs, done, stats = _serve(p2g, jobs, BUDGET)
