@@ -1099,7 +1099,10 @@ constexpr size_t kBatchRingBytes = (size_t)kHashThreads * kBatchRingLane;
 // address, an abort flag and the pipeline state live past the other regions,
 // so they persist across items.
 constexpr size_t kBatchMmaBarsOff = kBatchEncBytes + kBatchRingBytes + 4 * 256 * 4 + 64;
-constexpr size_t kBatchSmem = kBatchMmaBarsOff + mma::kBarBytes + 32;
+// the G^-1 tables of tensor-core items, copied once per launch, after the
+// pipeline state words
+constexpr size_t kBatchGinvOff = kBatchMmaBarsOff + mma::kBarBytes + 32;
+constexpr size_t kBatchSmem = kBatchGinvOff + mma::kGinvBytes;
 static_assert(kBatchEncBytes % 16 == 0, "MD5 rings must start 16-byte aligned");
 static_assert(mma::kRingBytes + mma::kGinvBytes <= kBatchEncBytes + kBatchRingBytes,
               "tensor-core rings fit the encode region and the MD5 rings");
@@ -1114,8 +1117,8 @@ __device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ Jp, con
                                             uint32_t kind_rg, uint32_t a, uint32_t b, uint32_t s0, uint32_t sn) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint32_t* mm = reinterpret_cast<uint32_t*>(smem + kBatchMmaBarsOff + mma::kBarBytes);
-    uint16_t* gsm = reinterpret_cast<uint16_t*>(smem + mma::kRingBytes);  // shared with other item kinds
-    for (int i = threadIdx.x; i < 512; i += kEncThreads) gsm[i] = ginv[i];
+    (void)ginv;
+    const uint16_t* gsm = reinterpret_cast<const uint16_t*>(smem + kBatchGinvOff);  // filled at launch start
     // Earlier items stored to this shared memory through the generic proxy;
     // the tile's bulk and tensor copies write it through the async proxy.
     // Order the two before any copy is issued.
@@ -1449,6 +1452,8 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     if (MMA) {
         mma::tc_fence_after();
         if ((tid >> 5) >= 4 && (tid >> 5) < 8) mma::sf_fill(mma_misc[0], (uint32_t)(tid >> 5) & 3u);
+        uint16_t* gsm = reinterpret_cast<uint16_t*>(smem + kBatchGinvOff);
+        for (int i = tid; i < 512; i += kEncThreads) gsm[i] = mma_ginv[i];
         mma::tc_fence_before();
         __syncthreads();
         mma::tc_fence_after();
