@@ -83,6 +83,10 @@ def lib() -> C.CDLL:
         L.cb_create_timed.restype = C.c_double
         L.cb_create_timed.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_int, C.c_void_p,
                                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.cb_create_timed_ex.restype = C.c_double
+        L.cb_create_timed_ex.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_int, C.c_void_p,
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.c_int]
         L.cb_recovery_packet_md5.argtypes = [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_uint32,
                                              C.c_void_p, C.c_int]
         _lib = L
@@ -321,15 +325,16 @@ def create(inputs, slice_size, R, kind=SCHEME_SINGLE, count=0, cap=0, inner=None
     return out
 
 
-def create_timed(data, slice_size, R, threads=0, want_rec=False):
-    """CPU-baseline create of one in-memory file; (seconds, scan, encode, pkt[, rec])."""
+def create_timed(data, slice_size, R, threads=0, want_rec=False, whole_file_md5=True):
+    """CPU-baseline create of one in-memory file; (seconds, scan, encode, pkt[, rec]).
+    whole_file_md5=False leaves the whole-file MD5 out of the scan."""
     import numpy as np
 
     a, p = _addr(data)
     rec = np.zeros(R * slice_size, dtype=np.uint8) if want_rec else None
     ts, te, tp = C.c_double(), C.c_double(), C.c_double()
-    t = lib().cb_create_timed(p, len(a), slice_size, R, threads, rec.ctypes.data if want_rec else None,
-                              C.byref(ts), C.byref(te), C.byref(tp))
+    t = lib().cb_create_timed_ex(p, len(a), slice_size, R, threads, rec.ctypes.data if want_rec else None,
+                                 C.byref(ts), C.byref(te), C.byref(tp), 1 if whole_file_md5 else 0)
     if want_rec:
         return t, ts.value, te.value, tp.value, rec
     return t, ts.value, te.value, tp.value

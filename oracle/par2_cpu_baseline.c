@@ -175,9 +175,11 @@ static void cb_md5(const uint8_t *d, size_t n, uint8_t out[16]) {
 }
 
 /* scan_via_mmap, src/source.rs:145-232: per-slice hashes on the pool joined
- * with the whole-file hashes on one task. */
-void cb_scan(const uint8_t *data, uint64_t len, uint64_t slice_size, or_slice_checksum *cks,
-             uint8_t hash_full[16], uint8_t hash16k[16], int threads) {
+ * with the whole-file hashes on one task.  whole_file 0 leaves out the
+ * whole-file MD5 (hash_full is then zero): the work a device job does when
+ * that hash is placed on the host. */
+static void cb_scan_ex(const uint8_t *data, uint64_t len, uint64_t slice_size, or_slice_checksum *cks,
+                       uint8_t hash_full[16], uint8_t hash16k[16], int threads, int whole_file) {
     if (threads <= 0) threads = omp_get_max_threads();
     uint64_t n = (len + slice_size - 1) / slice_size;
 #pragma omp parallel num_threads(threads)
@@ -185,7 +187,10 @@ void cb_scan(const uint8_t *data, uint64_t len, uint64_t slice_size, or_slice_ch
     {
 #pragma omp task
         {
-            cb_md5(data, len, hash_full);
+            if (whole_file)
+                cb_md5(data, len, hash_full);
+            else
+                memset(hash_full, 0, 16);
             cb_md5(data, len < 16384 ? len : 16384, hash16k);
         }
 #pragma omp taskloop grainsize(1)
@@ -204,6 +209,11 @@ void cb_scan(const uint8_t *data, uint64_t len, uint64_t slice_size, or_slice_ch
         }
 #pragma omp taskwait
     }
+}
+
+void cb_scan(const uint8_t *data, uint64_t len, uint64_t slice_size, or_slice_checksum *cks,
+             uint8_t hash_full[16], uint8_t hash16k[16], int threads) {
+    cb_scan_ex(data, len, slice_size, cks, hash_full, hash16k, threads, 1);
 }
 
 /* Recovery packet MD5s, one task per volume, serial inside a volume
@@ -252,15 +262,15 @@ static double now_s(void) {
  * all R rows, and the recovery-packet MD5s of an exponential volume split.
  * This is the compute of `par2rust create -s slice -c R` minus file I/O.
  * Returns seconds; `rec_out` (R*slice bytes, may be NULL) receives recovery. */
-double cb_create_timed(const uint8_t *data, uint64_t len, uint64_t slice_size, uint32_t R,
-                       int threads, uint8_t *rec_out, double *t_scan, double *t_encode,
-                       double *t_pkt) {
+double cb_create_timed_ex(const uint8_t *data, uint64_t len, uint64_t slice_size, uint32_t R,
+                          int threads, uint8_t *rec_out, double *t_scan, double *t_encode,
+                          double *t_pkt, int whole_file) {
     if (threads <= 0) threads = omp_get_max_threads();
     uint64_t S = (len + slice_size - 1) / slice_size;
     or_slice_checksum *cks = (or_slice_checksum *)calloc(S, sizeof *cks);
     uint8_t hf[16], h16[16], fid[16], set_id[16];
     double t0 = now_s();
-    cb_scan(data, len, slice_size, cks, hf, h16, threads);
+    cb_scan_ex(data, len, slice_size, cks, hf, h16, threads, whole_file);
     or_file_id(h16, len, (const uint8_t *)"source.bin", 10, fid);
     uint8_t mp[128];
     or_build_main_packet(slice_size, fid, 1, set_id, mp);
@@ -290,6 +300,12 @@ double cb_create_timed(const uint8_t *data, uint64_t len, uint64_t slice_size, u
     if (t_encode) *t_encode = t2 - t1;
     if (t_pkt) *t_pkt = t3 - t2;
     return t3 - t0;
+}
+
+double cb_create_timed(const uint8_t *data, uint64_t len, uint64_t slice_size, uint32_t R,
+                       int threads, uint8_t *rec_out, double *t_scan, double *t_encode,
+                       double *t_pkt) {
+    return cb_create_timed_ex(data, len, slice_size, R, threads, rec_out, t_scan, t_encode, t_pkt, 1);
 }
 
 int cb_max_threads(void) { return omp_get_max_threads(); }
