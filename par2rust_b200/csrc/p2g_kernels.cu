@@ -1319,10 +1319,11 @@ __device__ __noinline__ void batch_packets(const BatchJob& J, uint32_t ring, con
     __syncthreads();
 }
 
-// Chain segment: rows of block q advance over the message blocks that band b
-// completed (set id ‖ type ‖ exponent ‖ row bytes; the last band also pads
-// and writes the digests).  State between bands lives in J.chain.
-__device__ __noinline__ void advance_rows(const BatchJob& J, uint32_t q, uint32_t b, uint32_t ring, const uint32_t* sid) {
+// Chain segment: rows of block q advance over the message blocks that bands
+// b..b_last completed (set id ‖ type ‖ exponent ‖ row bytes; the last band
+// also pads and writes the digests).  State between passes lives in J.chain.
+__device__ __noinline__ void advance_rows(const BatchJob& J, uint32_t q, uint32_t b, uint32_t b_last, uint32_t ring,
+                                          const uint32_t* sid) {
     const int tid = threadIdx.x;
     const uint64_t total = 36 + J.slice;
     const uint64_t nblocks = (total + 8) / 64 + 1;
@@ -1331,9 +1332,9 @@ __device__ __noinline__ void advance_rows(const BatchJob& J, uint32_t q, uint32_
         const uint64_t end = min((uint64_t)Np, (uint64_t)(band + 1) * J.band_syms);
         return min(J.slice, 2 * end);
     };
-    const bool final = b + 1 == J.n_bands;
+    const bool final = b_last + 1 == J.n_bands;
     const uint64_t from = b == 0 ? 0 : (36 + done_bytes(b - 1)) / 64;
-    const uint64_t to = final ? nblocks : (36 + done_bytes(b)) / 64;
+    const uint64_t to = final ? nblocks : (36 + done_bytes(b_last)) / 64;
     const uint32_t r = q * kChainRows + tid;
     if (tid < (int)kChainRows && r < J.R) {
         const uint32_t pre[9] = {sid[0], sid[1], sid[2], sid[3], 0x20524150u, 0x00302E32u, 0x76636552u,
@@ -1364,6 +1365,7 @@ __device__ __noinline__ void advance_rows(const BatchJob& J, uint32_t q, uint32_
 // (a band that became ready while the token was held was left to us).  Each
 // pass either advances at least one band or returns, so this ends.  No CTA
 // waits for another: a busy token means its holder will see the new band.
+constexpr uint32_t kChainBandsPerPass = 16;
 __device__ void try_advance(const BatchJob& J, uint32_t q, uint32_t ring, uint32_t* misc) {
     const int tid = threadIdx.x;
     const uint32_t nb = J.n_bands, Q = (J.R + kChainRows - 1) / kChainRows;
@@ -1381,22 +1383,26 @@ __device__ void try_advance(const BatchJob& J, uint32_t q, uint32_t ring, uint32
         __syncthreads();
         if (!got) return;
         for (;;) {
+            // every band that is ready in a row goes in one pass: one chain
+            // state load and store, one ring start and one hand-over for all
             if (tid == 0) {
                 const uint32_t b = atomicAdd(&next[q], 0u);
+                uint32_t k = 0;
+                while (k < kChainBandsPerPass && ready(b + k)) ++k;
                 misc[3] = b;
-                misc[2] = ready(b) ? 1u : 0u;
+                misc[2] = k;
             }
             __syncthreads();
-            const bool ok = misc[2] != 0;
+            const uint32_t k = misc[2];
             const uint32_t b = misc[3];
-            if (ok && tid < 4) misc[4 + tid] = __ldcg(reinterpret_cast<const uint32_t*>(J.set_id) + tid);
+            if (k && tid < 4) misc[4 + tid] = __ldcg(reinterpret_cast<const uint32_t*>(J.set_id) + tid);
             __syncthreads();
-            if (!ok) break;
-            __threadfence();  // acquire: the band's rows and the set id
-            advance_rows(J, q, b, ring, misc + 4);
+            if (!k) break;
+            __threadfence();  // acquire: the bands' rows and the set id
+            advance_rows(J, q, b, b + k - 1, ring, misc + 4);
             if (tid == 0) {
                 __threadfence();
-                atomicExch(&next[q], b + 1);
+                atomicExch(&next[q], b + k);
             }
             __syncthreads();
         }
