@@ -230,7 +230,11 @@ p2g_status p2g_gf_mul_xor(uint16_t coeff, const uint8_t *input, uint8_t *output,
  * src + s*src_stride (zero-padded slices), recovery row r is written at
  * recovery + r*recovery_stride.  With P2G_DEVICE_POINTERS, src_stride and
  * recovery_stride must be multiples of 16 and both pointers 16-byte
- * aligned, and the work is enqueued on `stream` (0 = legacy default).
+ * aligned, and the work is enqueued on `stream` (0 = legacy default); a
+ * call waits on `stream` for the previous device-pointer call's use of the
+ * library's scratch (coefficient tables, error word), whatever its stream
+ * (not while `stream` is being captured into a graph: captured calls must
+ * not overlap other device-pointer encodes).
  * Device rows are read and written in whole 16-byte units: bytes
  * [slice_size, round_up(slice_size, 16)) of every source row are read --
  * for the last row too, so src must be readable up to

@@ -94,6 +94,10 @@ struct Context {
     static constexpr int kBandEvents = 64;
     cudaStream_t st[kStreams] = {};
     cudaEvent_t ev_fork = nullptr, ev_h16k = nullptr, ev_join[kStreams] = {}, ev_band[kBandEvents] = {};
+    // device-pointer encodes on the caller's stream share the scratch below:
+    // each waits for the previous one's use of it
+    cudaEvent_t ev_scratch = nullptr;
+    bool scratch_pending = false;
     DevBuf src, src_al, rec, basis, checks, h16k, hfull, pkt, spans, err, tmp_in, tmp_out, md5_state;
     DevBuf aimg;       // A operand image of the tensor-core encode
     DevBuf gseg;       // segment table of the one-launch upload of page-locked inputs
@@ -132,6 +136,7 @@ static p2g_status ensure_ready(Context& c) {
         for (int i = 0; i < Context::kStreams; ++i)
             P2G_CU(cudaStreamCreateWithPriority(&c.st[i], cudaStreamNonBlocking, (i == 0 || i == 5) ? lo_pri : hi_pri));
         P2G_CU(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
+        P2G_CU(cudaEventCreateWithFlags(&c.ev_scratch, cudaEventDisableTiming));
         P2G_CU(cudaEventCreateWithFlags(&c.ev_h16k, cudaEventDisableTiming));
         for (auto& ev : c.ev_join) P2G_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         for (auto& ev : c.ev_band) P2G_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -429,7 +434,7 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     uint8_t* D = c.persist.as<uint8_t>();
     uint8_t* H = c.h_persist.as<uint8_t>();
     // basis (precomputed unless P2G_ENCODE_BASIS=derive) and 16-byte aligned slices
-    const bool gen = generate_basis() || mma;  // the tensor-core items take trace strings instead
+    const bool gen = generate_basis() || mma;  // the tensor-core items read their A image instead
     if (j.R && j.S && !gen) P2G_CU(c.basis.ensure(basis_bytes(j.S, RG)));
     if (mma) P2G_CU(c.aimg.ensure(mma_aimg_bytes(j.S, j.R)));
     const uint8_t* esrc = j.d_src;
@@ -1170,6 +1175,12 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
             P2G_CU(cudaMemset2DAsync(jb.recovery, jb.recovery_stride, 0, jb.slice_size, R, s));
             return P2G_OK;
         }
+        // the error word, bases and A image are the library's: a call on
+        // another stream must not overwrite them while an earlier call reads
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        P2G_CU(cudaStreamIsCapturing(s, &cap));
+        const bool order = cap == cudaStreamCaptureStatusNone;  // no outside event inside a capture
+        if (order && c.scratch_pending) P2G_CU(cudaStreamWaitEvent(s, c.ev_scratch, 0));
         P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s));
         if (use_tensor_encode(jb.flags, S, R, jb.slice_size)) {
             P2G_CU(c.aimg.ensure(mma_aimg_bytes(S, R)));
@@ -1183,6 +1194,10 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
             }
             P2G_CU(launch_encode(jb.src, jb.src_stride, S, gen ? nullptr : c.basis.as<uint16_t>(), RG, R,
                                  jb.slice_size, jb.recovery, jb.recovery_stride, c.err.as<int>(), s, jb.first_exponent));
+        }
+        if (order) {
+            P2G_CU(cudaEventRecord(c.ev_scratch, s));
+            c.scratch_pending = true;
         }
         if (jb.flags & P2G_ENCODE_WAIT) {
             P2G_CU(cudaMemcpyAsync(c.h_err.p, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -87,3 +87,33 @@ def test_device_job_on_tensor_cores_matches_oracle(p2g, gpu, oracle, lengths, sl
     bad = parity.check_device_job(files, names, slice_, R, out["rec"], out["checks"], out["hash16k"], bufs.set_id,
                                   out["packet_md5"], hash_full=out["hash_full"])
     assert not bad, bad
+
+
+@pytest.mark.parametrize("variant", ["tensor", "lut"])
+def test_device_encodes_on_two_streams_keep_their_scratch_apart(p2g, gpu, variant):
+    """Two device-pointer encodes with different exponents on two streams,
+    issued back to back: the library's coefficient scratch is shared, so the
+    second waits for the first; each result equals the same encode alone."""
+    import torch
+
+    v = p2g.ENCODE_TENSOR if variant == "tensor" else p2g.ENCODE_LUT
+    S, sl, R = 96, 65536, 40
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    src = torch.randint(0, 256, (S * sl,), dtype=torch.uint8, device="cuda", generator=g)
+    alone = []
+    for fe in (0, 9000):
+        out = torch.zeros(R * sl, dtype=torch.uint8, device="cuda")
+        p2g.encode_device(src.data_ptr(), sl, S, sl, R, out.data_ptr(), sl, torch.cuda.current_stream().cuda_stream,
+                          variant=v, wait=True, first_exponent=fe)
+        alone.append(out)
+    torch.cuda.synchronize()
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    a = torch.zeros(R * sl, dtype=torch.uint8, device="cuda")
+    b = torch.zeros(R * sl, dtype=torch.uint8, device="cuda")
+    for _ in range(3):
+        p2g.encode_device(src.data_ptr(), sl, S, sl, R, a.data_ptr(), sl, s1.cuda_stream, variant=v, first_exponent=0)
+        p2g.encode_device(src.data_ptr(), sl, S, sl, R, b.data_ptr(), sl, s2.cuda_stream, variant=v,
+                          first_exponent=9000)
+    torch.cuda.synchronize()
+    assert torch.equal(a, alone[0]) and torch.equal(b, alone[1])
