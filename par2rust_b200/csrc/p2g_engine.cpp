@@ -428,8 +428,11 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
     const size_t o_files = take(16ull * n), o_noff = take(8ull * n), o_names = take(names_bytes);
     const size_t o_scratch = take(32ull * n + 12), o_sid = take(16);
     const size_t host_bytes = o_ctl;  // descriptor and items staged together
+    // the staging buffer may still feed the previous call's copies, and the
+    // device scratch (descriptor, A image, bases) its kernels, on any stream
+    if (c.scratch_pending) P2G_CU(cudaEventSynchronize(c.ev_scratch));
+    P2G_CU(cudaStreamSynchronize(st));
     P2G_CU(c.persist.ensure(off));
-    P2G_CU(cudaStreamSynchronize(st));  // the staging buffer may still feed the previous call's copies
     P2G_CU(c.h_persist.ensure(off));
     uint8_t* D = c.persist.as<uint8_t>();
     uint8_t* H = c.h_persist.as<uint8_t>();
@@ -521,6 +524,8 @@ static p2g_status run_device_job_persistent(Context& c, DeviceJob& j, cudaStream
                         (uint32_t)pl.items.size(), reinterpret_cast<uint32_t*>(D + o_ctl), err,
                         (uint32_t)device_sm_count(), st, mma));
     P2G_CU(cudaMemcpyAsync(c.h_err.p, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    P2G_CU(cudaEventRecord(c.ev_scratch, st));
+    c.scratch_pending = true;
     if (j.progress && j.R && j.S) P2G_TRY(poll_progress(c, j, pl, reinterpret_cast<const uint32_t*>(D + o_ctl), st));
     if (!j.have_set_id) {
         // set id = MD5(main packet body) over the sorted file ids

@@ -117,3 +117,32 @@ def test_device_encodes_on_two_streams_keep_their_scratch_apart(p2g, gpu, varian
                           first_exponent=9000)
     torch.cuda.synchronize()
     assert torch.equal(a, alone[0]) and torch.equal(b, alone[1])
+
+
+def test_device_jobs_on_two_streams_keep_their_scratch_apart(p2g, gpu):
+    """Two device jobs (different sources) issued back to back on two streams
+    share the library's descriptor, A image and staging buffers: each must
+    give what it gives alone."""
+    import torch
+
+    sl, L = 65536, 96 * 65536 - 1000
+    S = (L + sl - 1) // sl
+    srcs = []
+    for seed in (1, 2):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        t = torch.zeros(S * sl, dtype=torch.uint8, device="cuda")
+        t[:L] = torch.randint(0, 256, (L,), dtype=torch.uint8, device="cuda", generator=g)
+        srcs.append(t)
+    alone = []
+    for t in srcs:
+        bufs = p2g.run_device_job(t, [L], [b"f.bin"], sl, 40, skip_hash_full=True)
+        torch.cuda.synchronize()
+        alone.append((bufs.recovery.clone(), bufs.packet_md5.clone(), bufs.checksums.clone()))
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    got = []
+    for t, st in zip(srcs, (s1, s2)):
+        got.append(p2g.run_device_job(t, [L], [b"f.bin"], sl, 40, stream=st.cuda_stream, skip_hash_full=True))
+    torch.cuda.synchronize()
+    for b, (rec, pkt, cks) in zip(got, alone):
+        assert torch.equal(b.recovery, rec) and torch.equal(b.packet_md5, pkt) and torch.equal(b.checksums, cks)
