@@ -1211,9 +1211,11 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
         }
         return P2G_OK;
     }
-    // host pointers: stage through device buffers
+    // host pointers: stage through device buffers (after any earlier call's
+    // use of the shared scratch, whatever its stream)
     const uint64_t stride = round_up(jb.slice_size, 16);
     cudaStream_t s = c.st[0];
+    if (c.scratch_pending) P2G_CU(cudaStreamWaitEvent(s, c.ev_scratch, 0));
     P2G_CU(c.src.ensure((size_t)stride * std::max<uint32_t>(S, 1)));
     P2G_CU(c.rec.ensure((size_t)stride * R));
     P2G_CU(cudaMemsetAsync(c.err.p, 0, sizeof(int), s));
@@ -1241,6 +1243,7 @@ extern "C" p2g_status p2g_encode(const p2g_encode_job* job) {
                              cudaMemcpyDeviceToHost, s));
     P2G_CU(cudaMemcpyAsync(c.h_err.p, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     P2G_CU(cudaStreamSynchronize(s));
+    c.scratch_pending = false;  // all of it is done
     return check_device_error(c);
 }
 
