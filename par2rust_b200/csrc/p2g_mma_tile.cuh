@@ -417,9 +417,13 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
                     uint32_t v[32];
                     tmem_ld32(P.tmem + ((32 * q) << 16) + t * kAccCol1 + c0, v);
                     uint32_t mine = 0;
+                    // parity of each count: the counts are integers below
+                    // 16 * 32768 = 2^19, so in count + 2^23 the mantissa's
+                    // lowest bit is the count's (one add, no conversion)
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
-                        const uint32_t b = __ballot_sync(0xFFFFFFFFu, __float2uint_rz(__uint_as_float(v[j])) & 1u);
+                        const uint32_t par = __float_as_uint(__uint_as_float(v[j]) + 8388608.0f) & 1u;
+                        const uint32_t b = __ballot_sync(0xFFFFFFFFu, par);
                         if (lane == j) mine = b;
                     }
                     // ballot lanes 0-15: the bits of row ra, lanes 16-31: row rb
