@@ -1111,8 +1111,9 @@ size_t batch_smem_bytes() { return kBatchSmem; }
 
 // One tensor-core item of the batch kernel, all threads: 14 operand-building
 // warps (warps 2..15).  Kept out of line, with its pipeline state in shared
-// memory (words [2..5] past the barriers: K-steps, tiles, drains, input
-// stages), so that it adds no registers to the other item kinds.
+// memory (words [2..6] past the barriers: operand stages, tiles, drains,
+// input stages, stages issued ahead), so that it adds no registers to the
+// other item kinds.
 __device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ Jp, const uint16_t* __restrict__ ginv,
                                             uint32_t kind_rg, uint32_t a, uint32_t b, uint32_t s0, uint32_t sn) {
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -1135,6 +1136,7 @@ __device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ Jp, con
     P.tcount = mm[3];
     P.drains = mm[4];
     P.gi = mm[5];
+    P.pre = mm[6];
     if (threadIdx.x == 0) mma::tensormap_acquire(&J.src_map);  // written by the host's upload of the jobs
     mma::Tile T;
     T.src_map = &J.src_map;
@@ -1155,6 +1157,7 @@ __device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ Jp, con
         mm[3] = P.tcount;
         mm[4] = P.drains;
         mm[5] = P.gi;
+        mm[6] = P.pre;
     }
     __syncthreads();
     return ok;
@@ -1441,14 +1444,14 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     const int tid = threadIdx.x;
     // tensor-core items (mma_ginv set): TMEM for the whole launch, barriers
     // and scale factors set up once.  mma_misc: [0] TMEM address, [1] abort
-    // flag, [2..5] pipeline state.
+    // flag, [2..6] pipeline state.
     uint32_t* mma_misc = reinterpret_cast<uint32_t*>(smem + kBatchMmaBarsOff + mma::kBarBytes);
     const uint32_t mma_bars = smem_u32(smem + kBatchMmaBarsOff);
     if (tid == 0) {
         for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
         if (MMA) {
             mma::init_bars(mma_bars, 14);
-            mma_misc[1] = mma_misc[2] = mma_misc[3] = mma_misc[4] = mma_misc[5] = 0;
+            mma_misc[1] = mma_misc[2] = mma_misc[3] = mma_misc[4] = mma_misc[5] = mma_misc[6] = 0;
         }
         fence_mbar_init();
     }

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     P.bars = smem_addr(smem + kOffBars);
     P.ginv = ginv;
     P.abort_flag = misc + 1;
-    P.g = P.gi = P.tcount = P.drains = 0;
+    P.g = P.gi = P.tcount = P.drains = P.pre = 0;
     if (tid == 0) {
         init_bars(P.bars, kGenWarps);
         misc[1] = 0;
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     // tiles in order of symbol tile, row tile fastest: concurrent CTAs share
     // their source bytes in L2
     bool ok = true;
-    for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
+    auto tile_of = [&](uint32_t tile) {
         Tile T;
         T.src_map = &src_map;
         T.aimg = aimg;
@@ -157,7 +157,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         T.n0 = (tile / n_row_tiles) * kN;
         T.syms = min(kN, Np - T.n0);
         T.accumulate = 0;
-        ok = run_tile<kGenWarps>(P, T);
+        return T;
+    };
+    for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
+        const Tile T = tile_of(tile);
+        const bool more = tile + gridDim.x < n_tiles;
+        const Tile Tn = tile_of(more ? tile + gridDim.x : tile);
+        ok = run_tile<kGenWarps>(P, T, more ? &Tn : nullptr);
     }
     if (tid == 0 && !ok) atomicOr(err, 1);
     tc_fence_before();

@@ -258,6 +258,7 @@ struct Pipe {
     const uint16_t* ginv;  // shared memory
     volatile uint32_t* abort_flag;
     uint32_t g, gi, tcount, drains;
+    uint32_t pre;  // input stages of the coming tile already issued by the previous call
 };
 
 // All threads of the CTA call this.  Warp 0 lane 0 streams the inputs, warp
@@ -266,8 +267,11 @@ struct Pipe {
 // 32*(w%4)..).  Other warps idle.  Returns false (uniformly, after a CTA
 // barrier) when a bounded wait gave up; copies and MMAs in flight have then
 // landed.
+// next (may be null): the tile this CTA runs after this one; the producer
+// issues its first input stages while this tile's last K-steps and
+// epilogue run, so the next tile starts without a copy round trip.
 template <int NGEN>
-__device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
+__device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T, const Tile* next = nullptr) {
     static_assert(NGEN >= 8, "eight warps cover the two accumulators' four lane quadrants");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const Bars B(P.bars);
@@ -278,25 +282,38 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
     // a tensor copy's x offset must be 16-byte aligned, the A image is cut in
     // whole input stages (the same in every thread)
     if ((T.n0 & 7u) || (T.s0 % kInSlices)) return false;
+    const bool ahead = next && !(next->n0 & 7u) && !(next->s0 % kInSlices);
+    const uint32_t NI_next =
+        ahead ? ((next->sn + kKSlices - 1) / kKSlices + kInSteps - 1) / kInSteps : 0u;
+    const uint32_t pre_next = NI_next < (uint32_t)kInStages ? NI_next : (uint32_t)kInStages;
     bool ok = true;
     if (warp == 0) {
         if (lane == 0) {
-            uint32_t gi = gi0;
-            for (uint32_t k = 0; k < NI; ++k, ++gi) {
-                const uint32_t st = gi % kInStages;
-                if (!bar_wait(B.in_empty + 8 * st, ((gi / kInStages) & 1u) ^ 1u, P.abort_flag)) {
+            // stages [0, P.pre) of this tile went out with the previous tile
+            uint32_t gi = gi0 + P.pre;
+            auto issue = [&](const Tile& U, uint32_t rtu, uint32_t k, uint32_t gi_) {
+                const uint32_t st = gi_ % kInStages;
+                if (!bar_wait(B.in_empty + 8 * st, ((gi_ / kInStages) & 1u) ^ 1u, P.abort_flag)) return false;
+                const uint32_t sa = U.s0 + k * kInSlices;
+                const uint32_t dst = in0 + st * kInStageBytes;
+                bar_expect_tx(B.in_full + 8 * st, kInStageBytes);
+                tma_1d(dst, U.aimg + ((size_t)rtu * U.ksteps + sa / kKSlices) * kAStepBytes, kInABytes,
+                       B.in_full + 8 * st);
+                tma_2d(dst + kInABytes, U.src_map, (int32_t)U.n0, (int32_t)sa, B.in_full + 8 * st);
+                return true;
+            };
+            // slices past the tile's range (up to 15) are copied too: the
+            // builders mask their B rows
+            for (uint32_t k = P.pre; k < NI; ++k, ++gi)
+                if (!issue(T, rt, k, gi)) {
                     ok = false;
                     break;
                 }
-                const uint32_t sa = T.s0 + k * kInSlices;
-                const uint32_t dst = in0 + st * kInStageBytes;
-                // slices past the tile's range (up to 15) are copied too: the
-                // builders mask their B rows
-                bar_expect_tx(B.in_full + 8 * st, kInStageBytes);
-                tma_1d(dst, T.aimg + ((size_t)rt * T.ksteps + sa / kKSlices) * kAStepBytes, kInABytes,
-                       B.in_full + 8 * st);
-                tma_2d(dst + kInABytes, T.src_map, (int32_t)T.n0, (int32_t)sa, B.in_full + 8 * st);
-            }
+            for (uint32_t k = 0; ok && k < pre_next; ++k, ++gi)
+                if (!issue(*next, next->r0 / kTileRows, k, gi)) {
+                    ok = false;
+                    break;
+                }
             if (!ok)  // copies issued but maybe not consumed land before the stages are reused
                 for (uint32_t q = gi > gi0 + kInStages ? gi - kInStages : gi0; q < gi; ++q)
                     bar_drain(B.in_full + 8 * (q % kInStages), (q / kInStages) & 1u);
@@ -455,6 +472,7 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T) {
     const bool bad = __syncthreads_or(!ok) != 0;
     P.g += NS;
     P.gi += NI;
+    P.pre = bad ? 0u : pre_next;
     P.tcount += 1;
     if (bad) P.drains += 1;
     return !bad;
