@@ -433,3 +433,20 @@ def test_batch_validation(p2g, gpu, batch_jobs):
     with pytest.raises(p2g.InvalidSliceSize):
         p2g.Batch([p2g.BatchJobSpec(spec.src, [10], [b"x"], 4098, 4, spec.bufs)])
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("slice_,S,R,want", [
+    (524288, 1027, 200, "tensor"),   # the 538 MB job: 5.4 ms on the tensor cores against 9.0 ms
+    (262144, 8723, 2000, "tensor"),  # many_2000's shape
+    (524288, 1027, 16, "tensor"),    # 0.49 ms against 1.01 ms
+    (262144, 64, 32, "lut"),         # small: 0.084 ms on the lookup kernel against 0.107 ms
+    (4096, 40, 3, "lut"),
+])
+def test_planner_picks_the_encode_kernel_by_shape(p2g, monkeypatch, slice_, S, R, want):
+    """With no flag or environment override, the single-job planner puts the
+    encode on the kernel its cost model finds faster for the shape (measured
+    times in the comments); tensor-core items report fold 0."""
+    monkeypatch.delenv("P2G_ENCODE_VARIANT", raising=False)
+    items, _, _ = p2g.plan_device_job(slice_, S, R)
+    got = "tensor" if items[0]["fold"] == 0 else "lut"
+    assert got == want, (slice_, S, R, got)
