@@ -452,7 +452,12 @@ p2g_status p2g_plan_device_job(uint64_t slice_size, uint32_t input_slices, uint3
  * work overlaps.  Outputs (as for p2g_batch_job, hash_full excluded) stay in
  * device memory until the caller releases the job.  A scheduler thread
  * inside the library drives admission and waves; all calls are thread-safe.
- * Each job's outputs are byte-identical to the same job run alone. */
+ * A job's encode runs on the tensor cores when the cost model prefers that
+ * and its coefficient image (recovery_count x input slices x 128 bytes,
+ * counted in its footprint) is at most a quarter of its source bytes, else
+ * on the lookup kernel; P2G_ENCODE_VARIANT=lut|tensor in the environment
+ * overrides the preference.  Each job's outputs are byte-identical to the
+ * same job run alone. */
 typedef struct p2g_server p2g_server;   /* opaque */
 typedef struct p2g_server_options {
     uint64_t hbm_budget;                /* bytes of source + recovery resident jobs may hold (0: 120e9) */
