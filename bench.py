@@ -424,14 +424,59 @@ def serve_cpu_baseline(jobs, target_s, threads=0):
                       "buffer (scan + encode + packet MD5s)", "seconds": spent}, spent
 
 
-def serve_run(srv, jobs, arrivals, p2g):
+def serve_parity_pick(jobs, n_sample=8, max_bytes=64 << 20, max_macs=2e11, seed=5):
+    """A seeded sample of requests whose oracle check stays cheap (source
+    and CPU encode bounded), always including the smallest request."""
+    import random
+
+    cost = lambda j: j.slices * j.recovery * (j.slice_size // 2)
+    cand = [k for k, j in enumerate(jobs) if j.source_bytes <= max_bytes and cost(j) <= max_macs / n_sample]
+    if not cand:
+        return set()
+    pick = set(random.Random(seed).sample(cand, min(n_sample, len(cand))))
+    pick.add(min(cand, key=lambda k: jobs[k].source_bytes))
+    return pick
+
+
+def serve_parity(jobs, kept):
+    """Oracle check of the sampled requests' outputs as the serving loop
+    returned them mid-sweep: every recovery row (GFNI port), slice MD5/CRC32,
+    hash16k, set id and packet MD5."""
+    import numpy as np
+
+    from oracle import parity
+    from par2rust_b200 import workloads as W
+
+    t0 = time.perf_counter()
+    bad = {}
+    for i, out in sorted(kept.items()):
+        j = jobs[i]
+        R, n, sl = j.recovery, len(j.file_lengths), j.slice_size
+        files = [W.file_bytes(sd, ln) for ln, sd in zip(j.file_lengths, j.seeds)]
+        names = [f"req{i:05d}_f{k:02d}.bin".encode() for k in range(n)]
+        rec = (np.frombuffer(b"".join(out["recovery"]), np.uint8).reshape(R, sl) if R
+               else np.zeros((0, sl), np.uint8))
+        b = parity.check_device_job(files, names, sl, R, rec, np.frombuffer(out["checksums"], np.uint8),
+                                    np.frombuffer(out["hash16k"], np.uint8).reshape(n, 16), out["set_id"],
+                                    np.frombuffer(out["packet_md5"], np.uint8))
+        if b:
+            bad[i] = b[:5]
+    return {"result": "bit-exact" if not bad else "MISMATCH", "requests_checked": sorted(kept),
+            "source_bytes_checked": sum(jobs[i].source_bytes for i in kept), "seconds": time.perf_counter() - t0,
+            "mismatches": bad}
+
+
+def serve_run(srv, jobs, arrivals, p2g, keep=()):
     """Open loop: submit job i at arrivals[i] (server clock from now), a
     poller thread reads each completed job's set id and packet MD5s back and
-    releases it.  Returns per-job latencies and totals."""
+    releases it; for the requests in `keep` it first copies every output to
+    the host (returned under "kept", for the oracle check after the run).
+    Returns per-job latencies and totals."""
     import threading
 
     n = len(jobs)
     lat, done_bytes, d2h = [], [0], [0]
+    kept = {}
     last_done = [0.0]
     finished = threading.Event()
 
@@ -445,9 +490,13 @@ def serve_run(srv, jobs, arrivals, p2g):
                     got += 1
                     if r.status != 0:
                         raise RuntimeError(f"request {r.tag} failed with status {r.status}")
-                    p2g.copy_to_host(r.ptr["set_id"], 16)
-                    p2g.copy_to_host(r.ptr["packet_md5"], 16 * r.recovery_count)
-                    d2h[0] += 16 + 16 * r.recovery_count
+                    if r.tag in keep:
+                        kept[r.tag] = out = srv.outputs(r)
+                        d2h[0] += sum(len(v) if isinstance(v, bytes) else sum(map(len, v)) for v in out.values())
+                    else:
+                        p2g.copy_to_host(r.ptr["set_id"], 16)
+                        p2g.copy_to_host(r.ptr["packet_md5"], 16 * r.recovery_count)
+                        d2h[0] += 16 + 16 * r.recovery_count
                     srv.release(r.ticket)
                     lat.append(r.done_s - r.submit_s)
                     done_bytes[0] += r.source_bytes
@@ -478,11 +527,11 @@ def serve_run(srv, jobs, arrivals, p2g):
     pct = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
     return {"requests": n, "source_bytes": done_bytes[0], "seconds": span, "gbs": done_bytes[0] / span / 1e9,
             "jobs_per_s": n / span, "p50_ms": pct(0.50) * 1e3, "p99_ms": pct(0.99) * 1e3,
-            "mean_ms": sum(lat) / len(lat) * 1e3, "max_ms": lat[-1] * 1e3, "d2h_bytes": d2h[0]}
+            "mean_ms": sum(lat) / len(lat) * 1e3, "max_ms": lat[-1] * 1e3, "d2h_bytes": d2h[0], "kept": kept}
 
 
 def bench_serve(requests, rate_fracs=(0.5, 0.8, 0.95), rates=None, probe_jobs=200, wave_ms=20.0, seed=5,
-                local=0):
+                local=0, check_parity=True):
     """The serving loop on the request mix: a closed-batch capacity probe,
     then open-loop Poisson arrivals at each rate (fractions of that capacity
     unless explicit rates are given).  Returns the sweep and its clocks."""
@@ -496,12 +545,15 @@ def bench_serve(requests, rate_fracs=(0.5, 0.8, 0.95), rates=None, probe_jobs=20
     clocks.start()
     probe = jobs[:min(probe_jobs, len(jobs))]
     pr = serve_run(srv, probe, [0.0] * len(probe), p2g)
+    pr.pop("kept")
     cap_jobs = pr["jobs_per_s"]
     rates = list(rates) if rates else [f * cap_jobs for f in rate_fracs]
-    sweep = []
+    keep = serve_parity_pick(jobs, seed=seed) if check_parity else set()
+    sweep, kept = [], []
     for ri, rate in enumerate(rates):
         arr = W.poisson_arrivals(len(jobs), rate, seed=100 + ri)
-        res = serve_run(srv, jobs, arr, p2g)
+        res = serve_run(srv, jobs, arr, p2g, keep=keep)
+        kept.append(res.pop("kept"))
         res["rate_jobs_per_s"] = rate
         res["offered_gbs"] = rate * sum(j.source_bytes for j in jobs) / len(jobs) / 1e9
         st = srv.stats()
@@ -512,6 +564,10 @@ def bench_serve(requests, rate_fracs=(0.5, 0.8, 0.95), rates=None, probe_jobs=20
     clk = clocks.stop()
     waves = srv.stats()["waves"]
     srv.close()
+    for res, kp in zip(sweep, kept):  # outside the sweep: the oracle runs on the host
+        res["parity"] = serve_parity(jobs, kp) if keep else None
+    parity_all = (None if not keep else
+                  "bit-exact" if all(r["parity"]["result"] == "bit-exact" for r in sweep) else "MISMATCH")
     return {
         "workload": f"serve: {len(jobs)} requests per rate, totals log-uniform [1 MiB, 2 GiB] in 1-32 files, "
                     "slice {16K,64K,256K,1M} (smallest with <= 32768 slices), R 1-20% of slices, Poisson arrivals",
@@ -519,7 +575,10 @@ def bench_serve(requests, rate_fracs=(0.5, 0.8, 0.95), rates=None, probe_jobs=20
         "total_source_bytes": sum(j.source_bytes for j in jobs), "capacity_probe": pr, "sweep": sweep,
         "p50_ms": [r["p50_ms"] for r in sweep], "p99_ms": [r["p99_ms"] for r in sweep],
         "rates_jobs_per_s": [r["rate_jobs_per_s"] for r in sweep], "gbs": [r["gbs"] for r in sweep],
-        "clocks": clk, "waves": waves, "jobs": jobs,
+        "clocks": clk, "waves": waves, "jobs": jobs, "parity": parity_all,
+        "parity_what": "per rate, a seeded sample of requests (source <= 64 MiB) keeps every output; each is "
+                       "checked against the oracle after the sweep: every recovery row, slice MD5/CRC32, hash16k, "
+                       "set id and packet MD5",
     }
 
 
@@ -530,7 +589,7 @@ def run_serve(args, wl):
     torch.cuda.set_device(local)
     rates = [float(x) for x in args.rates.split(",") if x]
     res = bench_serve(args.requests, rates=rates, probe_jobs=args.probe_jobs, wave_ms=args.wave_ms, seed=wl["seed"],
-                      local=local)
+                      local=local, check_parity=not args.no_parity)
     jobs = res.pop("jobs")
     cb = None
     if not args.no_cpu_baseline:
@@ -544,7 +603,7 @@ def run_serve(args, wl):
         "config": {"workload": res["workload"], "hbm_budget_bytes": res["hbm_budget_bytes"], "wave_ms": args.wave_ms,
                    "total_source_bytes": res["total_source_bytes"], "parallelism": "1 GPU"},
         "capacity_probe": res["capacity_probe"], "sweep": res["sweep"],
-        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
+        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "parity": res["parity"],
         "e2e": {"value": top["gbs"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": top["d2h_bytes"],
                 "note": "host clock from each request's submit to its completion; sources generated on the device"},
         "roofline": None, "cpu_baseline": cb, "clocks": res["clocks"], "gpu_launches": res["waves"],
@@ -1017,7 +1076,7 @@ def main():
     serving = None
     if world == 1 and args.serve_requests > 0:
         serving = bench_serve(args.serve_requests, rate_fracs=tuple(float(x) for x in args.serve_fracs.split(",")),
-                              local=local)
+                              local=local, check_parity=not args.no_parity)
         serving.pop("jobs")
 
     # ---- CPU baseline (rank 0, N=1) ----
