@@ -91,6 +91,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void fence_mbar_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
+// Ends an mbarrier object's life, so that its bytes may hold other data.
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
@@ -1095,37 +1099,78 @@ constexpr int kBatchRingAhead = 4;
 constexpr int kBatchRingLane = kBatchRingUnits * 64 + 16;
 constexpr size_t kBatchRingBytes = (size_t)kHashThreads * kBatchRingLane;
 // Tensor-core items reuse the encode region and the MD5 rings for their
-// operand and input rings and the G^-1 tables; their barriers, the TMEM
-// address, an abort flag and the pipeline state live past the other regions,
-// so they persist across items.
-constexpr size_t kBatchMmaBarsOff = kBatchEncBytes + kBatchRingBytes + 4 * 256 * 4 + 64;
+// operand and input rings; their barriers, the TMEM address, an abort flag,
+// the pipeline state and the G^-1 tables live past the other regions, so
+// they persist across items.  The MD5 rings start past the tensor-core input
+// stages: a tile's producer issues the next tile's first input stages before
+// the CTA has counted the tile's band, and the packet-MD5 chains that a band
+// completes run on the rings meanwhile (the rings then overlap only operand
+// stages, which are idle between tiles).
+constexpr size_t kBatchRingOff = ((kBatchEncBytes > (size_t)mma::kInStages * mma::kInStageBytes
+                                       ? kBatchEncBytes
+                                       : (size_t)mma::kInStages * mma::kInStageBytes) + 15) / 16 * 16;
+constexpr size_t kBatchMmaBarsOff = kBatchRingOff + kBatchRingBytes + 4 * 256 * 4 + 64;
 // the G^-1 tables of tensor-core items, copied once per launch, after the
 // pipeline state words
 constexpr size_t kBatchGinvOff = kBatchMmaBarsOff + mma::kBarBytes + 32;
-constexpr size_t kBatchSmem = kBatchGinvOff + mma::kGinvBytes;
-static_assert(kBatchEncBytes % 16 == 0, "MD5 rings must start 16-byte aligned");
-static_assert(mma::kRingBytes + mma::kGinvBytes <= kBatchEncBytes + kBatchRingBytes,
+// the next tile a tensor-core tile's producer claimed (one mma::Tile)
+constexpr size_t kBatchNextTileOff = (kBatchGinvOff + mma::kGinvBytes + 15) / 16 * 16;
+constexpr size_t kBatchSmem = kBatchNextTileOff + 64;
+static_assert(sizeof(mma::Tile) <= 64 && kBatchNextTileOff % 16 == 0, "next-tile slot");
+static_assert(kBatchEncBytes % 16 == 0 && kBatchRingOff % 16 == 0, "MD5 rings must start 16-byte aligned");
+static_assert(mma::kRingBytes <= kBatchRingOff + kBatchRingBytes,
               "tensor-core rings fit the encode region and the MD5 rings");
 static_assert(kBatchMmaBarsOff % 8 == 0 && kBatchSmem <= 227 * 1024, "batch shared memory");
 size_t batch_smem_bytes() { return kBatchSmem; }
+
+// The tile of a tensor-core item.
+__device__ __forceinline__ mma::Tile batch_mma_tile_of(const BatchJob& J, const BatchItem& it) {
+    mma::Tile T;
+    T.src_map = &J.src_map;
+    T.aimg = J.aimg;
+    T.rec = J.rec;
+    T.rec_stride = J.rec_stride;
+    T.s0 = it.s0;
+    T.sn = it.sn ? it.sn : J.S - it.s0;
+    T.ksteps = J.ksteps;
+    T.R = J.R;
+    T.r0 = ((it.kind_rg >> 8) & 0xFFFFu) * kMmaTileRows;
+    T.n0 = it.a;
+    T.syms = it.b & 0xFFFFu;
+    T.accumulate = (it.kind_rg & kItemAccumulate) ? 1u : 0u;
+    return T;
+}
 
 // One tensor-core item of the batch kernel, all threads: 14 operand-building
 // warps (warps 2..15).  Kept out of line, with its pipeline state in shared
 // memory (words [2..6] past the barriers: operand stages, tiles, drains,
 // input stages, stages issued ahead), so that it adds no registers to the
 // other item kinds.
-__device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ Jp, const uint16_t* __restrict__ ginv,
-                                            uint32_t kind_rg, uint32_t a, uint32_t b, uint32_t s0, uint32_t sn) {
+//
+// The CTA's next item is claimed from the queue here, by the producer thread
+// once it has issued this tile's last input stage (a few K-steps before the
+// tile ends, about when the CTA would otherwise claim it); its index goes to
+// *held (shared memory, read by every thread after this returns) and its
+// first input stages are issued at once.  Nothing is claimed ahead
+// (held = kNoHeldItem) once the error flag is set, when the queue head is not
+// a tensor-core item, or when fewer than kClaimMargin other tiles of this
+// tile's band are unfinished: the CTA that completes a band runs its
+// packet-MD5 chains next, and a claimed item would wait behind them.
+constexpr uint32_t kNoHeldItem = 0xFFFFFFFFu;
+constexpr uint32_t kClaimMargin = 8;
+__device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ jobs, const BatchItem* __restrict__ items,
+                                            uint32_t n_items, uint32_t* __restrict__ ctl, const int* err,
+                                            uint32_t idx, uint32_t* held) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint32_t* mm = reinterpret_cast<uint32_t*>(smem + kBatchMmaBarsOff + mma::kBarBytes);
-    (void)ginv;
     const uint16_t* gsm = reinterpret_cast<const uint16_t*>(smem + kBatchGinvOff);  // filled at launch start
     // Earlier items stored to this shared memory through the generic proxy;
     // the tile's bulk and tensor copies write it through the async proxy.
     // Order the two before any copy is issued.
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    const BatchJob& J = *Jp;
+    const BatchItem it = items[idx];
+    const BatchJob& J = jobs[it.job];
     mma::Pipe P;
     P.ring = smem_u32(smem);
     P.bars = smem_u32(smem + kBatchMmaBarsOff);
@@ -1138,20 +1183,30 @@ __device__ __noinline__ bool batch_mma_tile(const BatchJob* __restrict__ Jp, con
     P.gi = mm[5];
     P.pre = mm[6];
     if (threadIdx.x == 0) mma::tensormap_acquire(&J.src_map);  // written by the host's upload of the jobs
-    mma::Tile T;
-    T.src_map = &J.src_map;
-    T.aimg = J.aimg;
-    T.rec = J.rec;
-    T.rec_stride = J.rec_stride;
-    T.s0 = s0;
-    T.sn = sn ? sn : J.S - s0;
-    T.ksteps = J.ksteps;
-    T.R = J.R;
-    T.r0 = ((kind_rg >> 8) & 0xFFFFu) * kMmaTileRows;
-    T.n0 = a;
-    T.syms = b & 0xFFFFu;
-    T.accumulate = (kind_rg & kItemAccumulate) ? 1u : 0u;
-    const bool ok = mma::run_tile<14>(P, T);  // ends with a CTA barrier
+    const mma::Tile T = batch_mma_tile_of(J, it);
+    // producer thread only (thread 0); the tile goes to its shared-memory slot
+    auto claim_next = [&]() -> const mma::Tile* {
+        *held = kNoHeldItem;
+        if (*reinterpret_cast<const volatile int*>(err)) return nullptr;
+        if (J.n_bands) {
+            const uint32_t band = it.b >> 16;
+            const uint32_t done = *reinterpret_cast<const volatile uint32_t*>(&J.bstate[band]);
+            if (done + kClaimMargin >= J.band_items[band]) return nullptr;
+        }
+        const uint32_t h = *reinterpret_cast<const volatile uint32_t*>(&ctl[0]);
+        if (h >= n_items || (items[h].kind_rg & kItemKindMask) != kItemEncodeMma) return nullptr;
+        const uint32_t nidx = atomicAdd(&ctl[0], 1u);
+        *held = nidx;
+        if (nidx >= n_items) return nullptr;
+        const BatchItem nit = items[nidx];
+        if ((nit.kind_rg & kItemKindMask) != kItemEncodeMma) return nullptr;
+        const BatchJob& Jn = jobs[nit.job];
+        mma::tensormap_acquire(&Jn.src_map);
+        mma::Tile* slot = reinterpret_cast<mma::Tile*>(smem + kBatchNextTileOff);
+        *slot = batch_mma_tile_of(Jn, nit);
+        return slot;
+    };
+    const bool ok = mma::run_tile<14>(P, T, claim_next);  // ends with a CTA barrier
     if (threadIdx.x == 0) {
         mm[2] = P.g;
         mm[3] = P.tcount;
@@ -1437,9 +1492,10 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* enc = smem;
     uint64_t* bars = reinterpret_cast<uint64_t*>(enc + encode_bars_offset<kEncChunks, 4, kBatchEncStages>());
-    uint8_t* ring_p = smem + kBatchEncBytes;
+    uint8_t* ring_p = smem + kBatchRingOff;
     uint32_t(*T)[256] = reinterpret_cast<uint32_t(*)[256]>(ring_p + kBatchRingBytes);
-    uint32_t* misc = reinterpret_cast<uint32_t*>(ring_p + kBatchRingBytes + 4 * 256 * 4);  // [0] item [1] last [4..7] set id
+    // [0] item [1] last [2..3] chain tokens [4..7] set id [8] item claimed ahead by a tensor-core tile
+    uint32_t* misc = reinterpret_cast<uint32_t*>(ring_p + kBatchRingBytes + 4 * 256 * 4);
     const uint32_t ring = smem_u32(ring_p);
     const int tid = threadIdx.x;
     // tensor-core items (mma_ginv set): TMEM for the whole launch, barriers
@@ -1447,8 +1503,14 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     // flag, [2..6] pipeline state.
     uint32_t* mma_misc = reinterpret_cast<uint32_t*>(smem + kBatchMmaBarsOff + mma::kBarBytes);
     const uint32_t mma_bars = smem_u32(smem + kBatchMmaBarsOff);
+    // The lookup items' barriers lie inside the tensor-core input stages.
+    // Launches with tensor-core items set them up only around a lookup item
+    // and invalidate them after it (an mbarrier's bytes may hold other data
+    // only once it is invalidated); such launches plan no lookup items.
     if (tid == 0) {
-        for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
+        misc[8] = kNoHeldItem;
+        if (!MMA)
+            for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
         if (MMA) {
             mma::init_bars(mma_bars, 14);
             mma_misc[1] = mma_misc[2] = mma_misc[3] = mma_misc[4] = mma_misc[5] = mma_misc[6] = 0;
@@ -1469,7 +1531,15 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     }
     uint32_t phase = 0;
     for (;;) {
-        if (tid == 0) misc[0] = *reinterpret_cast<volatile int*>(err) ? n_items : atomicAdd(&ctl[0], 1u);
+        if (tid == 0) {
+            // an item a tensor-core tile claimed ahead runs next whatever the
+            // error flag says: its first input copies may be in flight
+            const uint32_t h = misc[8];
+            misc[8] = kNoHeldItem;
+            misc[0] = h != kNoHeldItem ? h
+                      : *reinterpret_cast<volatile int*>(err) ? n_items
+                                                                : atomicAdd(&ctl[0], 1u);
+        }
         __syncthreads();
         const uint32_t idx = misc[0];
         if (idx >= n_items) break;
@@ -1522,16 +1592,10 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             continue;
         }
         if (MMA && kind == kItemEncodeMma) {
-            const bool ok = batch_mma_tile(&J, mma_ginv, it.kind_rg, it.a, it.b, it.s0, it.sn);
-            // the operand rings covered the encode region's barriers: set them up
-            // again; and the builders' generic stores there come before any
-            // later item's bulk copies (async proxy) into the same bytes
+            const bool ok = batch_mma_tile(jobs, items, n_items, ctl, err, idx, misc + 8);
+            // the builders' generic stores come before any later item's bulk
+            // copies (async proxy) into the same bytes
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (tid == 0) {
-                for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
-                fence_mbar_init();
-            }
-            phase = 0;
             __syncthreads();
             if (!ok) {
                 if (tid == 0) atomicOr(err, 1);
@@ -1549,6 +1613,14 @@ __global__ void __launch_bounds__(kEncThreads, 1)
             continue;
         }
         if (kind == kItemEncode) {
+            if (MMA) {  // its barriers, set up for this item alone (nothing is in flight now)
+                if (tid == 0) {
+                    for (int st = 0; st < kBatchEncStages; ++st) mbar_init(&bars[st], 1);
+                    fence_mbar_init();
+                }
+                phase = 0;
+                __syncthreads();
+            }
             // the job's precomputed basis when it has one, else derived per slice
             const uint32_t rg = (it.kind_rg >> 8) & 0xFFFFu, sn = it.sn ? it.sn : J.S;
             const uint32_t fold = 1u << ((it.kind_rg >> 24) & 3u);
@@ -1560,6 +1632,13 @@ __global__ void __launch_bounds__(kEncThreads, 1)
                                     : encode_tile<kEncChunks, true, 4, kBatchEncStages>(J.esrc, J.estride, sn, nullptr, J.RG, rg, J.R,
                                                                         it.a, syms, J.rec, J.rec_stride, enc, phase,
                                                                         J.first_exp, it.s0, acc, fold, J.ts);
+            if (MMA) {  // the barriers' bytes go back to the tensor-core input stages
+                __syncthreads();
+                if (tid == 0)
+                    for (int st = 0; st < kBatchEncStages; ++st) mbar_inval(&bars[st]);
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncthreads();
+            }
             if (!ok) {
                 if (tid == 0) atomicOr(err, 1);
                 break;
@@ -1577,6 +1656,14 @@ __global__ void __launch_bounds__(kEncThreads, 1)
     if (MMA) {  // every MMA issued has completed before TMEM is given back
         mma::tc_fence_before();
         __syncthreads();
+        if (tid == 0 && mma_misc[6]) {
+            // input stages issued ahead for a tile that did not run (the loop
+            // always runs a claimed tile, so this stays idle): they land before
+            // the CTA exits
+            const mma::Bars B(mma_bars);
+            for (uint32_t q = mma_misc[5]; q < mma_misc[5] + mma_misc[6]; ++q)
+                mma::bar_drain(B.in_full + 8 * (q % mma::kInStages), (q / mma::kInStages) & 1u);
+        }
         if ((tid >> 5) == 1) {
             if ((tid & 31) == 0) {
                 const mma::Bars B(mma_bars);

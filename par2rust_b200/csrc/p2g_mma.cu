@@ -161,9 +161,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     };
     for (uint32_t tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x) {
         const Tile T = tile_of(tile);
-        const bool more = tile + gridDim.x < n_tiles;
-        const Tile Tn = tile_of(more ? tile + gridDim.x : tile);
-        ok = run_tile<kGenWarps>(P, T, more ? &Tn : nullptr);
+        const uint32_t nt = tile + gridDim.x;
+        Tile Tn;
+        ok = run_tile<kGenWarps>(P, T, [&]() -> const Tile* {
+            if (nt >= n_tiles) return nullptr;
+            Tn = tile_of(nt);
+            return &Tn;
+        });
     }
     if (tid == 0 && !ok) atomicOr(err, 1);
     tc_fence_before();

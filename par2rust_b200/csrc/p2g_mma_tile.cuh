@@ -267,11 +267,19 @@ struct Pipe {
 // 32*(w%4)..).  Other warps idle.  Returns false (uniformly, after a CTA
 // barrier) when a bounded wait gave up; copies and MMAs in flight have then
 // landed.
-// next (may be null): the tile this CTA runs after this one; the producer
-// issues its first input stages while this tile's last K-steps and
-// epilogue run, so the next tile starts without a copy round trip.
-template <int NGEN>
-__device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T, const Tile* next = nullptr) {
+// next_fn: called once, by the producer thread alone, after it has issued
+// this tile's last input stage; it returns the tile this CTA runs next (it
+// stays valid until the producer has issued its first stages), or null.  The producer then issues
+// that tile's first input stages while this tile's last K-steps and epilogue
+// run, so the next tile starts without a copy round trip.  Only the producer
+// thread's P.pre counts (the stages it issued ahead); the next call must be
+// for that same tile.  When any role's wait gives up, the producer waits for
+// every copy it issued, the next tile's included, before this returns.
+struct NoNextTile {
+    __device__ const Tile* operator()() const { return nullptr; }
+};
+template <int NGEN, class NextFn>
+__device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T, NextFn&& next_fn) {
     static_assert(NGEN >= 8, "eight warps cover the two accumulators' four lane quadrants");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const Bars B(P.bars);
@@ -282,10 +290,9 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T, const Tile* nex
     // a tensor copy's x offset must be 16-byte aligned, the A image is cut in
     // whole input stages (the same in every thread)
     if ((T.n0 & 7u) || (T.s0 % kInSlices)) return false;
-    const bool ahead = next && !(next->n0 & 7u) && !(next->s0 % kInSlices);
-    const uint32_t NI_next =
-        ahead ? ((next->sn + kKSlices - 1) / kKSlices + kInSteps - 1) / kInSteps : 0u;
-    const uint32_t pre_next = NI_next < (uint32_t)kInStages ? NI_next : (uint32_t)kInStages;
+    // producer: the input-stage position after the last copy it issued and
+    // has not drained (0: none), the next tile's first stages included
+    uint32_t issued_end = 0;
     bool ok = true;
     if (warp == 0) {
         if (lane == 0) {
@@ -309,14 +316,22 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T, const Tile* nex
                     ok = false;
                     break;
                 }
-            for (uint32_t k = 0; ok && k < pre_next; ++k, ++gi)
-                if (!issue(*next, next->r0 / kTileRows, k, gi)) {
-                    ok = false;
-                    break;
-                }
-            if (!ok)  // copies issued but maybe not consumed land before the stages are reused
+            const Tile* U = ok ? next_fn() : nullptr;
+            if (U && !(U->n0 & 7u) && !(U->s0 % kInSlices)) {
+                const uint32_t NI_next = ((U->sn + kKSlices - 1) / kKSlices + kInSteps - 1) / kInSteps;
+                const uint32_t want = NI_next < (uint32_t)kInStages ? NI_next : (uint32_t)kInStages;
+                for (uint32_t k = 0; k < want; ++k, ++gi)
+                    if (!issue(*U, U->r0 / kTileRows, k, gi)) {
+                        ok = false;
+                        break;
+                    }
+            }
+            if (!ok) {  // copies issued but maybe not consumed land before the stages are reused
                 for (uint32_t q = gi > gi0 + kInStages ? gi - kInStages : gi0; q < gi; ++q)
                     bar_drain(B.in_full + 8 * (q % kInStages), (q / kInStages) & 1u);
+            } else {
+                issued_end = gi;  // >= gi0 + NI: this tile's stages all went out
+            }
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -470,9 +485,16 @@ __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T, const Tile* nex
         if (ok && lane == 0) bar_arrive(B.acc_empty);
     }
     const bool bad = __syncthreads_or(!ok) != 0;
+    if (bad && issued_end) {
+        // another role gave up: the copies the producer issued (this tile's
+        // last stages, the next tile's first) land before the stages are
+        // reused or the CTA exits
+        for (uint32_t q = issued_end - kInStages; q < issued_end; ++q)
+            if (q >= gi0) bar_drain(B.in_full + 8 * (q % kInStages), (q / kInStages) & 1u);
+    }
     P.g += NS;
     P.gi += NI;
-    P.pre = bad ? 0u : pre_next;
+    P.pre = bad || !issued_end ? 0u : issued_end - gi0 - NI;
     P.tcount += 1;
     if (bad) P.drains += 1;
     return !bad;
