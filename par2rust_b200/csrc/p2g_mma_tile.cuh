@@ -269,15 +269,13 @@ struct Pipe {
 // landed.
 // next_fn: called once, by the producer thread alone, after it has issued
 // this tile's last input stage; it returns the tile this CTA runs next (it
-// stays valid until the producer has issued its first stages), or null.  The producer then issues
-// that tile's first input stages while this tile's last K-steps and epilogue
-// run, so the next tile starts without a copy round trip.  Only the producer
-// thread's P.pre counts (the stages it issued ahead); the next call must be
-// for that same tile.  When any role's wait gives up, the producer waits for
-// every copy it issued, the next tile's included, before this returns.
-struct NoNextTile {
-    __device__ const Tile* operator()() const { return nullptr; }
-};
+// stays valid until the producer has issued its first stages), or null.
+// The producer then issues that tile's first input stages while this tile's
+// last K-steps and epilogue run, so the next tile starts without a copy
+// round trip.  Only the producer thread's P.pre counts (the stages it issued
+// ahead); the next call must be for that same tile.  When any role's wait
+// gives up, the producer waits for every copy it issued, the next tile's
+// included, before this returns.
 template <int NGEN, class NextFn>
 __device__ __forceinline__ bool run_tile(Pipe& P, const Tile& T, NextFn&& next_fn) {
     static_assert(NGEN >= 8, "eight warps cover the two accumulators' four lane quadrants");
